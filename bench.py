@@ -1,0 +1,337 @@
+#!/usr/bin/env python3
+"""Benchmark: bodies/s of the collision pipeline (GenerateAABB ->
+detectPossibleCollisions -> DoNarrowphase) at 1,048,576 mixed convex shapes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full pipeline pass over the scene (synthetic, seeded: 40%
+spheres, 30% boxes, 15% ellipsoids, 15% cylinders; half extents U[0.001,
+0.004]; random orientations; centres in [0,10]x[0,10]x[0,0.5]). `value` times
+the pipeline on device-resident inputs (L2 flushed between steps), `e2e` the
+same through the host-pointer C entry point with the host<->device copies
+inside the timed region. N > 1 (torchrun) runs one independent replica per
+GPU: weak scaling, no collective on the data path.
+
+The reference arm (--impl reference) times the reference's own CPU/OpenMP
+implementation (its sources compiled by oracle/Makefile into oracle/_ref) on
+the same scene with every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "collision-detection_b200"))
+
+N_BODIES = 1 << 20
+WORKLOAD = ("mixed_slab: 1,048,576 convex shapes (40% sphere, 30% box, 15% ellipsoid, 15% cylinder), "
+            "half extents U[0.001,0.004], uniform random orientations, centres U([0,10]x[0,10]x[0,0.5])")
+METRIC, UNIT = "bodies/s", "bodies/s"
+BINS = (16, 16, 16)  # the reference's default bins per axis (Broadphase.cu:37)
+
+# Algorithmic bytes per launch of each stage (reads + writes a perfect
+# implementation must move), as functions of N bodies, E search entries,
+# G search cells, P pairs, C contacts.
+STAGE_BYTES = {
+    "aabb": lambda N, E, G, P, C: 112 * N,            # 88 B of shape/body data in, 24 B of AABB out
+    "bounds": lambda N, E, G, P, C: 24 * N,
+    "count": lambda N, E, G, P, C: 48 * N + 4 * G,     # shift in place (24 r + 24 w) + cell counts
+    "scan_cells": lambda N, E, G, P, C: 8 * G,
+    "scatter": lambda N, E, G, P, C: 24 * N + 4 * G + 32 * E,
+    "pair_test": lambda N, E, G, P, C: 32 * E + 4 * G + 8 * P + 4 * N,
+    "scan_owner": lambda N, E, G, P, C: 12 * N,
+    "owner_scatter": lambda N, E, G, P, C: 16 * P + 8 * N,
+    "segsort": lambda N, E, G, P, C: 8 * N + 16 * P,
+    "mpr": lambda N, E, G, P, C: P * (8 + 2 * 88) + 56 * P,
+    "np_compact": lambda N, E, G, P, C: 60 * P + 60 * C,
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_BODIES, help=argparse.SUPPRESS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def scene_for(rank, n):
+    from collide_b200 import scenes as S
+    return S.mixed_slab(n, seed=rank)
+
+
+# ---------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling (200 ms) during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------- distributed
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------- reference (CPU) timing
+def reference_session(scene, threads):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from collide_b200 import tuner
+    grid = tuner.heuristic_dims(O.aabb(scene))
+    return O.RefSession(scene, grid, threads=threads, all_parallel=True), grid
+
+
+def cpu_baseline(scene, seconds):
+    """The reference's own CPU path on this host, every thread, bounded time."""
+    sess, grid = reference_session(scene, os.cpu_count() or 1)
+    sess.run()  # warm-up
+    times, t0 = [], time.perf_counter()
+    while len(times) < 3 or (time.perf_counter() - t0 < seconds and len(times) < 50):
+        t, P, C = sess.run()
+        times.append(float(t.sum()))
+    med = statistics.median(times)
+    out = {"value": scene.n / med, "unit": UNIT, "cores": sess.threads, "kind": "reference",
+           "sample": f"full {scene.n}-shape workload, {len(times)} runs (median), grid {list(grid)}, "
+                     f"all setParallelConfiguration flags on; pairs {P}, contacts {C}"}
+    sess.close()
+    return out
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args.gpus)
+    if rank != 0:
+        return 0
+    scene = scene_for(0, args.n)
+    sess, grid = reference_session(scene, os.cpu_count() or 1)
+    for _ in range(args.warmup):
+        sess.run()
+    times = []
+    for _ in range(args.steps):
+        t, P, C = sess.run()
+        times.append(float(t.sum()))
+    ms = 1000.0 * sum(times) / len(times)
+    value = scene.n / (ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "seed": 0, "grid": list(grid), "pairs": P, "contacts": C},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": sess.threads, "kind": "reference",
+                         "sample": f"each step = one GenerateAABB + detectPossibleCollisions + DoNarrowphase "
+                                   f"on the full {scene.n}-shape scene"},
+    }
+    sess.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------- our arm
+def traffic_from_profiles(kernel):
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    import collide_b200 as cb
+    scene = scene_for(rank, args.n)
+    ctx = cb.Context(local)
+    ds = cb.DeviceScene(scene, device=dev)
+    pipe = cb.DevicePipeline(ds, grid=BINS, ctx=ctx)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    for i in range(max(args.warmup, 3)):
+        pipe.run()
+        flush.fill_(i & 255)
+    torch.cuda.synchronize()
+    P, C = pipe.n_pairs, pipe.n_contacts
+    dims, E = ctx.last_grid()
+    G = dims[0] * dims[1] * dims[2]
+
+    # ---- value: device-resident, per-step CUDA events, L2 flushed between steps
+    ctx.set_profiling(True)
+    ctx.reset_stage_times()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    clocks = Clocks(local)
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_((i + 7) & 255)
+        evs[i][0].record(stream)
+        pipe.run()
+        evs[i][1].record(stream)
+        launches += ctx.launches()
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    clk = clocks.stop()
+    stage = ctx.stage_times()
+    ctx.set_profiling(False)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    total_ms = dist_max(total_ms, world)
+    ms = total_ms / args.steps
+    value = world * scene.n / (ms / 1000.0)
+
+    # ---- e2e: the host-pointer entry point, copies inside the timed region
+    hs = cb.HostSession(scene, grid=BINS, ctx=ctx)
+    for i in range(2):
+        hs.run()
+    evs2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_((i + 3) & 255)
+        evs2[i][0].record(stream)
+        hs.run()
+        evs2[i][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = dist_max(sum(a.elapsed_time(b) for a, b in evs2) / args.steps, world)
+    e2e = {"value": world * scene.n / (e2e_ms / 1000.0), "unit": UNIT, "ms_per_step": e2e_ms,
+           "h2d_bytes_per_step": hs.input_bytes(), "d2h_bytes_per_step": hs.output_bytes()}
+
+    # ---- roofline of the dominant kernel stage
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    kern = {k: v for k, v in stage.items() if k in STAGE_BYTES}
+    dom = max(kern, key=lambda k: kern[k][0])
+    dom_ms = kern[dom][0] / kern[dom][1]
+    dom_bytes = STAGE_BYTES[dom](scene.n, E, G, P, C)
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+    stage_summary = {k: {"ms_per_launch": v[0] / v[1], "share": v[0] / sum(x[0] for x in kern.values()),
+                         "algorithmic_GBps": STAGE_BYTES[k](scene.n, E, G, P, C) / (v[0] / v[1] / 1000) / 1e9}
+                     for k, v in kern.items()}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "seed": "rank", "bins_per_axis": list(BINS), "search_grid": list(dims),
+                   "entries": E, "pairs": P, "contacts": C, "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": dom_bytes, "traffic": traffic_from_profiles(dom)},
+        "stages": stage_summary,
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(scene, args.cpu_seconds)
+        except Exception as e:  # the reference build is missing: say so, do not fake it
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

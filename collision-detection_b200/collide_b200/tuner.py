@@ -1,0 +1,62 @@
+"""Search-grid choice of the broadphase.
+
+``heuristic_dims`` mirrors the device-side default of the library (make_plan
+in csrc/cc_broadphase.cu): cells sized so about ``cell_target`` boxes fall in
+each, but at least ``min_ratio`` mean box extents wide, capped at 1024 cells
+per axis and ``g_max`` cells in total. The pair list does not depend on the
+grid; only speed does.
+
+``autotune`` measures a few (cell_target, min_ratio) settings on the actual
+scene and keeps the fastest per size bucket.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+MAX_DIM = 1024
+
+
+def heuristic_dims(aabb, cell_target=4.0, min_ratio=2.0, g_max=None):
+    a = np.asarray(aabb, np.float32)
+    n = a.shape[0] // 2
+    if n == 0:
+        return (1, 1, 1)
+    mn, mx = a.min(0), a.max(0)
+    origin = np.abs(mn)
+    lo, hi = (mn + origin).astype(np.float32), (mx + origin).astype(np.float32)
+    ext = (hi - lo).astype(np.float64)
+    mean = (a[n:].astype(np.float64) - a[:n]).sum(0) / n
+    mean_max = float(mean.max())
+    floor_len = max(mean_max, 1e-30)
+    vol = float(np.prod(np.maximum(ext, floor_len)))
+    c = max(math.pow(vol * cell_target / n, 1.0 / 3.0), min_ratio * mean_max)
+    dims = [int(min(max(e / c if c > 0 else 1.0, 1.0), MAX_DIM)) for e in ext]
+    g_max = g_max or max(4096, n)
+    while dims[0] * dims[1] * dims[2] > g_max:
+        dims = [max(1, int(d * 0.8)) for d in dims]
+    return tuple(dims)
+
+
+_cache = {}
+
+
+def size_bucket(n):
+    return int(round(math.log2(max(n, 1)) * 2))
+
+
+def autotune(run_with, candidates=((2.0, 2.0), (4.0, 2.0), (8.0, 2.0), (4.0, 1.0), (16.0, 1.0)), reps=3,
+             key=None):
+    """run_with(cell_target, min_ratio) -> seconds of one broadphase call.
+    Returns the fastest (cell_target, min_ratio); cached under `key`."""
+    if key is not None and key in _cache:
+        return _cache[key]
+    best, best_t = None, float("inf")
+    for cand in candidates:
+        t = min(run_with(*cand) for _ in range(reps))
+        if t < best_t:
+            best, best_t = cand, t
+    if key is not None:
+        _cache[key] = best
+    return best

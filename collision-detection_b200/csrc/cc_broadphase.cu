@@ -1,0 +1,486 @@
+// Uniform-grid broadphase (the reference's Broadphase::detectPossibleCollisions,
+// src/broadphase/Broadphase.cu:344-545) as sm_100a kernels.
+//
+// Pair path (always):
+//   k_bounds        scene bounds + extent sums + validation     (Broadphase.cu:368-376)
+//   k_count         in-place shift by fabs(min) (:379-386) + per-cell counts on
+//                   the search grid
+//   scan            cell offsets (decoupled look-back)
+//   k_scatter       cell-ordered (AABB, body) entries
+//   k_pair_test     closed AABB overlap (:237) of every entry with the later
+//                   entries of its cell; a pair is emitted only from its home
+//                   cell (the lowest cell the two cell ranges share), so each
+//                   overlapping pair appears exactly once and no unique pass is
+//                   needed (replaces :484-533)
+//   scan            per-owner offsets (owner = smaller index)
+//   k_owner_scatter bucket pairs by owner; k_segsort sorts each bucket
+//                   -> the sorted, duplicate-free int64 list of :522-535
+//
+// Two overlapping boxes always share a cell of ANY grid built from a monotone
+// cell map (float subtraction, multiplication and truncation are monotone), and
+// the reference re-tests every candidate on the shifted boxes, so its pair list
+// is exactly {(a,b): a<b, closed overlap of the shifted boxes}: the search grid
+// here is chosen for speed, independent of the caller's bins per axis.
+//
+// Bin-list path (on request): the reference's own sorted (bin, body) list on
+// the caller's grid, with its HashMin truncation and unclamped linear index
+// (:125-200, :428-480), for parity checks.
+//
+// Compiled with -fmad=false (the shift and the bin scale must round exactly as
+// the reference's host build does).
+#include <algorithm>
+#include <climits>
+
+#include "cc_common.cuh"
+#include "cc_internal.h"
+#include "cc_math.cuh"
+#include "cc_stats.cuh"
+
+namespace cc {
+
+namespace {
+constexpr int kNT = 256;
+
+__device__ __forceinline__ float3 ld3p(const float *p, uint64_t i) { return f3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+__device__ __forceinline__ void st3p(float *p, uint64_t i, float3 v) {
+	p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z;
+}
+
+// Grid parameters from the reduced bounds. Every block of k_count computes it
+// (deterministically); block 0 also stores it for the later kernels.
+__device__ Plan make_plan(const DevStats *st, const GridParams &gp, int gx, int gy, int gz, uint64_t n) {
+	Plan p;
+	const int grid[3] = {gx, gy, gz};
+	float mn[3], mx[3];
+	p.valid = (st->err & (kErrNonFinite | kErrInverted)) ? 0 : 1;
+	for (int d = 0; d < 3; d++) {
+		mn[d] = ord2f(~st->bmin_inv[d]);
+		mx[d] = ord2f(st->bmax[d]);
+		p.origin[d] = fabsf(mn[d]);                                    // :379
+		p.invbin[d] = (float)grid[d] / fabsf(mx[d] + fabsf(mn[d]));    // :380-381
+		p.grid[d] = grid[d];
+		p.lo[d] = mn[d] + p.origin[d];  // exact minimum of the shifted coordinates
+	}
+	float ext[3], mean[3];
+	float mean_max = 0.f;
+	for (int d = 0; d < 3; d++) {
+		const float hi = mx[d] + p.origin[d];
+		ext[d] = hi - p.lo[d];
+		mean[d] = (float)(st->ext_sum[d] / (double)(n ? n : 1));
+		mean_max = fmaxf(mean_max, mean[d]);
+	}
+	int dim[3];
+	if (gp.user_dim[0] > 0) {
+		for (int d = 0; d < 3; d++) dim[d] = min(max(gp.user_dim[d], 1), kMaxDim);
+	} else {
+		// cell edge: the cube root of the volume that holds k_target boxes on
+		// average, but at least min_ratio times the mean box extent
+		double vol = 1.0;
+		const float floor_len = fmaxf(mean_max, 1e-30f);
+		for (int d = 0; d < 3; d++) vol *= (double)fmaxf(ext[d], floor_len);
+		double c = cbrt(vol * (double)gp.k_target / (double)(n ? n : 1));
+		c = fmax(c, (double)gp.min_ratio * (double)mean_max);
+		for (int d = 0; d < 3; d++) {
+			double q = c > 0.0 ? (double)ext[d] / c : 1.0;
+			dim[d] = (int)fmin(fmax(q, 1.0), (double)kMaxDim);
+		}
+	}
+	while ((uint64_t)dim[0] * dim[1] * dim[2] > gp.g_max) {
+		for (int d = 0; d < 3; d++) dim[d] = max(1, (int)(dim[d] * 0.8f));
+	}
+	for (int d = 0; d < 3; d++) {
+		p.dim[d] = dim[d];
+		p.inv[d] = ext[d] > 0.f ? (float)dim[d] / ext[d] : 0.f;
+	}
+	p.G = (uint32_t)dim[0] * dim[1] * dim[2];
+	return p;
+}
+
+// Search-grid cell of a shifted coordinate: monotone in v.
+__device__ __forceinline__ int cell_of(float v, float lo, float inv, int dim) {
+	float t = (v - lo) * inv;
+	int c = (int)fminf(fmaxf(t, 0.f), (float)(dim - 1));
+	return c;
+}
+struct CellRange {
+	int c0[3], c1[3];
+};
+__device__ __forceinline__ CellRange cell_range(const Plan &p, float3 mn, float3 mx) {
+	CellRange r;
+	r.c0[0] = cell_of(mn.x, p.lo[0], p.inv[0], p.dim[0]);
+	r.c0[1] = cell_of(mn.y, p.lo[1], p.inv[1], p.dim[1]);
+	r.c0[2] = cell_of(mn.z, p.lo[2], p.inv[2], p.dim[2]);
+	r.c1[0] = cell_of(mx.x, p.lo[0], p.inv[0], p.dim[0]);
+	r.c1[1] = cell_of(mx.y, p.lo[1], p.inv[1], p.dim[1]);
+	r.c1[2] = cell_of(mx.z, p.lo[2], p.inv[2], p.dim[2]);
+	return r;
+}
+__device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
+	return (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
+}
+
+__global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restrict__ aabb, DevStats *stats) {
+	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	float3 mn = f3(0.f, 0.f, 0.f), mx = mn;
+	const bool have = i < n;
+	if (have) {
+		mn = ld3p(aabb, i);
+		mx = ld3p(aabb, i + n);
+	}
+	accumulate_stats<kNT>(mn, mx, have, stats);
+}
+
+__global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, GridParams gp, int gx, int gy,
+                                                int gz, DevStats *stats, uint32_t *__restrict__ cell_count,
+                                                uint32_t *__restrict__ owner_count) {
+	__shared__ Plan sp;
+	if (threadIdx.x == 0) {
+		sp = make_plan(stats, gp, gx, gy, gz, n);
+		if (blockIdx.x == 0) stats->plan = sp;
+	}
+	__syncthreads();
+	if (!sp.valid) return;  // invalid input: nothing is modified
+	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (i >= n) return;
+	const float3 o = f3(sp.origin[0], sp.origin[1], sp.origin[2]);
+	const float3 mn = ld3p(aabb, i) + o, mx = ld3p(aabb, i + n) + o;  // :382-386
+	st3p(aabb, i, mn);
+	st3p(aabb, i + n, mx);
+	owner_count[i] = 0u;
+	const CellRange r = cell_range(sp, mn, mx);
+	for (int z = r.c0[2]; z <= r.c1[2]; z++)
+		for (int y = r.c0[1]; y <= r.c1[1]; y++)
+			for (int x = r.c0[0]; x <= r.c1[0]; x++)
+				atomicAdd(&cell_count[(uint32_t)x + (uint32_t)sp.dim[0] * ((uint32_t)y + (uint32_t)sp.dim[1] * z)], 1u);
+}
+
+__global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
+                                                  const uint32_t *__restrict__ cell_start,
+                                                  uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
+                                                  uint64_t cap, uint32_t *err) {
+	__shared__ Plan sp;
+	if (threadIdx.x == 0) sp = stats->plan;
+	__syncthreads();
+	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (!sp.valid || i >= n) return;
+	const float3 mn = ld3p(aabb, i), mx = ld3p(aabb, i + n);
+	const CellRange r = cell_range(sp, mn, mx);
+	bool over = false;
+	for (int z = r.c0[2]; z <= r.c1[2]; z++)
+		for (int y = r.c0[1]; y <= r.c1[1]; y++)
+			for (int x = r.c0[0]; x <= r.c1[0]; x++) {
+				const uint32_t c = (uint32_t)x + (uint32_t)sp.dim[0] * ((uint32_t)y + (uint32_t)sp.dim[1] * z);
+				const uint64_t slot = (uint64_t)cell_start[c] + atomicAdd(&cursor[c], 1u);
+				if (slot < cap) {
+					entries[2 * slot] = make_float4(mn.x, mn.y, mn.z, __uint_as_float((uint32_t)i));
+					entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(pack_cell(x, y, z)));
+				} else {
+					over = true;
+				}
+			}
+	if (over) atomicOr(err, (uint32_t)kErrCapacity);
+}
+
+// One lane per entry; each lane tests its entry against the later entries of
+// the same cell. Loops are warp-uniform so the emission can be warp-aggregated.
+__global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const uint32_t *__restrict__ cell_start,
+                                                    const float4 *__restrict__ entries,
+                                                    uint64_t entry_cap, uint32_t *__restrict__ owner_count,
+                                                    unsigned long long *__restrict__ pairs, uint64_t pair_cap,
+                                                    unsigned long long *pair_counter) {
+	__shared__ Plan sp;
+	if (threadIdx.x == 0) sp = stats->plan;
+	__syncthreads();
+	if (!sp.valid) return;
+	const uint64_t E = min((uint64_t)stats->entries, entry_cap);
+	const uint32_t lane = threadIdx.x & 31;
+	const uint32_t lt = (1u << lane) - 1u;
+	const uint64_t warps = (uint64_t)gridDim.x * (kNT / 32);
+	for (uint64_t base = ((uint64_t)blockIdx.x * (kNT / 32) + (threadIdx.x >> 5)) * 32; base < E; base += warps * 32) {
+		const uint64_t e = base + lane;
+		const bool valid = e < E;
+		float4 alo = make_float4(0.f, 0.f, 0.f, 0.f), ahi = alo;
+		int my_n = 0;
+		int cx = 0, cy = 0, cz = 0;
+		if (valid) {
+			alo = entries[2 * e];
+			ahi = entries[2 * e + 1];
+			const uint32_t pc = __float_as_uint(ahi.w);
+			cx = pc & 1023; cy = (pc >> 10) & 1023; cz = (pc >> 20) & 1023;
+			const uint32_t c = (uint32_t)cx + (uint32_t)sp.dim[0] * ((uint32_t)cy + (uint32_t)sp.dim[1] * cz);
+			const uint64_t end = min((uint64_t)cell_start[c + 1], entry_cap);
+			my_n = (int)(end > e + 1 ? end - e - 1 : 0);
+		}
+		const uint32_t ida = __float_as_uint(alo.w);
+		// home-cell test: the pair belongs to this cell iff, on every axis, one
+		// of the two min corners lies in this cell's slab
+		const bool ax = valid && cell_of(alo.x, sp.lo[0], sp.inv[0], sp.dim[0]) == cx;
+		const bool ay = valid && cell_of(alo.y, sp.lo[1], sp.inv[1], sp.dim[1]) == cy;
+		const bool az = valid && cell_of(alo.z, sp.lo[2], sp.inv[2], sp.dim[2]) == cz;
+		const int iters = __reduce_max_sync(0xffffffffu, my_n);
+		uint32_t owned = 0;
+		for (int t = 0; t < iters; t++) {
+			bool emit = false;
+			unsigned long long key = 0;
+			uint32_t other_owner = 0xffffffffu;
+			if (t < my_n) {
+				const uint64_t q = e + 1 + t;
+				const float4 blo = entries[2 * q], bhi = entries[2 * q + 1];
+				if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
+				    blo.z <= ahi.z) {
+					const bool hx = ax || cell_of(blo.x, sp.lo[0], sp.inv[0], sp.dim[0]) == cx;
+					const bool hy = ay || cell_of(blo.y, sp.lo[1], sp.inv[1], sp.dim[1]) == cy;
+					const bool hz = az || cell_of(blo.z, sp.lo[2], sp.inv[2], sp.dim[2]) == cz;
+					if (hx && hy && hz) {
+						const uint32_t idb = __float_as_uint(blo.w);
+						const uint32_t lo = min(ida, idb), hi = max(ida, idb);
+						key = ((unsigned long long)lo << 32) | hi;
+						emit = true;
+						if (lo == ida) owned++;
+						else other_owner = lo;
+					}
+				}
+			}
+			const uint32_t b = __ballot_sync(0xffffffffu, emit);
+			if (b) {
+				unsigned long long start = 0;
+				const int leader = __ffs(b) - 1;
+				if ((int)lane == leader) start = atomicAdd(pair_counter, (unsigned long long)__popc(b));
+				start = __shfl_sync(0xffffffffu, start, leader);
+				if (emit) {
+					const unsigned long long pos = start + __popc(b & lt);
+					if (pos < pair_cap) pairs[pos] = key;
+					if (other_owner != 0xffffffffu) atomicAdd(&owner_count[other_owner], 1u);
+				}
+			}
+		}
+		if (owned) atomicAdd(&owner_count[ida], owned);
+	}
+}
+
+__global__ void __launch_bounds__(kNT) k_owner_scatter(uint64_t P, const unsigned long long *__restrict__ tmp,
+                                                        const unsigned long long *__restrict__ owner_off,
+                                                        uint32_t *__restrict__ owner_count,
+                                                        unsigned long long *__restrict__ out) {
+	const uint64_t t = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (t >= P) return;
+	const unsigned long long key = tmp[t];
+	const uint32_t a = (uint32_t)(key >> 32);
+	const uint32_t k = atomicSub(&owner_count[a], 1u) - 1u;
+	out[owner_off[a] + k] = key;
+}
+
+constexpr int kSmallSeg = 32;
+constexpr int kBigSeg = 4096;
+
+__global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long long *__restrict__ owner_off,
+                                                  unsigned long long *__restrict__ out, uint32_t *big_list,
+                                                  uint64_t big_cap, DevStats *stats) {
+	const uint64_t a = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (a >= n) return;
+	const uint64_t beg = owner_off[a], end = owner_off[a + 1];
+	const uint64_t len = end - beg;
+	if (len <= 1) return;
+	if (len <= kSmallSeg) {  // insertion sort in place
+		for (uint64_t i = beg + 1; i < end; i++) {
+			const unsigned long long k = out[i];
+			uint64_t j = i;
+			while (j > beg && out[j - 1] > k) {
+				out[j] = out[j - 1];
+				j--;
+			}
+			out[j] = k;
+		}
+		return;
+	}
+	atomicMax(&stats->max_segment, (unsigned long long)len);
+	if (len > kBigSeg) {
+		atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
+		return;
+	}
+	const unsigned long long slot = atomicAdd(&stats->big_segments, 1ull);
+	if (slot < big_cap) big_list[slot] = (uint32_t)a;
+	else atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
+}
+
+// One block per segment of 33..4096 keys: bitonic sort in shared memory.
+__global__ void __launch_bounds__(512) k_segsort_big(const uint32_t *__restrict__ big_list,
+                                                      const unsigned long long *__restrict__ owner_off,
+                                                      unsigned long long *__restrict__ out) {
+	__shared__ unsigned long long s[kBigSeg];
+	const uint32_t a = big_list[blockIdx.x];
+	const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
+	int m = 1;
+	while ((uint64_t)m < len) m <<= 1;
+	for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? out[beg + i] : ~0ull;
+	__syncthreads();
+	for (int k = 2; k <= m; k <<= 1) {
+		for (int j = k >> 1; j > 0; j >>= 1) {
+			for (int i = threadIdx.x; i < m; i += blockDim.x) {
+				const int p = i ^ j;
+				if (p > i) {
+					const bool up = (i & k) == 0;
+					const unsigned long long x = s[i], y = s[p];
+					if ((x > y) == up) { s[i] = y; s[p] = x; }
+				}
+			}
+			__syncthreads();
+		}
+	}
+	for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = s[i];
+}
+
+// ---------------------------------------------------------------- bin list
+// float -> int as the reference's host build converts (x86 cvttss2si: NaN and
+// out-of-range values give INT_MIN), HashMin Broadphase.cu:125-133.
+__device__ __forceinline__ int32_t trunc_x86(float v) {
+	if (!(v >= -2147483648.0f && v < 2147483648.0f)) return INT_MIN;
+	return __float2int_rz(v);
+}
+struct RefRange {
+	int32_t g0[3], g1[3];
+};
+__device__ __forceinline__ RefRange ref_range(const Plan &p, float3 mn, float3 mx) {
+	RefRange r;
+	r.g0[0] = trunc_x86(mn.x * p.invbin[0]);
+	r.g0[1] = trunc_x86(mn.y * p.invbin[1]);
+	r.g0[2] = trunc_x86(mn.z * p.invbin[2]);
+	r.g1[0] = trunc_x86(mx.x * p.invbin[0]);
+	r.g1[1] = trunc_x86(mx.y * p.invbin[1]);
+	r.g1[2] = trunc_x86(mx.z * p.invbin[2]);
+	return r;
+}
+
+// function_Count_AABB_BIN_Intersection (:150-154) on the shifted boxes.
+__global__ void __launch_bounds__(kNT) k_ref_count(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
+                                                    uint32_t *__restrict__ cnt) {
+	__shared__ Plan sp;
+	if (threadIdx.x == 0) sp = stats->plan;
+	__syncthreads();
+	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (i >= n) return;
+	const RefRange r = ref_range(sp, ld3p(aabb, i), ld3p(aabb, i + n));
+	const uint32_t c = (uint32_t)(r.g1[0] - r.g0[0] + 1) * (uint32_t)(r.g1[1] - r.g0[1] + 1) *
+	                   (uint32_t)(r.g1[2] - r.g0[2] + 1);
+	cnt[i] = c;
+}
+
+// function_Store_AABB_BIN_Intersection (:172-195): x outer, z inner, bin id
+// z*gy*gx + y*gx + x in uint arithmetic (Hash_Index :140-147); the key is
+// (bin << 32) | body so a stable sort on the upper half gives :428-432.
+__global__ void __launch_bounds__(kNT) k_ref_emit(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
+                                                   const unsigned long long *__restrict__ off,
+                                                   unsigned long long *__restrict__ keys, uint64_t cap) {
+	__shared__ Plan sp;
+	if (threadIdx.x == 0) sp = stats->plan;
+	__syncthreads();
+	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (i >= n) return;
+	const RefRange r = ref_range(sp, ld3p(aabb, i), ld3p(aabb, i + n));
+	const uint32_t gx = (uint32_t)sp.grid[0], gy = (uint32_t)sp.grid[1];
+	uint64_t w = off[i];
+	const uint64_t wend = off[i + 1];
+	uint32_t mb = 0;
+	for (uint32_t x = (uint32_t)r.g0[0]; x <= (uint32_t)r.g1[0]; x++)
+		for (uint32_t y = (uint32_t)r.g0[1]; y <= (uint32_t)r.g1[1]; y++)
+			for (uint32_t z = (uint32_t)r.g0[2]; z <= (uint32_t)r.g1[2] && w < wend; z++) {
+				const uint32_t bin = z * gy * gx + y * gx + x;
+				mb = max(mb, bin);
+				if (w < cap) keys[w] = ((unsigned long long)bin << 32) | (uint32_t)i;
+				w++;
+			}
+	atomicMax(&stats->max_bin, mb);
+	if (w != wend) atomicOr(&stats->err, (uint32_t)kErrBinCount);
+}
+
+__global__ void __launch_bounds__(kNT) k_ref_flags(const unsigned long long *__restrict__ keys, uint64_t E,
+                                                    uint32_t *__restrict__ flags) {
+	const uint64_t e = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (e >= E) return;
+	flags[e] = (e == 0 || (keys[e] >> 32) != (keys[e - 1] >> 32)) ? 1u : 0u;
+}
+
+// reduce_by_key (:439-443) + inclusive scan of the run lengths (:476-480).
+__global__ void __launch_bounds__(kNT) k_ref_split(const unsigned long long *__restrict__ keys, uint64_t E,
+                                                    const uint32_t *__restrict__ run_pos, uint32_t *bin_number,
+                                                    uint32_t *body_number, uint32_t *active_bins, uint32_t *bin_end,
+                                                    uint64_t cap_a) {
+	const uint64_t e = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	if (e >= E) return;
+	const unsigned long long k = keys[e];
+	const uint32_t bin = (uint32_t)(k >> 32);
+	if (bin_number) bin_number[e] = bin;
+	if (body_number) body_number[e] = (uint32_t)k;
+	const uint32_t r = run_pos[e + 1] - 1u;  // run index of this entry
+	if (r < cap_a) {
+		if (active_bins && run_pos[e] == r) active_bins[r] = bin;  // first entry of the run
+		if (bin_end && (e + 1 == E || run_pos[e + 2] != run_pos[e + 1])) bin_end[r] = (uint32_t)(e + 1);
+	}
+}
+
+inline unsigned blocks_for(uint64_t n) { return (unsigned)((n + kNT - 1) / kNT); }
+}  // namespace
+
+void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, cudaStream_t s) {
+	if (n) k_bounds<<<blocks_for(n), kNT, 0, s>>>(n, aabb, stats);
+}
+
+void launch_count(uint64_t n, float *aabb, const GridParams &gp, const int grid[3], const BpBuffers &b,
+                  cudaStream_t s) {
+	k_count<<<blocks_for(n), kNT, 0, s>>>(n, aabb, gp, grid[0], grid[1], grid[2], b.stats, b.cell_count,
+	                                      b.owner_count);
+}
+
+void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
+	launch_scan_u32_to_u32(b.cell_count, g_max, b.cell_start, b.status, b.ticket, &b.stats->err, s, &b.stats->plan.G,
+	                       &b.stats->entries);
+}
+
+void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
+	k_scatter<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries, b.entry_cap,
+	                                        &b.stats->err);
+}
+
+void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s) {
+	(void)n;
+	uint64_t want = (entries_hint + kNT - 1) / kNT;
+	unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(want, 1), (uint64_t)kNumSMs * 8);
+	k_pair_test<<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count, b.pairs_tmp,
+	                                 b.pair_cap, &b.stats->pairs);
+}
+
+void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s) {
+	launch_scan_u32_to_u64(b.owner_count, n, b.owner_off, b.status, b.ticket, &b.stats->err, s);
+}
+
+void launch_owner_scatter(uint64_t P, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
+	if (P) k_owner_scatter<<<blocks_for(P), kNT, 0, s>>>(P, b.pairs_tmp, b.owner_off, b.owner_count, out);
+}
+
+void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
+	k_segsort<<<blocks_for(n), kNT, 0, s>>>(n, b.owner_off, out, b.big_list, b.big_cap, b.stats);
+}
+
+void launch_segsort_big(uint64_t nbig, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
+	if (nbig) k_segsort_big<<<(unsigned)nbig, 512, 0, s>>>(b.big_list, b.owner_off, out);
+}
+
+void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s) {
+	if (n) k_ref_count<<<blocks_for(n), kNT, 0, s>>>(n, aabb_shifted, stats, cnt);
+}
+void launch_ref_emit(uint64_t n, const float *aabb_shifted, DevStats *stats, const unsigned long long *off,
+                     unsigned long long *keys, uint64_t cap, cudaStream_t s) {
+	if (n) k_ref_emit<<<blocks_for(n), kNT, 0, s>>>(n, aabb_shifted, stats, off, keys, cap);
+}
+void launch_ref_flags(const unsigned long long *keys, uint64_t E, uint32_t *flags, cudaStream_t s) {
+	if (E) k_ref_flags<<<blocks_for(E), kNT, 0, s>>>(keys, E, flags);
+}
+void launch_ref_split(const unsigned long long *keys, uint64_t E, const uint32_t *run_pos, uint32_t *bin_number,
+                      uint32_t *body_number, uint32_t *active_bins, uint32_t *bin_end, uint64_t cap_a,
+                      cudaStream_t s) {
+	if (E)
+		k_ref_split<<<blocks_for(E), kNT, 0, s>>>(keys, E, run_pos, bin_number, body_number, active_bins, bin_end,
+		                                          cap_a);
+}
+
+}  // namespace cc

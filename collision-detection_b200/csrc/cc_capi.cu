@@ -1,0 +1,804 @@
+// C ABI of libcollide_b200.so (include/collide_b200.h): context, scratch
+// management and the host-side orchestration of the kernels. No kernels live
+// here; every device pass is a launcher from cc_aabb.cu, cc_broadphase.cu,
+// cc_narrowphase.cu or cc_sort.cu.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/collide_b200.h"
+#include "cc_common.cuh"
+#include "cc_internal.h"
+
+using namespace cc;
+
+namespace {
+
+struct Buf {
+	void *p = nullptr;
+	size_t bytes = 0;
+};
+
+// Kernel stages timed by the optional profiler.
+enum Stage : int {
+	ST_AABB, ST_BOUNDS, ST_COUNT, ST_SCAN_CELLS, ST_SCATTER, ST_PAIR_TEST, ST_SCAN_OWNER, ST_OWNER_SCATTER,
+	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_COUNT_
+};
+const char *kStageNames[ST_COUNT_] = {"aabb", "bounds", "count", "scan_cells", "scatter", "pair_test",
+                                      "scan_owner", "owner_scatter", "segsort", "mpr", "np_compact", "bins",
+                                      "copy_in", "copy_out"};
+constexpr int kMaxMarks = 64;
+
+}  // namespace
+
+struct cc_ctx {
+	int device = 0;
+	std::string err;
+	GridParams gp{};
+	cudaError_t cuda_err = cudaSuccess;
+	// device scratch
+	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list;
+	Buf ref_cnt, ref_off, ref_keys, ref_tmp, ref_flags, ref_runpos, rx_hist, rx_hoff;
+	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos;
+	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
+	    out_depth, out_bids;
+	DevStats *h_stats = nullptr;  // pinned
+	uint64_t *h_word = nullptr;   // pinned scratch words
+	// retained broadphase result (owner buckets not yet scattered)
+	bool retained = false;
+	uint64_t retained_n = 0, retained_P = 0;
+	uint64_t last_E = 0, last_P = 0;
+	int last_dim[3] = {0, 0, 0};
+	uint64_t launches = 0;
+	// stage profiler
+	bool prof = false;
+	cudaEvent_t ev[2 * kMaxMarks] = {};
+	int mark_stage[kMaxMarks] = {};
+	int nmarks = 0;
+	double stage_ms[ST_COUNT_] = {};
+	uint64_t stage_n[ST_COUNT_] = {};
+};
+
+namespace {
+
+cc_status set_err(cc_ctx *c, cc_status st, const char *fmt, ...) {
+	char buf[512];
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(buf, sizeof(buf), fmt, ap);
+	va_end(ap);
+	c->err = buf;
+	return st;
+}
+
+#define CC_CUDA(c, expr)                                                                                 \
+	do {                                                                                                 \
+		cudaError_t e_ = (expr);                                                                         \
+		if (e_ != cudaSuccess) {                                                                         \
+			(c)->cuda_err = e_;                                                                          \
+			return set_err((c), e_ == cudaErrorMemoryAllocation ? CC_ERR_OUT_OF_MEMORY : CC_ERR_CUDA,   \
+			               "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__);        \
+		}                                                                                                \
+	} while (0)
+
+#define CC_TRY(expr)                    \
+	do {                                \
+		cc_status s_ = (expr);          \
+		if (s_ != CC_OK) return s_;     \
+	} while (0)
+
+cc_status ensure(cc_ctx *c, Buf &b, size_t bytes) {
+	if (bytes <= b.bytes) return CC_OK;
+	size_t nb = std::max(bytes, b.bytes + b.bytes / 2);
+	nb = (nb + 255) & ~size_t(255);
+	if (b.p) {
+		CC_CUDA(c, cudaFree(b.p));
+		b.p = nullptr;
+		b.bytes = 0;
+	}
+	CC_CUDA(c, cudaMalloc(&b.p, nb));
+	b.bytes = nb;
+	return CC_OK;
+}
+
+template <class T>
+T *ptr(const Buf &b) { return reinterpret_cast<T *>(b.p); }
+
+// Brackets one stage with events when profiling is on (RAII).
+struct StageMark {
+	cc_ctx *c;
+	int slot = -1;
+	cudaStream_t s;
+	StageMark(cc_ctx *c_, int stage, cudaStream_t s_) : c(c_), s(s_) {
+		if (!c->prof || c->nmarks >= kMaxMarks) return;
+		slot = c->nmarks++;
+		c->mark_stage[slot] = stage;
+		cudaEventRecord(c->ev[2 * slot], s);
+	}
+	~StageMark() {
+		if (slot >= 0) cudaEventRecord(c->ev[2 * slot + 1], s);
+	}
+};
+
+void prof_collect(cc_ctx *c);
+
+// Collects a call's stage marks on every return path.
+struct ProfGuard {
+	cc_ctx *c;
+	cudaStream_t s;
+	ProfGuard(cc_ctx *c_, void *s_) : c(c_), s((cudaStream_t)s_) { c->nmarks = 0; }
+	~ProfGuard() {
+		if (c->prof && c->nmarks) {
+			cudaStreamSynchronize(s);
+			prof_collect(c);
+		}
+	}
+};
+
+// Folds the completed marks of a call into the totals (after its final sync).
+void prof_collect(cc_ctx *c) {
+	for (int i = 0; i < c->nmarks; i++) {
+		float ms = 0.f;
+		if (cudaEventElapsedTime(&ms, c->ev[2 * i], c->ev[2 * i + 1]) == cudaSuccess) {
+			c->stage_ms[c->mark_stage[i]] += ms;
+			c->stage_n[c->mark_stage[i]] += 1;
+		}
+	}
+	c->nmarks = 0;
+}
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+cc_status check_launch(cc_ctx *c) {
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) {
+		c->cuda_err = e;
+		return set_err(c, CC_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+	}
+	return CC_OK;
+}
+
+cc_status read_stats(cc_ctx *c, cudaStream_t s) {
+	CC_CUDA(c, cudaMemcpyAsync(c->h_stats, c->stats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, s));
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	return CC_OK;
+}
+
+cc_status device_err(cc_ctx *c) {
+	const uint32_t e = c->h_stats->err;
+	if (e & (kErrNonFinite | kErrInverted))
+		return set_err(c, CC_ERR_INVALID_INPUT, "AABB input has %s%s", (e & kErrNonFinite) ? "non-finite corners " : "",
+		               (e & kErrInverted) ? "boxes with min > max" : "");
+	if (e & kErrBadIndex) return set_err(c, CC_ERR_INVALID_INPUT, "a body id is >= nb");
+	if (e & kErrSpinLimit) return set_err(c, CC_ERR_INTERNAL, "device-side look-back wait gave up");
+	return CC_OK;
+}
+
+uint32_t g_max_for(uint64_t n) {
+	uint64_t g = std::max<uint64_t>(4096, n);
+	return (uint32_t)std::min<uint64_t>(g, (uint64_t)1 << 28);
+}
+
+BpBuffers bp_buffers(cc_ctx *c) {
+	BpBuffers b;
+	b.stats = ptr<DevStats>(c->stats);
+	b.cell_count = ptr<uint32_t>(c->cell_count);
+	b.cell_start = ptr<uint32_t>(c->cell_start);
+	b.g_max = c->gp.g_max;
+	b.entries = ptr<float4>(c->entries);
+	b.entry_cap = c->entries.bytes / (2 * sizeof(float4));
+	b.owner_count = ptr<uint32_t>(c->owner_count);
+	b.owner_off = ptr<unsigned long long>(c->owner_off);
+	b.pairs_tmp = ptr<unsigned long long>(c->pairs_tmp);
+	b.pair_cap = c->pairs_tmp.bytes / sizeof(unsigned long long);
+	b.status = ptr<uint64_t>(c->status);
+	b.ticket = ptr<uint32_t>(c->ticket);
+	b.big_list = ptr<uint32_t>(c->big_list);
+	b.big_cap = c->big_list.bytes / sizeof(uint32_t);
+	return b;
+}
+
+size_t status_words_for(uint64_t n) { return scan_tiles(n) + 8; }
+
+// Allocates the n-dependent broadphase scratch.
+cc_status bp_prepare(cc_ctx *c, uint64_t n) {
+	c->gp.g_max = g_max_for(n);
+	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
+	CC_TRY(ensure(c, c->cell_count, sizeof(uint32_t) * c->gp.g_max));
+	CC_TRY(ensure(c, c->cell_start, sizeof(uint32_t) * (c->gp.g_max + 1)));
+	CC_TRY(ensure(c, c->owner_count, sizeof(uint32_t) * std::max<uint64_t>(n, 1)));
+	CC_TRY(ensure(c, c->owner_off, sizeof(unsigned long long) * (n + 1)));
+	const uint64_t e_guess = std::max<uint64_t>(c->last_E + c->last_E / 4, 2 * n + 1024);
+	CC_TRY(ensure(c, c->entries, 2 * sizeof(float4) * e_guess));
+	const uint64_t p_guess = std::max<uint64_t>(c->last_P + c->last_P / 4, n / 4 + 1024);
+	CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * p_guess));
+	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(std::max<uint64_t>(c->gp.g_max, n + 1))));
+	CC_TRY(ensure(c, c->ticket, 64));
+	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * std::max<uint64_t>(1024, n / 16)));
+	return CC_OK;
+}
+
+// Broadphase up to the per-owner offsets. Requires stats zeroed and the
+// bounds pass done (k_bounds or the fused AABB kernel). Returns P in *P_out.
+cc_status bp_core(cc_ctx *c, uint64_t n, float *aabb, const int grid[3], cudaStream_t s, uint64_t *P_out) {
+	BpBuffers b = bp_buffers(c);
+	const uint32_t gmax = c->gp.g_max;
+	{
+		StageMark m(c, ST_COUNT, s);
+		CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s));
+		launch_count(n, aabb, c->gp, grid, b, s);
+	}
+	{
+		StageMark m(c, ST_SCAN_CELLS, s);
+		launch_scan_cells(b, gmax, s);
+	}
+	{
+		StageMark m(c, ST_SCATTER, s);
+		CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s));
+		launch_scatter(n, aabb, b, s);
+	}
+	{
+		StageMark m(c, ST_PAIR_TEST, s);
+		launch_pair_test(n, b, std::max<uint64_t>(c->last_E, n), s);
+	}
+	{
+		StageMark m(c, ST_SCAN_OWNER, s);
+		launch_scan_owner(n, b, s);
+	}
+	c->launches += 5;
+	CC_TRY(check_launch(c));
+	CC_TRY(read_stats(c, s));
+	CC_TRY(device_err(c));
+	uint64_t E = c->h_stats->entries, P = c->h_stats->pairs;
+	for (int round = 0; round < 2 && (E > b.entry_cap || P > b.pair_cap); round++) {
+		// a capacity guess was too small: grow and redo the passes after the count
+		if (E > b.entry_cap) {
+			if (E >= 0xffffffffull) return set_err(c, CC_ERR_CAPACITY, "search grid needs %llu entries (>= 2^32)",
+			                                        (unsigned long long)E);
+			CC_TRY(ensure(c, c->entries, 2 * sizeof(float4) * (E + E / 8)));
+		}
+		if (P > b.pair_cap) CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * (P + P / 8)));
+		b = bp_buffers(c);
+		CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s));
+		CC_CUDA(c, cudaMemsetAsync(b.owner_count, 0, sizeof(uint32_t) * n, s));
+		CC_CUDA(c, cudaMemsetAsync(&b.stats->pairs, 0, sizeof(unsigned long long), s));
+		launch_scatter(n, aabb, b, s);
+		launch_pair_test(n, b, E, s);
+		launch_scan_owner(n, b, s);
+		c->launches += 3;
+		CC_TRY(check_launch(c));
+		CC_TRY(read_stats(c, s));
+		CC_TRY(device_err(c));
+		E = c->h_stats->entries;
+		P = c->h_stats->pairs;
+	}
+	if (E > b.entry_cap || P > b.pair_cap)
+		return set_err(c, CC_ERR_INTERNAL, "broadphase scratch did not converge (E=%llu P=%llu)",
+		               (unsigned long long)E, (unsigned long long)P);
+	c->last_E = E;
+	c->last_P = P;
+	for (int d = 0; d < 3; d++) c->last_dim[d] = c->h_stats->plan.dim[d];
+	*P_out = P;
+	return CC_OK;
+}
+
+// Buckets the retained pairs by owner into `out` and sorts every bucket.
+cc_status bp_emit(cc_ctx *c, uint64_t n, uint64_t P, unsigned long long *out, cudaStream_t s) {
+	BpBuffers b = bp_buffers(c);
+	{
+		StageMark m(c, ST_OWNER_SCATTER, s);
+		launch_owner_scatter(P, out, b, s);
+	}
+	{
+		StageMark m(c, ST_SEGSORT, s);
+		launch_segsort(n, out, b, s);
+	}
+	c->launches += 2;
+	CC_TRY(check_launch(c));
+	CC_TRY(read_stats(c, s));
+	const uint64_t nbig = std::min<uint64_t>(c->h_stats->big_segments, b.big_cap);
+	if (nbig) {
+		StageMark m(c, ST_SEGSORT, s);
+		launch_segsort_big(nbig, out, b, s);
+		c->launches += 1;
+	}
+	if (c->h_stats->err & kErrSegmentTooLong) {
+		// a bucket is longer than the block sort handles: sort the whole list
+		const size_t hw = radix_hist_words(P);
+		CC_TRY(ensure(c, c->ref_tmp, sizeof(unsigned long long) * P));
+		CC_TRY(ensure(c, c->rx_hist, sizeof(uint32_t) * hw));
+		CC_TRY(ensure(c, c->rx_hoff, sizeof(unsigned long long) * (hw + 1)));
+		CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(hw + 1)));
+		int bits = 1;
+		while (bits < 32 && ((uint64_t)1 << bits) < n) bits++;
+		radix_sort_u64(out, ptr<unsigned long long>(c->ref_tmp), P, 0, 32 + bits, ptr<uint32_t>(c->rx_hist),
+		               ptr<unsigned long long>(c->rx_hoff), ptr<uint64_t>(c->status), ptr<uint32_t>(c->ticket),
+		               &ptr<DevStats>(c->stats)->err, s);
+		c->launches += 3 * ((32 + bits + 7) / 8);
+	}
+	CC_TRY(check_launch(c));
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	return CC_OK;
+}
+
+cc_status check_scene(cc_ctx *c, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
+                      const float *R, const uint32_t *ID, uint64_t nb, const float *pos, const float *rot) {
+	if (n == 0) return CC_OK;
+	if (!T || !A || !B || !C || !R || !ID || !pos || !rot || nb == 0)
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "null shape/body array with n = %llu", (unsigned long long)n);
+	if (!aligned16(R) || !aligned16(rot))
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "real4 arrays (R, body_rot) must be 16-byte aligned");
+	return CC_OK;
+}
+
+cc_status check_grid(cc_ctx *c, int gx, int gy, int gz) {
+	if (gx < 0 || gy < 0 || gz < 0) return set_err(c, CC_ERR_INVALID_ARGUMENT, "negative bins per axis");
+	return CC_OK;
+}
+
+cc_status np_run(cc_ctx *c, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
+                 const float *R, const uint32_t *ID, uint64_t nb, const uint8_t *active, const float *pos,
+                 const float *rot,
+                 float envelope, int64_t *pairs, uint64_t P, float *norm, float *cpta, float *cptb, float *depth,
+                 int32_t *bids, uint64_t *n_contacts, cudaStream_t s) {
+	*n_contacts = 0;
+	if (P == 0) return CC_OK;
+	CC_TRY(ensure(c, c->np_norm, 12 * P));
+	CC_TRY(ensure(c, c->np_pa, 12 * P));
+	CC_TRY(ensure(c, c->np_pb, 12 * P));
+	CC_TRY(ensure(c, c->np_depth, 4 * P));
+	CC_TRY(ensure(c, c->np_ids, 8 * P));
+	CC_TRY(ensure(c, c->np_pairs, 8 * P));
+	CC_TRY(ensure(c, c->np_flag, 4 * P));
+	CC_TRY(ensure(c, c->np_pos, 8 * (P + 1)));
+	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
+	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(P + 1)));
+	CC_TRY(ensure(c, c->ticket, 64));
+	NpScratch sc;
+	sc.norm = ptr<float>(c->np_norm);
+	sc.pa = ptr<float>(c->np_pa);
+	sc.pb = ptr<float>(c->np_pb);
+	sc.depth = ptr<float>(c->np_depth);
+	sc.ids = ptr<int32_t>(c->np_ids);
+	sc.pairs = ptr<unsigned long long>(c->np_pairs);
+	sc.flag = ptr<uint32_t>(c->np_flag);
+	sc.pos = ptr<unsigned long long>(c->np_pos);
+	sc.status = ptr<uint64_t>(c->status);
+	sc.ticket = ptr<uint32_t>(c->ticket);
+	sc.err = &ptr<DevStats>(c->stats)->err;
+	CC_CUDA(c, cudaMemsetAsync(sc.err, 0, sizeof(uint32_t), s));
+	{
+		StageMark m(c, ST_MPR, s);
+		launch_mpr(P, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, reinterpret_cast<const long long *>(pairs),
+		           sc, s);
+	}
+	{
+		StageMark m(c, ST_NP_COMPACT, s);
+		launch_np_compact(P, sc, reinterpret_cast<long long *>(pairs), norm, cpta, cptb, depth, bids, s);
+	}
+	c->launches += 3;
+	CC_TRY(check_launch(c));
+	CC_CUDA(c, cudaMemcpyAsync(c->h_word, sc.pos + P, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->h_word + 1, sc.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	if ((uint32_t)c->h_word[1] & kErrBadIndex)
+		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is >= nb");
+	if ((uint32_t)c->h_word[1] & kErrSpinLimit) return set_err(c, CC_ERR_INTERNAL, "device-side look-back wait gave up");
+	*n_contacts = c->h_word[0];
+	return CC_OK;
+}
+
+// Shared body of cc_collide / cc_collide_host on device pointers.
+cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
+                      int64_t *pairs, uint64_t pairs_cap, float *norm, float *cpta, float *cptb, float *depth,
+                      int32_t *bids, uint64_t *n_pairs, uint64_t *n_contacts, cudaStream_t s) {
+	*n_pairs = 0;
+	*n_contacts = 0;
+	c->retained = false;
+	const uint64_t n = sc.n;
+	if (n == 0) return CC_OK;
+	CC_TRY(bp_prepare(c, n));
+	{
+		StageMark m(c, ST_AABB, s);
+		CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
+		launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb,
+		            ptr<DevStats>(c->stats), &ptr<DevStats>(c->stats)->err, s);
+	}
+	c->launches += 1;
+	const int grid[3] = {gx, gy, gz};
+	uint64_t P = 0;
+	CC_TRY(bp_core(c, n, aabb, grid, s, &P));
+	*n_pairs = P;
+	if (P > pairs_cap) {
+		c->retained = true;
+		c->retained_n = n;
+		c->retained_P = P;
+		return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries, capacity %llu", (unsigned long long)P,
+		               (unsigned long long)pairs_cap);
+	}
+	CC_TRY(bp_emit(c, n, P, reinterpret_cast<unsigned long long *>(pairs), s));
+	return np_run(c, n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.active, sc.body_pos, sc.body_rot, envelope,
+	              pairs, P, norm, cpta, cptb, depth, bids, n_contacts, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+cc_status cc_ctx_create(cc_ctx **out, int device) {
+	if (!out) return CC_ERR_INVALID_ARGUMENT;
+	*out = nullptr;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return CC_ERR_CUDA;
+	cc_ctx *c = new cc_ctx();
+	c->device = device;
+	c->gp.k_target = 4.0f;
+	c->gp.min_ratio = 2.0f;
+	c->gp.user_dim[0] = c->gp.user_dim[1] = c->gp.user_dim[2] = 0;
+	if (cudaSetDevice(device) != cudaSuccess || cudaMallocHost(&c->h_stats, sizeof(DevStats)) != cudaSuccess ||
+	    cudaMallocHost(&c->h_word, 64) != cudaSuccess) {
+		delete c;
+		return CC_ERR_CUDA;
+	}
+	*out = c;
+	return CC_OK;
+}
+
+void cc_ctx_destroy(cc_ctx *c) {
+	if (!c) return;
+	cudaSetDevice(c->device);
+	Buf *bufs[] = {&c->stats,    &c->cell_count, &c->cell_start, &c->entries,  &c->owner_count, &c->owner_off,
+	               &c->pairs_tmp, &c->status,    &c->ticket,     &c->big_list, &c->ref_cnt,     &c->ref_off,
+	               &c->ref_keys, &c->ref_tmp,    &c->ref_flags,  &c->ref_runpos, &c->rx_hist,   &c->rx_hoff,
+	               &c->np_norm,  &c->np_pa,      &c->np_pb,      &c->np_depth, &c->np_ids,      &c->np_pairs,
+	               &c->np_flag,  &c->np_pos,     &c->in_T,       &c->in_A,     &c->in_B,        &c->in_C,
+	               &c->in_R,     &c->in_ID,      &c->in_pos,     &c->in_rot,   &c->in_act,      &c->out_aabb,
+	               &c->out_pairs, &c->out_norm,  &c->out_pa,     &c->out_pb,   &c->out_depth,   &c->out_bids};
+	for (Buf *b : bufs)
+		if (b->p) cudaFree(b->p);
+	if (c->h_stats) cudaFreeHost(c->h_stats);
+	if (c->h_word) cudaFreeHost(c->h_word);
+	for (int i = 0; i < 2 * kMaxMarks; i++)
+		if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+	delete c;
+}
+
+const char *cc_status_string(cc_status s) {
+	switch (s) {
+	case CC_OK: return "ok";
+	case CC_ERR_INVALID_ARGUMENT: return "invalid argument";
+	case CC_ERR_INVALID_INPUT: return "invalid input (non-finite or inverted AABB)";
+	case CC_ERR_CAPACITY: return "output capacity too small";
+	case CC_ERR_CUDA: return "CUDA error";
+	case CC_ERR_OUT_OF_MEMORY: return "out of device memory";
+	case CC_ERR_INTERNAL: return "internal error (device wait limit)";
+	case CC_ERR_NO_RESULT: return "no retained result";
+	}
+	return "unknown status";
+}
+
+const char *cc_last_error(const cc_ctx *c) { return c ? c->err.c_str() : ""; }
+const char *cc_version(void) { return "collide_b200 0.1 (sm_100a)"; }
+
+cc_status cc_set_search_grid(cc_ctx *c, int gx, int gy, int gz) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	if (gx < 0 || gy < 0 || gz < 0 || gx > kMaxDim || gy > kMaxDim || gz > kMaxDim)
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "search grid dims must be in [0, %d]", kMaxDim);
+	const bool pin = gx > 0 && gy > 0 && gz > 0;
+	c->gp.user_dim[0] = pin ? gx : 0;
+	c->gp.user_dim[1] = pin ? gy : 0;
+	c->gp.user_dim[2] = pin ? gz : 0;
+	return CC_OK;
+}
+
+cc_status cc_set_tuning(cc_ctx *c, float cell_target, float min_ratio) {
+	if (!c || !(cell_target > 0.f) || !(min_ratio >= 0.f)) return CC_ERR_INVALID_ARGUMENT;
+	c->gp.k_target = cell_target;
+	c->gp.min_ratio = min_ratio;
+	return CC_OK;
+}
+
+cc_status cc_get_last_grid(const cc_ctx *c, int *dims3, uint64_t *entries) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	if (dims3)
+		for (int d = 0; d < 3; d++) dims3[d] = c->last_dim[d];
+	if (entries) *entries = c->last_E;
+	return CC_OK;
+}
+
+uint64_t cc_last_launch_count(const cc_ctx *c) { return c ? c->launches : 0; }
+
+cc_status cc_set_profiling(cc_ctx *c, int on) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	if (on && !c->ev[0]) {
+		CC_CUDA(c, cudaSetDevice(c->device));
+		for (int i = 0; i < 2 * kMaxMarks; i++) CC_CUDA(c, cudaEventCreate(&c->ev[i]));
+	}
+	c->prof = on != 0;
+	return CC_OK;
+}
+
+int cc_stage_count(void) { return ST_COUNT_; }
+
+const char *cc_stage_name(int st) { return (st >= 0 && st < ST_COUNT_) ? kStageNames[st] : ""; }
+
+cc_status cc_stage_times(const cc_ctx *c, double *ms, uint64_t *launches, int cap) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	for (int i = 0; i < cap && i < ST_COUNT_; i++) {
+		if (ms) ms[i] = c->stage_ms[i];
+		if (launches) launches[i] = c->stage_n[i];
+	}
+	return CC_OK;
+}
+
+cc_status cc_reset_stage_times(cc_ctx *c) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	for (int i = 0; i < ST_COUNT_; i++) {
+		c->stage_ms[i] = 0.0;
+		c->stage_n[i] = 0;
+	}
+	return CC_OK;
+}
+
+cc_status cc_generate_aabb(cc_ctx *c, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
+                           const float *R, const uint32_t *ID, uint64_t nb, const float *pos, const float *rot,
+                           float *aabb, void *stream) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	CC_TRY(check_scene(c, n, T, A, B, C, R, ID, nb, pos, rot));
+	if (n && !aabb) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	cudaStream_t s = (cudaStream_t)stream;
+	if (n == 0) return CC_OK;
+	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
+	uint32_t *err = &ptr<DevStats>(c->stats)->err;
+	{
+		StageMark m(c, ST_AABB, s);
+		CC_CUDA(c, cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
+		launch_aabb(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, s);
+	}
+	c->launches += 1;
+	CC_TRY(check_launch(c));
+	CC_CUDA(c, cudaMemcpyAsync(c->h_word, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	if ((uint32_t)c->h_word[0] & kErrBadIndex) return set_err(c, CC_ERR_INVALID_INPUT, "a body id is >= nb");
+	return CC_OK;
+}
+
+cc_status cc_broadphase(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy, int gz, int64_t *pairs,
+                        uint64_t pairs_cap, uint64_t *n_pairs, void *stream) {
+	if (!c || !n_pairs) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	*n_pairs = 0;
+	c->retained = false;
+	CC_TRY(check_grid(c, gx, gy, gz));
+	if (n == 0) return CC_OK;
+	if (!aabb) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	cudaStream_t s = (cudaStream_t)stream;
+	CC_TRY(bp_prepare(c, n));
+	{
+		StageMark m(c, ST_BOUNDS, s);
+		CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
+		launch_bounds(n, aabb, ptr<DevStats>(c->stats), s);
+	}
+	c->launches += 1;
+	const int grid[3] = {gx, gy, gz};
+	uint64_t P = 0;
+	CC_TRY(bp_core(c, n, aabb, grid, s, &P));
+	*n_pairs = P;
+	if (!pairs || P > pairs_cap) {
+		c->retained = true;
+		c->retained_n = n;
+		c->retained_P = P;
+		if (P == 0) return CC_OK;
+		return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries, capacity %llu", (unsigned long long)P,
+		               (unsigned long long)pairs_cap);
+	}
+	return bp_emit(c, n, P, reinterpret_cast<unsigned long long *>(pairs), s);
+}
+
+cc_status cc_broadphase_fetch(cc_ctx *c, int64_t *pairs, uint64_t pairs_cap, void *stream) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	if (!c->retained) return set_err(c, CC_ERR_NO_RESULT, "no retained pair list");
+	if (c->retained_P > pairs_cap || (!pairs && c->retained_P))
+		return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries", (unsigned long long)c->retained_P);
+	CC_CUDA(c, cudaSetDevice(c->device));
+	c->retained = false;
+	return bp_emit(c, c->retained_n, c->retained_P, reinterpret_cast<unsigned long long *>(pairs),
+	               (cudaStream_t)stream);
+}
+
+cc_status cc_broadphase_bins(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy, int gz, uint32_t *bin_number,
+                             uint32_t *body_number, uint64_t entries_cap, uint64_t *n_entries, uint32_t *active_bins,
+                             uint32_t *bin_end, uint64_t active_cap, uint64_t *n_active, void *stream) {
+	if (!c || !n_entries || !n_active) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	*n_entries = 0;
+	*n_active = 0;
+	c->retained = false;
+	CC_TRY(check_grid(c, gx, gy, gz));
+	if (n == 0) return CC_OK;
+	if (!aabb) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	cudaStream_t s = (cudaStream_t)stream;
+	CC_TRY(bp_prepare(c, n));
+	StageMark bins_mark(c, ST_BINS, s);
+	BpBuffers b = bp_buffers(c);
+	CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
+	launch_bounds(n, aabb, b.stats, s);
+	CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * c->gp.g_max, s));
+	const int grid[3] = {gx, gy, gz};
+	launch_count(n, aabb, c->gp, grid, b, s);  // plan + in-place shift
+	// per-body bin counts -> offsets
+	CC_TRY(ensure(c, c->ref_cnt, sizeof(uint32_t) * n));
+	CC_TRY(ensure(c, c->ref_off, sizeof(unsigned long long) * (n + 1)));
+	launch_ref_count(n, aabb, b.stats, ptr<uint32_t>(c->ref_cnt), s);
+	launch_scan_u32_to_u64(ptr<uint32_t>(c->ref_cnt), n, ptr<unsigned long long>(c->ref_off), b.status, b.ticket,
+	                       &b.stats->err, s);
+	c->launches += 5;
+	CC_TRY(check_launch(c));
+	CC_CUDA(c, cudaMemcpyAsync(c->h_word, ptr<unsigned long long>(c->ref_off) + n, 8, cudaMemcpyDeviceToHost, s));
+	CC_TRY(read_stats(c, s));
+	CC_TRY(device_err(c));
+	const uint64_t E = c->h_word[0];
+	*n_entries = E;
+	// emit (bin << 32 | body) body-major, stable sort on the bin half
+	CC_TRY(ensure(c, c->ref_keys, sizeof(unsigned long long) * std::max<uint64_t>(E, 1)));
+	CC_TRY(ensure(c, c->ref_tmp, sizeof(unsigned long long) * std::max<uint64_t>(E, 1)));
+	launch_ref_emit(n, aabb, b.stats, ptr<unsigned long long>(c->ref_off), ptr<unsigned long long>(c->ref_keys), E, s);
+	c->launches += 1;
+	CC_TRY(read_stats(c, s));
+	if (c->h_stats->err & kErrBinCount) return set_err(c, CC_ERR_INTERNAL, "bin count/emit mismatch");
+	int bits = 0;
+	while (bits < 32 && ((uint64_t)c->h_stats->max_bin >> bits) != 0) bits++;
+	unsigned long long *keys = ptr<unsigned long long>(c->ref_keys);
+	// size all remaining scratch first: nothing may be reallocated while
+	// kernels that use it are in flight
+	const size_t hw = radix_hist_words(E);
+	CC_TRY(ensure(c, c->rx_hist, sizeof(uint32_t) * hw));
+	CC_TRY(ensure(c, c->rx_hoff, sizeof(unsigned long long) * (hw + 1)));
+	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(std::max<uint64_t>(hw, E) + 1)));
+	CC_TRY(ensure(c, c->ref_flags, sizeof(uint32_t) * std::max<uint64_t>(E, 1)));
+	CC_TRY(ensure(c, c->ref_runpos, sizeof(uint32_t) * (E + 1)));
+	b = bp_buffers(c);
+	if (E > 1 && bits > 0) {
+		radix_sort_u64(keys, ptr<unsigned long long>(c->ref_tmp), E, 32, 32 + bits, ptr<uint32_t>(c->rx_hist),
+		               ptr<unsigned long long>(c->rx_hoff), b.status, b.ticket, &b.stats->err, s);
+		c->launches += 3 * ((bits + 7) / 8);
+	}
+	// runs of equal bins
+	launch_ref_flags(keys, E, ptr<uint32_t>(c->ref_flags), s);
+	launch_scan_u32_to_u32(ptr<uint32_t>(c->ref_flags), E, ptr<uint32_t>(c->ref_runpos), b.status, b.ticket,
+	                       &b.stats->err, s);
+	c->launches += 2;
+	CC_TRY(check_launch(c));
+	CC_CUDA(c, cudaMemcpyAsync(c->h_word, ptr<uint32_t>(c->ref_runpos) + E, 4, cudaMemcpyDeviceToHost, s));
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	const uint64_t A = (uint32_t)c->h_word[0];
+	*n_active = A;
+	if ((bin_number || body_number) && E > entries_cap)
+		return set_err(c, CC_ERR_CAPACITY, "bin list needs %llu entries", (unsigned long long)E);
+	if ((active_bins || bin_end) && A > active_cap)
+		return set_err(c, CC_ERR_CAPACITY, "active-bin list needs %llu entries", (unsigned long long)A);
+	launch_ref_split(keys, E, ptr<uint32_t>(c->ref_runpos), bin_number, body_number, active_bins, bin_end, A, s);
+	c->launches += 1;
+	CC_TRY(check_launch(c));
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	return CC_OK;
+}
+
+cc_status cc_narrowphase(cc_ctx *c, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
+                         const float *R, const uint32_t *ID, uint64_t nb, const uint8_t *active, const float *pos,
+                         const float *rot, float envelope, int64_t *pairs, uint64_t n_pairs, float *norm, float *cpta,
+                         float *cptb, float *depth, int32_t *bids, uint64_t *n_contacts, void *stream) {
+	if (!c || !n_contacts) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	*n_contacts = 0;
+	CC_TRY(check_scene(c, n, T, A, B, C, R, ID, nb, pos, rot));
+	if (n_pairs && (!pairs || !norm || !cpta || !cptb || !depth || !bids || !active))
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "null pair/contact/active array");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	return np_run(c, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, n_pairs, norm, cpta, cptb, depth,
+	              bids, n_contacts, (cudaStream_t)stream);
+}
+
+cc_status cc_collide(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz, float envelope, cc_result *res,
+                     void *stream) {
+	if (!c || !sc || !res) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	CC_TRY(check_grid(c, gx, gy, gz));
+	CC_TRY(check_scene(c, sc->n, sc->T, sc->A, sc->B, sc->C, sc->R, sc->ID, sc->nb, sc->body_pos, sc->body_rot));
+	if (sc->n && (!res->aabb || !sc->active))
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb or active array");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	return collide_dev(c, *sc, gx, gy, gz, envelope, res->aabb, res->pairs, res->pairs_cap, res->norm, res->cpta,
+	                   res->cptb, res->depth, res->bids, &res->n_pairs, &res->n_contacts, (cudaStream_t)stream);
+}
+
+cc_status cc_collide_host(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz, float envelope, cc_result *res,
+                          void *stream) {
+	if (!c || !sc || !res) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	CC_TRY(check_grid(c, gx, gy, gz));
+	CC_TRY(check_scene(c, sc->n, sc->T, sc->A, sc->B, sc->C, sc->R, sc->ID, sc->nb, sc->body_pos, sc->body_rot));
+	if (sc->n && !sc->active) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null active array");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	cudaStream_t s = (cudaStream_t)stream;
+	const uint64_t n = sc->n, nb = sc->nb;
+	res->n_pairs = res->n_contacts = 0;
+	if (n == 0) return CC_OK;
+	CC_TRY(ensure(c, c->in_T, 4 * n));
+	CC_TRY(ensure(c, c->in_A, 12 * n));
+	CC_TRY(ensure(c, c->in_B, 12 * n));
+	CC_TRY(ensure(c, c->in_C, 12 * n));
+	CC_TRY(ensure(c, c->in_R, 16 * n));
+	CC_TRY(ensure(c, c->in_ID, 4 * n));
+	CC_TRY(ensure(c, c->in_pos, 12 * nb));
+	CC_TRY(ensure(c, c->in_rot, 16 * nb));
+	CC_TRY(ensure(c, c->in_act, nb));
+	CC_TRY(ensure(c, c->out_aabb, 24 * n));
+	const uint64_t cap = res->pairs_cap;
+	CC_TRY(ensure(c, c->out_pairs, 8 * std::max<uint64_t>(cap, 1)));
+	CC_TRY(ensure(c, c->out_norm, 12 * std::max<uint64_t>(cap, 1)));
+	CC_TRY(ensure(c, c->out_pa, 12 * std::max<uint64_t>(cap, 1)));
+	CC_TRY(ensure(c, c->out_pb, 12 * std::max<uint64_t>(cap, 1)));
+	CC_TRY(ensure(c, c->out_depth, 4 * std::max<uint64_t>(cap, 1)));
+	CC_TRY(ensure(c, c->out_bids, 8 * std::max<uint64_t>(cap, 1)));
+	std::unique_ptr<StageMark> cin(new StageMark(c, ST_COPY_IN, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_T.p, sc->T, 4 * n, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_A.p, sc->A, 12 * n, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_B.p, sc->B, 12 * n, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_C.p, sc->C, 12 * n, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_R.p, sc->R, 16 * n, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_ID.p, sc->ID, 4 * n, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_pos.p, sc->body_pos, 12 * nb, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_rot.p, sc->body_rot, 16 * nb, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(c->in_act.p, sc->active, nb, cudaMemcpyHostToDevice, s));
+	if (res->aabb) CC_CUDA(c, cudaMemcpyAsync(c->out_aabb.p, res->aabb, 24 * n, cudaMemcpyHostToDevice, s));
+	cin.reset();
+	cc_scene d;
+	d.n = n;
+	d.nb = nb;
+	d.T = ptr<int32_t>(c->in_T);
+	d.A = ptr<float>(c->in_A);
+	d.B = ptr<float>(c->in_B);
+	d.C = ptr<float>(c->in_C);
+	d.R = ptr<float>(c->in_R);
+	d.ID = ptr<uint32_t>(c->in_ID);
+	d.body_pos = ptr<float>(c->in_pos);
+	d.body_rot = ptr<float>(c->in_rot);
+	d.active = ptr<uint8_t>(c->in_act);
+	uint64_t P = 0, nc = 0;
+	cc_status st = collide_dev(c, d, gx, gy, gz, envelope, ptr<float>(c->out_aabb), ptr<int64_t>(c->out_pairs), cap,
+	                           ptr<float>(c->out_norm), ptr<float>(c->out_pa), ptr<float>(c->out_pb),
+	                           ptr<float>(c->out_depth), ptr<int32_t>(c->out_bids), &P, &nc, s);
+	res->n_pairs = P;
+	res->n_contacts = nc;
+	if (st != CC_OK) return st;
+	StageMark cout_mark(c, ST_COPY_OUT, s);
+	if (res->aabb) CC_CUDA(c, cudaMemcpyAsync(res->aabb, c->out_aabb.p, 24 * n, cudaMemcpyDeviceToHost, s));
+	if (res->pairs && P) CC_CUDA(c, cudaMemcpyAsync(res->pairs, c->out_pairs.p, 8 * P, cudaMemcpyDeviceToHost, s));
+	if (nc) {
+		if (res->norm) CC_CUDA(c, cudaMemcpyAsync(res->norm, c->out_norm.p, 12 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->cpta) CC_CUDA(c, cudaMemcpyAsync(res->cpta, c->out_pa.p, 12 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->cptb) CC_CUDA(c, cudaMemcpyAsync(res->cptb, c->out_pb.p, 12 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->depth) CC_CUDA(c, cudaMemcpyAsync(res->depth, c->out_depth.p, 4 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->bids) CC_CUDA(c, cudaMemcpyAsync(res->bids, c->out_bids.p, 8 * nc, cudaMemcpyDeviceToHost, s));
+	}
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	return CC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+// Shared device utilities for the collision kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cc {
+
+constexpr int kWarp = 32;
+constexpr int kNumSMs = 148;  // B200: 2 dies x 74 SMs; grids are sized in multiples of it
+
+// Device-side error bits, OR-ed into Workspace::err (read by the host after a
+// call). A set bit makes the C ABI return an error status; it never traps.
+enum DeviceError : uint32_t {
+	kErrNonFinite = 1u << 0,     // NaN/Inf in an AABB corner
+	kErrInverted = 1u << 1,      // min > max on some axis
+	kErrSpinLimit = 1u << 2,     // a bounded wait gave up (look-back scan)
+	kErrCapacity = 1u << 3,      // an output buffer was too small (sizes still reported)
+	kErrSegmentTooLong = 1u << 4,  // a pair segment exceeded the block sort size (host falls back)
+	kErrBinCount = 1u << 5,      // a body covers a negative / overflowing number of reference bins
+	kErrBadIndex = 1u << 6,      // a body id >= nb or a pair index >= n (the access is skipped)
+};
+
+// Order-preserving map float -> uint32 (for atomicMin/atomicMax reductions).
+__device__ __forceinline__ uint32_t f2ord(float f) {
+	uint32_t u = __float_as_uint(f);
+	return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t k) {
+	uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+	return __uint_as_float(u);
+}
+__host__ __device__ inline float ord2f_host(uint32_t k) {
+	uint32_t u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+	float f;
+	memcpy(&f, &u, 4);
+	return f;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+template <class T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		T t = __shfl_up_sync(0xffffffffu, v, o);
+		if ((int)lane_id() >= o) v += t;
+	}
+	return v;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+// Block-wide exclusive scan of one value per thread. `sm` holds >= 32 T.
+// Returns the exclusive prefix; *total receives the block sum.
+template <class T, int NT>
+__device__ __forceinline__ T block_excl_scan(T v, T *sm, T *total) {
+	constexpr int NW = NT / 32;
+	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+	T inc = warp_incl_scan(v);
+	if (l == 31) sm[w] = inc;
+	__syncthreads();
+	if (w == 0) {
+		T s = (l < NW) ? sm[l] : T(0);
+		T si = warp_incl_scan(s);
+		if (l < NW) sm[l] = si - s;
+		if (l == NW - 1) sm[NW] = si;
+	}
+	__syncthreads();
+	T r = sm[w] + inc - v;
+	*total = sm[NW];
+	__syncthreads();
+	return r;
+}
+
+// ---------------------------------------------------------------------------
+// Decoupled look-back (single pass) for 64-bit sums.
+//
+// Tile status word: bits 63..62 = state (0 empty, 1 aggregate, 2 prefix),
+// bits 61..0 = value. The status array must be zeroed before the launch.
+// Tiles take indices from an atomic ticket, so every predecessor a tile waits
+// on has already started; each wait is still bounded and sets kErrSpinLimit
+// (treating the missing value as 0) instead of spinning forever.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kStAgg = 1ull << 62, kStPre = 2ull << 62, kStMask = (1ull << 62) - 1;
+constexpr int kSpinLimit = 1 << 22;
+
+__device__ __forceinline__ void st_publish(uint64_t *status, uint32_t tile, uint64_t state, uint64_t v) {
+	__stcg((unsigned long long *)(status + tile), (unsigned long long)(state | (v & kStMask)));
+}
+
+// Called by warp 0 of a tile with the tile aggregate; returns the exclusive
+// prefix of the tile (valid in all lanes of warp 0).
+__device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint32_t tile, uint64_t agg, uint32_t *err) {
+	const int l = lane_id();
+	if (tile == 0) {
+		if (l == 0) st_publish(status, 0, kStPre, agg);
+		return 0;
+	}
+	if (l == 0) st_publish(status, tile, kStAgg, agg);
+	uint64_t excl = 0;
+	int64_t base = (int64_t)tile - 1;
+	int spins = 0;
+	while (true) {
+		int64_t idx = base - l;
+		uint64_t s = 0;
+		if (idx >= 0) {
+			s = __ldcg((const unsigned long long *)(status + idx));
+		} else {
+			s = kStPre;  // virtual tile before 0 has prefix 0
+		}
+		uint32_t pre = __ballot_sync(0xffffffffu, (s >> 62) == 2);
+		uint32_t empty = __ballot_sync(0xffffffffu, (s >> 62) == 0);
+		// lanes up to and including the first prefix lane contribute
+		int stop = pre ? (__ffs(pre) - 1) : 31;
+		uint32_t need = (stop == 31) ? 0xffffffffu : ((1u << (stop + 1)) - 1u);
+		if (empty & need) {
+			if (++spins > kSpinLimit) {
+				if (l == 0) atomicOr(err, (uint32_t)kErrSpinLimit);
+				break;
+			}
+			__nanosleep(32);
+			continue;
+		}
+		uint64_t v = (l <= stop) ? (s & kStMask) : 0;
+		excl += warp_sum(v);
+		if (pre) break;
+		base -= 32;
+	}
+	if (l == 0) st_publish(status, tile, kStPre, excl + agg);
+	return excl;
+}
+
+}  // namespace cc

@@ -1,0 +1,140 @@
+// Internal interfaces between the translation units of libcollide_b200.so.
+// Host code only sees launchers (each .cu file owns its kernels); nothing here
+// is part of the public C ABI (include/collide_b200.h).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cc {
+
+// Uniform search grid of the pair test (chosen on the device from the bounds,
+// see make_plan in cc_broadphase.cu). Any monotone cell map finds the same
+// pairs, so this grid is free to differ from the caller's bins-per-axis.
+struct Plan {
+	float lo[3];      // shifted minimum corner of the scene
+	float inv[3];     // cells per unit length per axis
+	int dim[3];       // cells per axis (1..kMaxDim)
+	uint32_t G;       // dim[0] * dim[1] * dim[2]
+	float origin[3];  // reference shift: fabs(min) (Broadphase.cu:379)
+	float invbin[3];  // reference inverse bin size: grid / fabs(max + fabs(min)) (:380-381)
+	int grid[3];      // reference bins per axis
+	int valid;        // bounds were finite and every box had min <= max
+};
+
+// Per-call device state; zeroed (one memset) at the start of every call.
+struct DevStats {
+	uint32_t bmin_inv[3];  // ~f2ord(min) accumulated with atomicMax (0 = neutral)
+	uint32_t bmax[3];      // f2ord(max) accumulated with atomicMax (0 = neutral)
+	uint32_t err;          // DeviceError bits
+	uint32_t max_bin;      // largest reference bin id emitted (bin-list path)
+	double ext_sum[3];     // sum of AABB extents per axis (tuner input)
+	unsigned long long pairs;     // unique pairs emitted by the tile test (may exceed capacity)
+	unsigned long long entries;   // (cell, body) entries of the search grid
+	unsigned long long ref_entries;
+	unsigned long long contacts;
+	unsigned long long big_segments;
+	unsigned long long max_segment;
+	Plan plan;
+};
+
+constexpr int kMaxDim = 1024;  // cells per axis (10-bit packed cell coordinates)
+
+// Tuner parameters of the search grid.
+struct GridParams {
+	float k_target;   // target mean entries per cell
+	float min_ratio;  // minimum cell edge as a multiple of the mean box extent
+	int user_dim[3];  // > 0: search on exactly this grid (tuner bypassed)
+	uint32_t g_max;   // capacity of the per-cell arrays
+};
+
+// ------------------------------------------------------------------ scan
+// Exclusive scan of `n` uint32 counts into uint64 offsets out[0..n] (out[n] =
+// total) with one decoupled look-back pass. status: >= scan_tiles(n) words.
+size_t scan_tiles(uint64_t n);
+void launch_scan_u32_to_u64(const uint32_t *in, uint64_t n, unsigned long long *out, uint64_t *status,
+                            uint32_t *ticket, uint32_t *err, cudaStream_t s);
+// Same, 32-bit output (caller guarantees total < 2^32). With n_dev the count
+// is min(n, *n_dev), read on the device; total_out (optional) receives the sum.
+void launch_scan_u32_to_u32(const uint32_t *in, uint64_t n, uint32_t *out, uint64_t *status, uint32_t *ticket,
+                            uint32_t *err, cudaStream_t s, const uint32_t *n_dev = nullptr,
+                            unsigned long long *total_out = nullptr);
+
+// ------------------------------------------------------------------ radix sort
+// Stable LSD radix sort of 64-bit keys on bits [bit_lo, bit_hi). `keys` and
+// `tmp` are n-element buffers; the result ends in `keys`. `hist` needs
+// radix_hist_words(n) words, `status` scan_tiles(radix_hist_words(n)) words.
+size_t radix_hist_words(uint64_t n);
+void radix_sort_u64(unsigned long long *keys, unsigned long long *tmp, uint64_t n, int bit_lo, int bit_hi,
+                    uint32_t *hist, unsigned long long *hoff, uint64_t *status, uint32_t *ticket, uint32_t *err,
+                    cudaStream_t s);
+
+// ------------------------------------------------------------------ AABB
+// GenerateAABB. With `stats` non-null the kernel also accumulates the scene
+// bounds, extent sums and validity (the broadphase's first pass).
+// Body ids >= nb set kErrBadIndex in *err and leave that shape's AABB unwritten.
+void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
+                 const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
+                 uint32_t *err, cudaStream_t s);
+
+// ------------------------------------------------------------------ broadphase
+struct BpBuffers {
+	DevStats *stats;
+	uint32_t *cell_count;    // g_max
+	uint32_t *cell_start;    // g_max + 1
+	uint32_t g_max;
+	float4 *entries;         // entry_cap * 2 (lo+id, hi+packed cell)
+	uint64_t entry_cap;
+	uint32_t *owner_count;   // n
+	unsigned long long *owner_off;  // n + 1
+	unsigned long long *pairs_tmp;  // pair_cap
+	uint64_t pair_cap;
+	uint64_t *status;        // look-back tiles
+	uint32_t *ticket;        // 4 counters
+	uint32_t *big_list;      // big segment owners
+	uint64_t big_cap;
+};
+
+void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, cudaStream_t s);
+void launch_count(uint64_t n, float *aabb, const GridParams &gp, const int grid[3], const BpBuffers &b,
+                  cudaStream_t s);
+void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
+void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
+void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
+void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
+void launch_owner_scatter(uint64_t P, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+void launch_segsort_big(uint64_t nbig, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+
+// Reference-grid bin list (the reference's internal sorted (bin, body) list).
+void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s);
+void launch_ref_emit(uint64_t n, const float *aabb_shifted, DevStats *stats, const unsigned long long *off,
+                     unsigned long long *keys, uint64_t cap, cudaStream_t s);
+// Run boundaries of the sorted keys: flags[e] = 1 where a new bin starts.
+void launch_ref_flags(const unsigned long long *keys, uint64_t E, uint32_t *flags, cudaStream_t s);
+void launch_ref_split(const unsigned long long *keys, uint64_t E, const uint32_t *run_pos, uint32_t *bin_number,
+                      uint32_t *body_number, uint32_t *active_bins, uint32_t *bin_end, uint64_t cap_a,
+                      cudaStream_t s);
+
+// ------------------------------------------------------------------ narrowphase
+struct NpScratch {
+	float *norm, *pa, *pb;  // 3 * P each
+	float *depth;           // P
+	int32_t *ids;           // 2 * P
+	unsigned long long *pairs;  // P (copy of the input keys)
+	uint32_t *flag;         // P
+	unsigned long long *pos;  // P + 1
+	uint64_t *status;       // look-back tiles of the flag scan
+	uint32_t *ticket;
+	uint32_t *err;
+};
+
+// Pair indices >= n and body ids >= nb set kErrBadIndex in *sc.err; such a
+// pair is reported as no contact.
+void launch_mpr(uint64_t P, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
+                const float *R, const uint32_t *ID, uint64_t nb, const uint8_t *active, const float *pos,
+                const float *rot, float envelope, const long long *pairs, const NpScratch &sc, cudaStream_t s);
+void launch_np_compact(uint64_t P, const NpScratch &sc, long long *pairs, float *norm, float *cpta, float *cptb,
+                       float *depth, int32_t *bids, cudaStream_t s);
+
+}  // namespace cc

@@ -1,0 +1,198 @@
+/*
+ * collide_b200 — C ABI of the B200 (sm_100a) collision pipeline.
+ *
+ * Drop-in for the collision path of uwsbel/collision-detection
+ * ("Chrono::Collide"): AABB generation -> uniform-grid broadphase -> MPR
+ * narrowphase. Each entry point below replaces one public method of the
+ * reference's C++ classes (cited per function, paths relative to the
+ * reference repository). Arguments are plain pointers and sizes; no CUDA or
+ * C++ types appear in the signatures.
+ *
+ * Conventions
+ *  - Array pointers are DEVICE pointers (cudaMalloc / thrust::device_vector
+ *    storage) unless the function name ends in _host.
+ *  - real3 arrays are packed float[3] (12-byte stride, the layout of the
+ *    reference's real3 = float3); real4 arrays are float[4] (w, x, y, z) and
+ *    must be 16-byte aligned (float4).
+ *  - An AABB array holds 2n real3: aabb[i] = min corner, aabb[i + n] = max
+ *    corner (AABBGenerator.cu:114-115).
+ *  - A pair is the int64 key (min_index << 32) | max_index
+ *    (Broadphase.cu:299-308); pair lists are sorted and duplicate-free.
+ *  - `stream` is a cudaStream_t (NULL = the legacy default stream). Calls are
+ *    stream-ordered and return once their results are complete.
+ *  - One cc_ctx must not be used by two host threads at the same time;
+ *    distinct contexts are independent.
+ *  - Every call returns a cc_status. On CC_ERR_CAPACITY the required count is
+ *    stored in the count out-parameter and the result is retained by the
+ *    context (see cc_broadphase_fetch).
+ */
+#ifndef COLLIDE_B200_H
+#define COLLIDE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CC_API __attribute__((visibility("default")))
+#else
+#define CC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cc_ctx cc_ctx;
+
+typedef enum cc_status {
+	CC_OK = 0,
+	CC_ERR_INVALID_ARGUMENT = 1, /* null pointer with n > 0, misaligned real4 array, negative grid */
+	CC_ERR_INVALID_INPUT = 2,    /* an AABB corner is NaN/Inf or has min > max on some axis */
+	CC_ERR_CAPACITY = 3,         /* output too small; the required count is returned */
+	CC_ERR_CUDA = 4,             /* CUDA runtime error (cc_last_error has the text) */
+	CC_ERR_OUT_OF_MEMORY = 5,    /* device allocation failed */
+	CC_ERR_INTERNAL = 6,         /* a bounded device-side wait expired */
+	CC_ERR_NO_RESULT = 7         /* cc_broadphase_fetch without a retained result */
+} cc_status;
+
+/* shape_type of the reference (src/collision_detection.h:57). */
+enum {
+	CC_SPHERE = 0,
+	CC_ELLIPSOID = 1,
+	CC_BOX = 2,
+	CC_CYLINDER = 3,
+	CC_RECT = 4,
+	CC_CONE = 5,
+	CC_TRIANGLEMESH = 6
+};
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Creates a context on CUDA device `device` (the library's scratch memory and
+ * tuning state live here). No reference counterpart: the reference classes
+ * allocate temporaries inside every call (Broadphase.cu:345-349). */
+CC_API cc_status cc_ctx_create(cc_ctx **ctx, int device);
+CC_API void cc_ctx_destroy(cc_ctx *ctx);
+CC_API const char *cc_status_string(cc_status s);
+/* Detail of the last error on this context ("" if none). */
+CC_API const char *cc_last_error(const cc_ctx *ctx);
+CC_API const char *cc_version(void);
+
+/* Search grid of the pair test. The pair list does not depend on it (two
+ * overlapping boxes share a cell of any grid), so by default (0,0,0) the
+ * library picks it from the scene bounds, the body count and the mean box
+ * extent: cells hold about `cell_target` boxes and are at least `min_ratio`
+ * mean box extents wide. (gx,gy,gz) > 0 pins the grid. */
+CC_API cc_status cc_set_search_grid(cc_ctx *ctx, int gx, int gy, int gz);
+CC_API cc_status cc_set_tuning(cc_ctx *ctx, float cell_target, float min_ratio);
+/* The grid the last broadphase searched on, and its entry count. */
+CC_API cc_status cc_get_last_grid(const cc_ctx *ctx, int *dims3, uint64_t *entries);
+
+/* ---- AABBGenerator::GenerateAABB (src/aabb/AABBGenerator.cuh:21-30,
+ *      AABBGenerator.cu:135-188) --------------------------------------------
+ * n shapes: T (shape type), A (local position), B (radius / half extents),
+ * C, R (local rotation, real4), ID (body of each shape); nb bodies: body_pos,
+ * body_rot (real4). Writes aabb[0..2n). Shapes of a type the reference does
+ * not bound (RECT, TRIANGLEMESH; AABBGenerator.cu:110-111) are left untouched;
+ * type 5 (CONE) is bounded as a triangle, as the reference does (:103-107). */
+CC_API cc_status cc_generate_aabb(cc_ctx *ctx, uint64_t n, const int32_t *T, const float *A, const float *B,
+                           const float *C, const float *R, const uint32_t *ID, uint64_t nb, const float *body_pos,
+                           const float *body_rot, float *aabb, void *stream);
+
+/* ---- Broadphase::detectPossibleCollisions (src/broadphase/Broadphase.cuh:17,
+ *      Broadphase.cu:344-545) + setBinsPerAxis (:57-60) + getNumPossibleContacts
+ *      (:66-68) ------------------------------------------------------------
+ * Shifts `aabb` in place by fabs(min corner) exactly as the reference does
+ * (Broadphase.cu:379-386) and writes the sorted unique pair list. (gx,gy,gz)
+ * is the reference's bins per axis; it fixes the bin list
+ * (cc_broadphase_bins) and the shift, not the pairs. *n_pairs receives the
+ * pair count. If pairs_cap < count: returns CC_ERR_CAPACITY, writes nothing,
+ * and keeps the result for one cc_broadphase_fetch. On CC_ERR_INVALID_INPUT
+ * `aabb` is not modified. n == 0 yields 0 pairs (the reference reads
+ * aabb_data[0] there, Broadphase.cu:368). */
+CC_API cc_status cc_broadphase(cc_ctx *ctx, uint64_t n, float *aabb, int gx, int gy, int gz, int64_t *pairs,
+                        uint64_t pairs_cap, uint64_t *n_pairs, void *stream);
+/* Writes the pair list retained by the last cc_broadphase / cc_collide that
+ * returned CC_ERR_CAPACITY (once). */
+CC_API cc_status cc_broadphase_fetch(cc_ctx *ctx, int64_t *pairs, uint64_t pairs_cap, void *stream);
+
+/* The reference's internal sorted bin list (locals of detectPossibleCollisions,
+ * Broadphase.cu:394-480) on grid (gx,gy,gz): bin_number / body_number sorted by
+ * bin, then body (:428-432); active_bins = unique bins and bin_end = inclusive
+ * end offsets (reduce_by_key :439-443 and scan :476-480). Shifts `aabb` in
+ * place like cc_broadphase. Any output may be NULL. Counts are always
+ * returned; CC_ERR_CAPACITY if a non-NULL output is too small. */
+CC_API cc_status cc_broadphase_bins(cc_ctx *ctx, uint64_t n, float *aabb, int gx, int gy, int gz, uint32_t *bin_number,
+                             uint32_t *body_number, uint64_t entries_cap, uint64_t *n_entries, uint32_t *active_bins,
+                             uint32_t *bin_end, uint64_t active_cap, uint64_t *n_active, void *stream);
+
+/* ---- Narrowphase::DoNarrowphase (src/narrowphase/Narrowphase.cuh:19-34,
+ *      Narrowphase.cu:511-595) + SetCollisionEnvelope (:53-55) --------------
+ * Shape and body arrays as in cc_generate_aabb; active[nb] is the body
+ * active flag (bool). For each of the n_pairs candidate keys: sphere-sphere
+ * analytic contact or MPR. Contacts are written in pair order to
+ * norm/cpta/cptb (real3), depth and bids (int32 pairs of body ids); all five
+ * outputs need room for n_pairs entries. `pairs` is permuted in place so its
+ * first *n_contacts keys are the contacts' pairs (Narrowphase.cu:584-588). */
+CC_API cc_status cc_narrowphase(cc_ctx *ctx, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
+                         const float *R, const uint32_t *ID, uint64_t nb, const uint8_t *active, const float *body_pos,
+                         const float *body_rot, float envelope, int64_t *pairs, uint64_t n_pairs, float *norm,
+                         float *cpta, float *cptb, float *depth, int32_t *bids, uint64_t *n_contacts, void *stream);
+
+/* ---- whole pipeline ------------------------------------------------------ */
+
+/* A scene in the reference's shape-array layout. */
+typedef struct cc_scene {
+	uint64_t n;          /* shapes */
+	const int32_t *T;
+	const float *A, *B, *C; /* real3[n] */
+	const float *R;      /* real4[n] */
+	const uint32_t *ID;
+	uint64_t nb;         /* bodies */
+	const float *body_pos; /* real3[nb] */
+	const float *body_rot; /* real4[nb] */
+	const uint8_t *active; /* bool[nb] */
+} cc_scene;
+
+typedef struct cc_result {
+	float *aabb;         /* real3[2n] (shifted, as after detectPossibleCollisions) */
+	int64_t *pairs;      /* pairs_cap keys; contacts' pairs first on return */
+	uint64_t pairs_cap;
+	float *norm, *cpta, *cptb; /* real3[pairs_cap] */
+	float *depth;        /* [pairs_cap] */
+	int32_t *bids;       /* int32[2 * pairs_cap] */
+	uint64_t n_pairs;    /* out */
+	uint64_t n_contacts; /* out */
+} cc_result;
+
+/* GenerateAABB -> detectPossibleCollisions -> DoNarrowphase, the sequence a
+ * Chrono time step runs, with the AABB pass fused into the broadphase's
+ * bounds reduction. Device pointers. */
+CC_API cc_status cc_collide(cc_ctx *ctx, const cc_scene *scene, int gx, int gy, int gz, float envelope, cc_result *res,
+                     void *stream);
+
+/* Same with HOST pointers in `scene` and `res` (pinned memory recommended):
+ * the inputs are copied to context-owned device buffers, the pipeline runs,
+ * and aabb (if non-NULL), pairs and contacts are copied back. */
+CC_API cc_status cc_collide_host(cc_ctx *ctx, const cc_scene *scene, int gx, int gy, int gz, float envelope,
+                          cc_result *res, void *stream);
+
+/* Number of kernels the last call on this context launched. */
+CC_API uint64_t cc_last_launch_count(const cc_ctx *ctx);
+
+/* Stage timing (no reference counterpart). With profiling on, every call
+ * brackets each kernel stage with CUDA events on the caller's stream and
+ * accumulates the device time per stage. cc_stage_times fills up to `cap`
+ * totals in milliseconds and launch counts, indexed by stage id; stage names
+ * come from cc_stage_name. cc_reset_stage_times zeroes the totals. */
+CC_API cc_status cc_set_profiling(cc_ctx *ctx, int on);
+CC_API int cc_stage_count(void);
+CC_API const char *cc_stage_name(int stage);
+CC_API cc_status cc_stage_times(const cc_ctx *ctx, double *ms, uint64_t *launches, int cap);
+CC_API cc_status cc_reset_stage_times(cc_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
