@@ -59,6 +59,7 @@ SIGNATURES = {
     "cc_stage_name": (ctypes.c_char_p, [I32]),
     "cc_stage_times": (I32, [P, ctypes.POINTER(ctypes.c_double), PU64, I32]),
     "cc_reset_stage_times": (I32, [P]),
+    "cc_broadphase_noalloc": (I32, [U64, P, I32, I32, I32, P, U64, PU64, P]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

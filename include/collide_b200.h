@@ -191,6 +191,29 @@ CC_API const char *cc_stage_name(int stage);
 CC_API cc_status cc_stage_times(const cc_ctx *ctx, double *ms, uint64_t *launches, int cap);
 CC_API cc_status cc_reset_stage_times(cc_ctx *ctx);
 
+/* ---- broadphase without allocation ---------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that may
+ * not allocate device memory — code running under CUDA stream capture (where
+ * cudaMalloc is an error), real-time step loops (cudaMalloc/cudaFree can
+ * synchronize the device and take unbounded time) and frameworks that own all
+ * device memory through their own pool. Same contract as cc_broadphase (shifts
+ * `aabb` in place, writes the sorted unique pair list, *n_pairs = count), but
+ * it needs no context and allocates nothing: its scratch is one fixed
+ * CC_NOALLOC_SCRATCH_BYTES device array that every GPU loading the library
+ * holds until exit. Limits: n <= CC_NOALLOC_MAX_BODIES, search-grid entries <=
+ * CC_NOALLOC_MAX_ENTRIES, pairs <= CC_NOALLOC_MAX_PAIRS; beyond them it returns
+ * CC_ERR_CAPACITY (with *n_pairs set once the count is known). pairs_cap below
+ * the count also returns CC_ERR_CAPACITY; nothing is retained. The first call
+ * on each device sets up the scratch address and should come before any stream
+ * capture. All calls share the one scratch array: calls that overlap on the
+ * GPU, or from two host threads at once, race. */
+#define CC_NOALLOC_MAX_BODIES 65536u
+#define CC_NOALLOC_MAX_ENTRIES (4u * CC_NOALLOC_MAX_BODIES)
+#define CC_NOALLOC_MAX_PAIRS (4u * CC_NOALLOC_MAX_BODIES)
+#define CC_NOALLOC_SCRATCH_BYTES (16u << 20)
+CC_API cc_status cc_broadphase_noalloc(uint64_t n, float *aabb, int gx, int gy, int gz, int64_t *pairs,
+                                       uint64_t pairs_cap, uint64_t *n_pairs, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
