@@ -77,6 +77,13 @@ class Context:
     def set_tuning(self, cell_target=4.0, min_ratio=2.0):
         self.check(lib.cc_set_tuning(self.h, float(cell_target), float(min_ratio)), "cc_set_tuning")
 
+    def set_narrowphase_precision(self, mode="exact"):
+        """"exact" (default): the reference's MPR arithmetic in FP64, equal to
+        the FP64 oracle up to float rounding of the outputs; "fp64": FP64 in a
+        pair-local frame with FMA; "mixed": FP32 support maps."""
+        self.check(lib.cc_set_narrowphase_precision(self.h, {"exact": 0, "fp64": 1, "mixed": 2}[mode]),
+                   "cc_set_narrowphase_precision")
+
     def last_grid(self):
         dims = (ctypes.c_int * 3)()
         e = ctypes.c_uint64()

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kNT) k_aabb(uint64_t n, const int32_t *__restr
                                                const float *__restrict__ R, const uint32_t *__restrict__ ID,
                                                uint64_t nb, const float *__restrict__ pos,
                                                const float *__restrict__ rot, float *__restrict__ aabb,
-                                               DevStats *stats, uint32_t *err) {
+                                               DevStats *stats, uint32_t *err, PlanArgs pa) {
 	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
 	float3 mn = f3(INFINITY, INFINITY, INFINITY), mx = f3(-INFINITY, -INFINITY, -INFINITY);
 	bool have = false;
@@ -89,19 +89,25 @@ __global__ void __launch_bounds__(kNT) k_aabb(uint64_t n, const int32_t *__restr
 		}
 		have = true;
 	}
-	if constexpr (kStats) accumulate_stats<kNT>(mn, mx, have, stats);
+	if constexpr (kStats) accumulate_stats<kNT>(mn, mx, have, stats, pa);
 }
 }  // namespace
 
 void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
-                 uint32_t *err, cudaStream_t s) {
+                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s) {
 	if (n == 0) return;
-	const unsigned grid = (unsigned)((n + kNT - 1) / kNT);
+	const unsigned blocks = (unsigned)((n + kNT - 1) / kNT);
+	PlanArgs pa;
+	pa.gp = gp;
+	pa.gx = grid ? grid[0] : 1;
+	pa.gy = grid ? grid[1] : 1;
+	pa.gz = grid ? grid[2] : 1;
+	pa.n = n;
 	if (stats)
-		k_aabb<true><<<grid, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, stats, err);
+		k_aabb<true><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, stats, err, pa);
 	else
-		k_aabb<false><<<grid, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err);
+		k_aabb<false><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, pa);
 }
 
 }  // namespace cc

@@ -46,56 +46,6 @@ __device__ __forceinline__ void st3p(float *p, uint64_t i, float3 v) {
 	p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z;
 }
 
-// Grid parameters from the reduced bounds. Every block of k_count computes it
-// (deterministically); block 0 also stores it for the later kernels.
-__device__ Plan make_plan(const DevStats *st, const GridParams &gp, int gx, int gy, int gz, uint64_t n) {
-	Plan p;
-	const int grid[3] = {gx, gy, gz};
-	float mn[3], mx[3];
-	p.valid = (st->err & (kErrNonFinite | kErrInverted)) ? 0 : 1;
-	for (int d = 0; d < 3; d++) {
-		mn[d] = ord2f(~st->bmin_inv[d]);
-		mx[d] = ord2f(st->bmax[d]);
-		p.origin[d] = fabsf(mn[d]);                                    // :379
-		p.invbin[d] = (float)grid[d] / fabsf(mx[d] + fabsf(mn[d]));    // :380-381
-		p.grid[d] = grid[d];
-		p.lo[d] = mn[d] + p.origin[d];  // exact minimum of the shifted coordinates
-	}
-	float ext[3], mean[3];
-	float mean_max = 0.f;
-	for (int d = 0; d < 3; d++) {
-		const float hi = mx[d] + p.origin[d];
-		ext[d] = hi - p.lo[d];
-		mean[d] = (float)(st->ext_sum[d] / (double)(n ? n : 1));
-		mean_max = fmaxf(mean_max, mean[d]);
-	}
-	int dim[3];
-	if (gp.user_dim[0] > 0) {
-		for (int d = 0; d < 3; d++) dim[d] = min(max(gp.user_dim[d], 1), kMaxDim);
-	} else {
-		// cell edge: the cube root of the volume that holds k_target boxes on
-		// average, but at least min_ratio times the mean box extent
-		double vol = 1.0;
-		const float floor_len = fmaxf(mean_max, 1e-30f);
-		for (int d = 0; d < 3; d++) vol *= (double)fmaxf(ext[d], floor_len);
-		double c = cbrt(vol * (double)gp.k_target / (double)(n ? n : 1));
-		c = fmax(c, (double)gp.min_ratio * (double)mean_max);
-		for (int d = 0; d < 3; d++) {
-			double q = c > 0.0 ? (double)ext[d] / c : 1.0;
-			dim[d] = (int)fmin(fmax(q, 1.0), (double)kMaxDim);
-		}
-	}
-	while ((uint64_t)dim[0] * dim[1] * dim[2] > gp.g_max) {
-		for (int d = 0; d < 3; d++) dim[d] = max(1, (int)(dim[d] * 0.8f));
-	}
-	for (int d = 0; d < 3; d++) {
-		p.dim[d] = dim[d];
-		p.inv[d] = ext[d] > 0.f ? (float)dim[d] / ext[d] : 0.f;
-	}
-	p.G = (uint32_t)dim[0] * dim[1] * dim[2];
-	return p;
-}
-
 // Search-grid cell of a shifted coordinate: monotone in v.
 __device__ __forceinline__ int cell_of(float v, float lo, float inv, int dim) {
 	float t = (v - lo) * inv;
@@ -119,7 +69,8 @@ __device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
 	return (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
 }
 
-__global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restrict__ aabb, DevStats *stats) {
+__global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
+                                                 PlanArgs pa) {
 	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
 	float3 mn = f3(0.f, 0.f, 0.f), mx = mn;
 	const bool have = i < n;
@@ -127,17 +78,14 @@ __global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restr
 		mn = ld3p(aabb, i);
 		mx = ld3p(aabb, i + n);
 	}
-	accumulate_stats<kNT>(mn, mx, have, stats);
+	accumulate_stats<kNT>(mn, mx, have, stats, pa);
 }
 
-__global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, GridParams gp, int gx, int gy,
-                                                int gz, DevStats *stats, uint32_t *__restrict__ cell_count,
-                                                uint32_t *__restrict__ owner_count) {
+__global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, const DevStats *stats,
+                                                uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count) {
 	__shared__ Plan sp;
-	if (threadIdx.x == 0) {
-		sp = make_plan(stats, gp, gx, gy, gz, n);
-		if (blockIdx.x == 0) stats->plan = sp;
-	}
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	if (!sp.valid) return;  // invalid input: nothing is modified
 	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
@@ -159,7 +107,8 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
                                                   uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
                                                   uint64_t cap, uint32_t *err) {
 	__shared__ Plan sp;
-	if (threadIdx.x == 0) sp = stats->plan;
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
 	if (!sp.valid || i >= n) return;
@@ -189,7 +138,8 @@ __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const 
                                                     unsigned long long *__restrict__ pairs, uint64_t pair_cap,
                                                     unsigned long long *pair_counter) {
 	__shared__ Plan sp;
-	if (threadIdx.x == 0) sp = stats->plan;
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	if (!sp.valid) return;
 	const uint64_t E = min((uint64_t)stats->entries, entry_cap);
@@ -258,16 +208,23 @@ __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const 
 	}
 }
 
-__global__ void __launch_bounds__(kNT) k_owner_scatter(uint64_t P, const unsigned long long *__restrict__ tmp,
+// Bucket the unsorted pairs by owner (the smaller index). P comes from the
+// device; if it exceeds the scratch or the output nothing is written.
+__global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t pair_cap, uint64_t out_cap,
+                                                        const unsigned long long *__restrict__ tmp,
                                                         const unsigned long long *__restrict__ owner_off,
                                                         uint32_t *__restrict__ owner_count,
                                                         unsigned long long *__restrict__ out) {
-	const uint64_t t = (uint64_t)blockIdx.x * kNT + threadIdx.x;
-	if (t >= P) return;
-	const unsigned long long key = tmp[t];
-	const uint32_t a = (uint32_t)(key >> 32);
-	const uint32_t k = atomicSub(&owner_count[a], 1u) - 1u;
-	out[owner_off[a] + k] = key;
+	const unsigned long long P = stats->pairs;
+	const bool fits = P <= pair_cap && P <= out_cap;
+	if (blockIdx.x == 0 && threadIdx.x == 0) stats->np_n = fits ? P : 0ull;
+	if (!fits) return;
+	for (uint64_t t = (uint64_t)blockIdx.x * kNT + threadIdx.x; t < P; t += (uint64_t)gridDim.x * kNT) {
+		const unsigned long long key = tmp[t];
+		const uint32_t a = (uint32_t)(key >> 32);
+		const uint32_t k = atomicSub(&owner_count[a], 1u) - 1u;
+		out[owner_off[a] + k] = key;
+	}
 }
 
 constexpr int kSmallSeg = 32;
@@ -277,7 +234,7 @@ __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long
                                                   unsigned long long *__restrict__ out, uint32_t *big_list,
                                                   uint64_t big_cap, DevStats *stats) {
 	const uint64_t a = (uint64_t)blockIdx.x * kNT + threadIdx.x;
-	if (a >= n) return;
+	if (a >= n || stats->np_n != stats->pairs) return;  // the pairs were not emitted
 	const uint64_t beg = owner_off[a], end = owner_off[a + 1];
 	const uint64_t len = end - beg;
 	if (len <= 1) return;
@@ -303,31 +260,37 @@ __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long
 	else atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
 }
 
-// One block per segment of 33..4096 keys: bitonic sort in shared memory.
-__global__ void __launch_bounds__(512) k_segsort_big(const uint32_t *__restrict__ big_list,
+// Segments of 33..4096 keys: one block per segment (grid-stride over the
+// device-side count), bitonic sort in shared memory.
+__global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint64_t big_cap,
+                                                      const uint32_t *__restrict__ big_list,
                                                       const unsigned long long *__restrict__ owner_off,
                                                       unsigned long long *__restrict__ out) {
 	__shared__ unsigned long long s[kBigSeg];
-	const uint32_t a = big_list[blockIdx.x];
-	const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
-	int m = 1;
-	while ((uint64_t)m < len) m <<= 1;
-	for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? out[beg + i] : ~0ull;
-	__syncthreads();
-	for (int k = 2; k <= m; k <<= 1) {
-		for (int j = k >> 1; j > 0; j >>= 1) {
-			for (int i = threadIdx.x; i < m; i += blockDim.x) {
-				const int p = i ^ j;
-				if (p > i) {
-					const bool up = (i & k) == 0;
-					const unsigned long long x = s[i], y = s[p];
-					if ((x > y) == up) { s[i] = y; s[p] = x; }
+	const uint64_t nbig = min((uint64_t)stats->big_segments, big_cap);
+	for (uint64_t g = blockIdx.x; g < nbig; g += gridDim.x) {
+		const uint32_t a = big_list[g];
+		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
+		int m = 1;
+		while ((uint64_t)m < len) m <<= 1;
+		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? out[beg + i] : ~0ull;
+		__syncthreads();
+		for (int k = 2; k <= m; k <<= 1) {
+			for (int j = k >> 1; j > 0; j >>= 1) {
+				for (int i = threadIdx.x; i < m; i += blockDim.x) {
+					const int p = i ^ j;
+					if (p > i) {
+						const bool up = (i & k) == 0;
+						const unsigned long long x = s[i], y = s[p];
+						if ((x > y) == up) { s[i] = y; s[p] = x; }
+					}
 				}
+				__syncthreads();
 			}
-			__syncthreads();
 		}
+		for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = s[i];
+		__syncthreads();
 	}
-	for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = s[i];
 }
 
 // ---------------------------------------------------------------- bin list
@@ -355,7 +318,8 @@ __device__ __forceinline__ RefRange ref_range(const Plan &p, float3 mn, float3 m
 __global__ void __launch_bounds__(kNT) k_ref_count(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
                                                     uint32_t *__restrict__ cnt) {
 	__shared__ Plan sp;
-	if (threadIdx.x == 0) sp = stats->plan;
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
 	if (i >= n) return;
@@ -372,7 +336,8 @@ __global__ void __launch_bounds__(kNT) k_ref_emit(uint64_t n, const float *__res
                                                    const unsigned long long *__restrict__ off,
                                                    unsigned long long *__restrict__ keys, uint64_t cap) {
 	__shared__ Plan sp;
-	if (threadIdx.x == 0) sp = stats->plan;
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
 	if (i >= n) return;
@@ -421,18 +386,23 @@ __global__ void __launch_bounds__(kNT) k_ref_split(const unsigned long long *__r
 inline unsigned blocks_for(uint64_t n) { return (unsigned)((n + kNT - 1) / kNT); }
 }  // namespace
 
-void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, cudaStream_t s) {
-	if (n) k_bounds<<<blocks_for(n), kNT, 0, s>>>(n, aabb, stats);
+void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridParams &gp, const int grid[3],
+                   cudaStream_t s) {
+	PlanArgs pa;
+	pa.gp = gp;
+	pa.gx = grid[0];
+	pa.gy = grid[1];
+	pa.gz = grid[2];
+	pa.n = n;
+	if (n) k_bounds<<<blocks_for(n), kNT, 0, s>>>(n, aabb, stats, pa);
 }
 
-void launch_count(uint64_t n, float *aabb, const GridParams &gp, const int grid[3], const BpBuffers &b,
-                  cudaStream_t s) {
-	k_count<<<blocks_for(n), kNT, 0, s>>>(n, aabb, gp, grid[0], grid[1], grid[2], b.stats, b.cell_count,
-	                                      b.owner_count);
+void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
+	k_count<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count);
 }
 
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
-	launch_scan_u32_to_u32(b.cell_count, g_max, b.cell_start, b.status, b.ticket, &b.stats->err, s, &b.stats->plan.G,
+	launch_scan_u32_to_u32(b.cell_count, g_max, b.cell_start, b.status, b.ticket, &b.stats->err, s, &b.stats->cells,
 	                       &b.stats->entries);
 }
 
@@ -453,16 +423,18 @@ void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s) {
 	launch_scan_u32_to_u64(b.owner_count, n, b.owner_off, b.status, b.ticket, &b.stats->err, s);
 }
 
-void launch_owner_scatter(uint64_t P, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
-	if (P) k_owner_scatter<<<blocks_for(P), kNT, 0, s>>>(P, b.pairs_tmp, b.owner_off, b.owner_count, out);
+void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
+	const uint64_t bound = std::min<uint64_t>(b.pair_cap, out_cap);
+	const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(blocks_for(bound), 1), (uint64_t)kNumSMs * 8);
+	k_owner_scatter<<<grid, kNT, 0, s>>>(b.stats, b.pair_cap, out_cap, b.pairs_tmp, b.owner_off, b.owner_count, out);
 }
 
 void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
 	k_segsort<<<blocks_for(n), kNT, 0, s>>>(n, b.owner_off, out, b.big_list, b.big_cap, b.stats);
 }
 
-void launch_segsort_big(uint64_t nbig, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
-	if (nbig) k_segsort_big<<<(unsigned)nbig, 512, 0, s>>>(b.big_list, b.owner_off, out);
+void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
+	k_segsort_big<<<kNumSMs, 512, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
 }
 
 void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s) {

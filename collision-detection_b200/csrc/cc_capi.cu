@@ -42,7 +42,7 @@ struct cc_ctx {
 	// device scratch
 	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list;
 	Buf ref_cnt, ref_off, ref_keys, ref_tmp, ref_flags, ref_runpos, rx_hist, rx_hoff;
-	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos;
+	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes;
 	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
 	    out_depth, out_bids;
 	DevStats *h_stats = nullptr;  // pinned
@@ -53,6 +53,7 @@ struct cc_ctx {
 	uint64_t last_E = 0, last_P = 0;
 	int last_dim[3] = {0, 0, 0};
 	uint64_t launches = 0;
+	int np_precision = CC_NP_EXACT;
 	// stage profiler
 	bool prof = false;
 	cudaEvent_t ev[2 * kMaxMarks] = {};
@@ -203,8 +204,29 @@ BpBuffers bp_buffers(cc_ctx *c) {
 
 size_t status_words_for(uint64_t n) { return scan_tiles(n) + 8; }
 
-// Allocates the n-dependent broadphase scratch.
-cc_status bp_prepare(cc_ctx *c, uint64_t n) {
+// Narrowphase scratch for up to P pairs.
+cc_status np_prepare(cc_ctx *c, uint64_t P) {
+	P = std::max<uint64_t>(P, 1);
+	CC_TRY(ensure(c, c->np_norm, 12 * P));
+	CC_TRY(ensure(c, c->np_pa, 12 * P));
+	CC_TRY(ensure(c, c->np_pb, 12 * P));
+	CC_TRY(ensure(c, c->np_depth, 4 * P));
+	CC_TRY(ensure(c, c->np_ids, 8 * P));
+	CC_TRY(ensure(c, c->np_pairs, 8 * P));
+	CC_TRY(ensure(c, c->np_flag, 4 * P));
+	CC_TRY(ensure(c, c->np_pos, 8 * (P + 1)));
+	CC_TRY(ensure(c, c->np_order, 4 * P));
+	CC_TRY(ensure(c, c->np_classes, (2 * kNpClasses + 32) * sizeof(uint32_t)));
+	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
+	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(P + 1)));
+	CC_TRY(ensure(c, c->ticket, 64));
+	return CC_OK;
+}
+
+// Allocates the n-dependent broadphase scratch and, if np_cap > 0, the
+// narrowphase scratch for np_cap pairs. Buffers only grow; every public call
+// ends with a synchronize, so nothing in flight uses a buffer replaced here.
+cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap) {
 	c->gp.g_max = g_max_for(n);
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
 	CC_TRY(ensure(c, c->cell_count, sizeof(uint32_t) * c->gp.g_max));
@@ -218,18 +240,50 @@ cc_status bp_prepare(cc_ctx *c, uint64_t n) {
 	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(std::max<uint64_t>(c->gp.g_max, n + 1))));
 	CC_TRY(ensure(c, c->ticket, 64));
 	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * std::max<uint64_t>(1024, n / 16)));
+	if (np_cap) CC_TRY(np_prepare(c, np_cap));
 	return CC_OK;
 }
 
-// Broadphase up to the per-owner offsets. Requires stats zeroed and the
-// bounds pass done (k_bounds or the fused AABB kernel). Returns P in *P_out.
-cc_status bp_core(cc_ctx *c, uint64_t n, float *aabb, const int grid[3], cudaStream_t s, uint64_t *P_out) {
+NpScratch np_scratch(cc_ctx *c) {
+	NpScratch sc;
+	sc.norm = ptr<float>(c->np_norm);
+	sc.pa = ptr<float>(c->np_pa);
+	sc.pb = ptr<float>(c->np_pb);
+	sc.depth = ptr<float>(c->np_depth);
+	sc.ids = ptr<int32_t>(c->np_ids);
+	sc.pairs = ptr<unsigned long long>(c->np_pairs);
+	sc.flag = ptr<uint32_t>(c->np_flag);
+	sc.pos = ptr<unsigned long long>(c->np_pos);
+	sc.status = ptr<uint64_t>(c->status);
+	sc.ticket = ptr<uint32_t>(c->ticket);
+	sc.err = &ptr<DevStats>(c->stats)->err;
+	sc.order = ptr<uint32_t>(c->np_order);
+	sc.classes = ptr<uint32_t>(c->np_classes);
+	return sc;
+}
+
+// Arguments of the narrowphase stage.
+struct NpArgs {
+	uint64_t n, nb;
+	const int32_t *T;
+	const float *A, *B, *C, *R;
+	const uint32_t *ID;
+	const uint8_t *active;
+	const float *pos, *rot;
+	float envelope;
+	int64_t *pairs;
+	float *norm, *cpta, *cptb, *depth;
+	int32_t *bids;
+};
+
+// count .. owner scan: needs stats zeroed and the plan from the bounds pass.
+void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s) {
 	BpBuffers b = bp_buffers(c);
 	const uint32_t gmax = c->gp.g_max;
 	{
 		StageMark m(c, ST_COUNT, s);
-		CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s));
-		launch_count(n, aabb, c->gp, grid, b, s);
+		cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
+		launch_count(n, aabb, b, s);
 	}
 	{
 		StageMark m(c, ST_SCAN_CELLS, s);
@@ -237,7 +291,7 @@ cc_status bp_core(cc_ctx *c, uint64_t n, float *aabb, const int grid[3], cudaStr
 	}
 	{
 		StageMark m(c, ST_SCATTER, s);
-		CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s));
+		cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
 		launch_scatter(n, aabb, b, s);
 	}
 	{
@@ -249,78 +303,128 @@ cc_status bp_core(cc_ctx *c, uint64_t n, float *aabb, const int grid[3], cudaStr
 		launch_scan_owner(n, b, s);
 	}
 	c->launches += 5;
-	CC_TRY(check_launch(c));
-	CC_TRY(read_stats(c, s));
-	CC_TRY(device_err(c));
-	uint64_t E = c->h_stats->entries, P = c->h_stats->pairs;
-	for (int round = 0; round < 2 && (E > b.entry_cap || P > b.pair_cap); round++) {
-		// a capacity guess was too small: grow and redo the passes after the count
-		if (E > b.entry_cap) {
-			if (E >= 0xffffffffull) return set_err(c, CC_ERR_CAPACITY, "search grid needs %llu entries (>= 2^32)",
-			                                        (unsigned long long)E);
-			CC_TRY(ensure(c, c->entries, 2 * sizeof(float4) * (E + E / 8)));
-		}
-		if (P > b.pair_cap) CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * (P + P / 8)));
-		b = bp_buffers(c);
-		CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s));
-		CC_CUDA(c, cudaMemsetAsync(b.owner_count, 0, sizeof(uint32_t) * n, s));
-		CC_CUDA(c, cudaMemsetAsync(&b.stats->pairs, 0, sizeof(unsigned long long), s));
-		launch_scatter(n, aabb, b, s);
-		launch_pair_test(n, b, E, s);
-		launch_scan_owner(n, b, s);
-		c->launches += 3;
-		CC_TRY(check_launch(c));
-		CC_TRY(read_stats(c, s));
-		CC_TRY(device_err(c));
-		E = c->h_stats->entries;
-		P = c->h_stats->pairs;
-	}
-	if (E > b.entry_cap || P > b.pair_cap)
-		return set_err(c, CC_ERR_INTERNAL, "broadphase scratch did not converge (E=%llu P=%llu)",
-		               (unsigned long long)E, (unsigned long long)P);
-	c->last_E = E;
-	c->last_P = P;
-	for (int d = 0; d < 3; d++) c->last_dim[d] = c->h_stats->plan.dim[d];
-	*P_out = P;
-	return CC_OK;
 }
 
-// Buckets the retained pairs by owner into `out` and sorts every bucket.
-cc_status bp_emit(cc_ctx *c, uint64_t n, uint64_t P, unsigned long long *out, cudaStream_t s) {
+// Sorted pair list into `out` (device-driven: writes nothing if the pair
+// count exceeds out_cap or the scratch).
+void enqueue_emit(cc_ctx *c, uint64_t n, unsigned long long *out, uint64_t out_cap, cudaStream_t s) {
 	BpBuffers b = bp_buffers(c);
 	{
 		StageMark m(c, ST_OWNER_SCATTER, s);
-		launch_owner_scatter(P, out, b, s);
+		launch_owner_scatter(out_cap, out, b, s);
 	}
 	{
 		StageMark m(c, ST_SEGSORT, s);
 		launch_segsort(n, out, b, s);
+		launch_segsort_big(out, b, s);
 	}
-	c->launches += 2;
-	CC_TRY(check_launch(c));
-	CC_TRY(read_stats(c, s));
-	const uint64_t nbig = std::min<uint64_t>(c->h_stats->big_segments, b.big_cap);
-	if (nbig) {
+	c->launches += 3;
+}
+
+// Narrowphase over min(P_cap, *P_dev) pairs (P_dev null: exactly P_cap).
+void enqueue_np(cc_ctx *c, const NpArgs &a, uint64_t P_cap, const unsigned long long *P_dev, cudaStream_t s) {
+	if (!P_cap) return;
+	NpScratch sc = np_scratch(c);
+	{
+		StageMark m(c, ST_MPR, s);
+		launch_mpr(P_cap, P_dev, a.n, a.T, a.A, a.B, a.C, a.R, a.ID, a.nb, a.active, a.pos, a.rot, a.envelope,
+		           reinterpret_cast<const long long *>(a.pairs), sc, c->np_precision,
+		           P_dev ? std::max<uint64_t>(c->last_P, 1) : P_cap, s);
+	}
+	{
+		StageMark m(c, ST_NP_COMPACT, s);
+		launch_np_compact(P_cap, P_dev, sc, reinterpret_cast<long long *>(a.pairs), a.norm, a.cpta, a.cptb, a.depth,
+		                  a.bids, &ptr<DevStats>(c->stats)->contacts, s);
+	}
+	c->launches += 5;
+}
+
+// Zeroes the per-pass counters before the passes after the count are redone.
+cc_status reset_pass_counters(cc_ctx *c, uint64_t n, cudaStream_t s) {
+	DevStats *d = ptr<DevStats>(c->stats);
+	CC_CUDA(c, cudaMemsetAsync(c->cell_count.p, 0, sizeof(uint32_t) * c->gp.g_max, s));
+	CC_CUDA(c, cudaMemsetAsync(c->owner_count.p, 0, sizeof(uint32_t) * n, s));
+	CC_CUDA(c, cudaMemsetAsync(&d->err, 0, sizeof(uint32_t), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->pairs, 0, sizeof(unsigned long long), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 2 * sizeof(unsigned long long), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->np_n, 0, sizeof(unsigned long long), s));
+	return CC_OK;
+}
+
+// After the synchronize: if a scratch guess (entries, unsorted pairs) was too
+// small, grow it and redo the passes after the count (rare: the guesses
+// follow the previous call). h_stats is current on return.
+cc_status settle(cc_ctx *c, uint64_t n, float *aabb, unsigned long long *out, uint64_t out_cap, const NpArgs *np,
+                 cudaStream_t s) {
+	for (int round = 0; round < 3; round++) {
+		const uint64_t E = c->h_stats->entries, P = c->h_stats->pairs;
+		BpBuffers b = bp_buffers(c);
+		if (E <= b.entry_cap && P <= b.pair_cap) return CC_OK;
+		if (E >= 0xffffffffull)
+			return set_err(c, CC_ERR_CAPACITY, "search grid needs %llu entries (>= 2^32)", (unsigned long long)E);
+		if (E > b.entry_cap) CC_TRY(ensure(c, c->entries, 2 * sizeof(float4) * (E + E / 8)));
+		if (P > b.pair_cap) CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * (P + P / 8)));
+		CC_TRY(reset_pass_counters(c, n, s));
+		b = bp_buffers(c);
+		launch_scatter(n, aabb, b, s);
+		launch_pair_test(n, b, E, s);
+		launch_scan_owner(n, b, s);
+		c->launches += 3;
+		if (out) enqueue_emit(c, n, out, out_cap, s);
+		if (np) enqueue_np(c, *np, out_cap, &ptr<DevStats>(c->stats)->np_n, s);
+		CC_TRY(check_launch(c));
+		CC_TRY(read_stats(c, s));
+		CC_TRY(device_err(c));
+	}
+	return set_err(c, CC_ERR_INTERNAL, "broadphase scratch did not converge");
+}
+
+// A bucket longer than the block sort handles: sort the whole list (rare).
+cc_status sort_fallback(cc_ctx *c, uint64_t n, uint64_t P, unsigned long long *out, cudaStream_t s) {
+	const size_t hw = radix_hist_words(P);
+	CC_TRY(ensure(c, c->ref_tmp, sizeof(unsigned long long) * P));
+	CC_TRY(ensure(c, c->rx_hist, sizeof(uint32_t) * hw));
+	CC_TRY(ensure(c, c->rx_hoff, sizeof(unsigned long long) * (hw + 1)));
+	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(hw + 1)));
+	int bits = 1;
+	while (bits < 32 && ((uint64_t)1 << bits) < n) bits++;
+	{
 		StageMark m(c, ST_SEGSORT, s);
-		launch_segsort_big(nbig, out, b, s);
-		c->launches += 1;
-	}
-	if (c->h_stats->err & kErrSegmentTooLong) {
-		// a bucket is longer than the block sort handles: sort the whole list
-		const size_t hw = radix_hist_words(P);
-		CC_TRY(ensure(c, c->ref_tmp, sizeof(unsigned long long) * P));
-		CC_TRY(ensure(c, c->rx_hist, sizeof(uint32_t) * hw));
-		CC_TRY(ensure(c, c->rx_hoff, sizeof(unsigned long long) * (hw + 1)));
-		CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(hw + 1)));
-		int bits = 1;
-		while (bits < 32 && ((uint64_t)1 << bits) < n) bits++;
 		radix_sort_u64(out, ptr<unsigned long long>(c->ref_tmp), P, 0, 32 + bits, ptr<uint32_t>(c->rx_hist),
 		               ptr<unsigned long long>(c->rx_hoff), ptr<uint64_t>(c->status), ptr<uint32_t>(c->ticket),
 		               &ptr<DevStats>(c->stats)->err, s);
-		c->launches += 3 * ((32 + bits + 7) / 8);
 	}
+	c->launches += 3 * ((32 + bits + 7) / 8);
 	CC_TRY(check_launch(c));
 	CC_CUDA(c, cudaStreamSynchronize(s));
+	return CC_OK;
+}
+
+void remember(cc_ctx *c) {
+	c->last_E = c->h_stats->entries;
+	c->last_P = c->h_stats->pairs;
+	for (int d = 0; d < 3; d++) c->last_dim[d] = c->h_stats->plan.dim[d];
+}
+
+void retain(cc_ctx *c, uint64_t n, uint64_t P) {
+	c->retained = true;
+	c->retained_n = n;
+	c->retained_P = P;
+}
+
+// Writes the retained pair list into `out` (cap >= P checked by the caller).
+cc_status emit_retained(cc_ctx *c, unsigned long long *out, uint64_t cap, cudaStream_t s) {
+	DevStats *d = ptr<DevStats>(c->stats);
+	c->h_word[0] = c->retained_P;
+	CC_CUDA(c, cudaMemcpyAsync(&d->pairs, c->h_word, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 2 * sizeof(unsigned long long), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->err, 0, sizeof(uint32_t), s));
+	enqueue_emit(c, c->retained_n, out, cap, s);
+	CC_TRY(check_launch(c));
+	CC_TRY(read_stats(c, s));
+	c->retained = false;
+	if (c->h_stats->err & kErrSegmentTooLong) CC_TRY(sort_fallback(c, c->retained_n, c->retained_P, out, s));
 	return CC_OK;
 }
 
@@ -339,59 +443,8 @@ cc_status check_grid(cc_ctx *c, int gx, int gy, int gz) {
 	return CC_OK;
 }
 
-cc_status np_run(cc_ctx *c, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
-                 const float *R, const uint32_t *ID, uint64_t nb, const uint8_t *active, const float *pos,
-                 const float *rot,
-                 float envelope, int64_t *pairs, uint64_t P, float *norm, float *cpta, float *cptb, float *depth,
-                 int32_t *bids, uint64_t *n_contacts, cudaStream_t s) {
-	*n_contacts = 0;
-	if (P == 0) return CC_OK;
-	CC_TRY(ensure(c, c->np_norm, 12 * P));
-	CC_TRY(ensure(c, c->np_pa, 12 * P));
-	CC_TRY(ensure(c, c->np_pb, 12 * P));
-	CC_TRY(ensure(c, c->np_depth, 4 * P));
-	CC_TRY(ensure(c, c->np_ids, 8 * P));
-	CC_TRY(ensure(c, c->np_pairs, 8 * P));
-	CC_TRY(ensure(c, c->np_flag, 4 * P));
-	CC_TRY(ensure(c, c->np_pos, 8 * (P + 1)));
-	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
-	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(P + 1)));
-	CC_TRY(ensure(c, c->ticket, 64));
-	NpScratch sc;
-	sc.norm = ptr<float>(c->np_norm);
-	sc.pa = ptr<float>(c->np_pa);
-	sc.pb = ptr<float>(c->np_pb);
-	sc.depth = ptr<float>(c->np_depth);
-	sc.ids = ptr<int32_t>(c->np_ids);
-	sc.pairs = ptr<unsigned long long>(c->np_pairs);
-	sc.flag = ptr<uint32_t>(c->np_flag);
-	sc.pos = ptr<unsigned long long>(c->np_pos);
-	sc.status = ptr<uint64_t>(c->status);
-	sc.ticket = ptr<uint32_t>(c->ticket);
-	sc.err = &ptr<DevStats>(c->stats)->err;
-	CC_CUDA(c, cudaMemsetAsync(sc.err, 0, sizeof(uint32_t), s));
-	{
-		StageMark m(c, ST_MPR, s);
-		launch_mpr(P, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, reinterpret_cast<const long long *>(pairs),
-		           sc, s);
-	}
-	{
-		StageMark m(c, ST_NP_COMPACT, s);
-		launch_np_compact(P, sc, reinterpret_cast<long long *>(pairs), norm, cpta, cptb, depth, bids, s);
-	}
-	c->launches += 3;
-	CC_TRY(check_launch(c));
-	CC_CUDA(c, cudaMemcpyAsync(c->h_word, sc.pos + P, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-	CC_CUDA(c, cudaMemcpyAsync(c->h_word + 1, sc.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-	CC_CUDA(c, cudaStreamSynchronize(s));
-	if ((uint32_t)c->h_word[1] & kErrBadIndex)
-		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is >= nb");
-	if ((uint32_t)c->h_word[1] & kErrSpinLimit) return set_err(c, CC_ERR_INTERNAL, "device-side look-back wait gave up");
-	*n_contacts = c->h_word[0];
-	return CC_OK;
-}
-
-// Shared body of cc_collide / cc_collide_host on device pointers.
+// GenerateAABB -> broadphase -> narrowphase on device pointers with one
+// synchronize in the common case.
 cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
                       int64_t *pairs, uint64_t pairs_cap, float *norm, float *cpta, float *cptb, float *depth,
                       int32_t *bids, uint64_t *n_pairs, uint64_t *n_contacts, cudaStream_t s) {
@@ -400,28 +453,46 @@ cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, flo
 	c->retained = false;
 	const uint64_t n = sc.n;
 	if (n == 0) return CC_OK;
-	CC_TRY(bp_prepare(c, n));
+	CC_TRY(prepare(c, n, pairs_cap));
+	DevStats *d = ptr<DevStats>(c->stats);
+	const int grid[3] = {gx, gy, gz};
 	{
 		StageMark m(c, ST_AABB, s);
-		CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
-		launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb,
-		            ptr<DevStats>(c->stats), &ptr<DevStats>(c->stats)->err, s);
+		CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), s));
+		launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb, d, &d->err, c->gp,
+		            grid, s);
 	}
 	c->launches += 1;
-	const int grid[3] = {gx, gy, gz};
-	uint64_t P = 0;
-	CC_TRY(bp_core(c, n, aabb, grid, s, &P));
+	enqueue_search(c, n, aabb, s);
+	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
+	enqueue_emit(c, n, out, pairs_cap, s);
+	const NpArgs a = {n, sc.nb, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, envelope,
+	                  pairs, norm, cpta, cptb, depth, bids};
+	enqueue_np(c, a, pairs_cap, &d->np_n, s);
+	CC_TRY(check_launch(c));
+	CC_TRY(read_stats(c, s));
+	CC_TRY(device_err(c));
+	CC_TRY(settle(c, n, aabb, out, pairs_cap, &a, s));
+	remember(c);
+	const uint64_t P = c->h_stats->pairs;
 	*n_pairs = P;
 	if (P > pairs_cap) {
-		c->retained = true;
-		c->retained_n = n;
-		c->retained_P = P;
+		retain(c, n, P);
 		return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries, capacity %llu", (unsigned long long)P,
 		               (unsigned long long)pairs_cap);
 	}
-	CC_TRY(bp_emit(c, n, P, reinterpret_cast<unsigned long long *>(pairs), s));
-	return np_run(c, n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.active, sc.body_pos, sc.body_rot, envelope,
-	              pairs, P, norm, cpta, cptb, depth, bids, n_contacts, s);
+	if (c->h_stats->err & kErrSegmentTooLong) {
+		// the list was sorted bucket-wise only up to 4096 per bucket: sort it whole, redo the narrowphase
+		CC_TRY(sort_fallback(c, n, P, out, s));
+		CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
+		enqueue_np(c, a, pairs_cap, &d->np_n, s);
+		CC_TRY(check_launch(c));
+		CC_TRY(read_stats(c, s));
+	}
+	if (c->h_stats->err & kErrBadIndex)
+		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is >= nb");
+	*n_contacts = c->h_stats->contacts;
+	return CC_OK;
 }
 
 }  // namespace
@@ -454,7 +525,7 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->pairs_tmp, &c->status,    &c->ticket,     &c->big_list, &c->ref_cnt,     &c->ref_off,
 	               &c->ref_keys, &c->ref_tmp,    &c->ref_flags,  &c->ref_runpos, &c->rx_hist,   &c->rx_hoff,
 	               &c->np_norm,  &c->np_pa,      &c->np_pb,      &c->np_depth, &c->np_ids,      &c->np_pairs,
-	               &c->np_flag,  &c->np_pos,     &c->in_T,       &c->in_A,     &c->in_B,        &c->in_C,
+	               &c->np_flag,  &c->np_pos,     &c->np_order, &c->np_classes, &c->in_T,       &c->in_A,     &c->in_B,        &c->in_C,
 	               &c->in_R,     &c->in_ID,      &c->in_pos,     &c->in_rot,   &c->in_act,      &c->out_aabb,
 	               &c->out_pairs, &c->out_norm,  &c->out_pa,     &c->out_pb,   &c->out_depth,   &c->out_bids};
 	for (Buf *b : bufs)
@@ -498,6 +569,12 @@ cc_status cc_set_tuning(cc_ctx *c, float cell_target, float min_ratio) {
 	if (!c || !(cell_target > 0.f) || !(min_ratio >= 0.f)) return CC_ERR_INVALID_ARGUMENT;
 	c->gp.k_target = cell_target;
 	c->gp.min_ratio = min_ratio;
+	return CC_OK;
+}
+
+cc_status cc_set_narrowphase_precision(cc_ctx *c, int mode) {
+	if (!c || (mode != CC_NP_EXACT && mode != CC_NP_FP64 && mode != CC_NP_MIXED)) return CC_ERR_INVALID_ARGUMENT;
+	c->np_precision = mode;
 	return CC_OK;
 }
 
@@ -559,7 +636,7 @@ cc_status cc_generate_aabb(cc_ctx *c, uint64_t n, const int32_t *T, const float 
 	{
 		StageMark m(c, ST_AABB, s);
 		CC_CUDA(c, cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
-		launch_aabb(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, s);
+		launch_aabb(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, c->gp, nullptr, s);
 	}
 	c->launches += 1;
 	CC_TRY(check_launch(c));
@@ -581,26 +658,32 @@ cc_status cc_broadphase(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy, int 
 	if (!aabb) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb");
 	CC_CUDA(c, cudaSetDevice(c->device));
 	cudaStream_t s = (cudaStream_t)stream;
-	CC_TRY(bp_prepare(c, n));
+	CC_TRY(prepare(c, n, 0));
+	const int grid[3] = {gx, gy, gz};
 	{
 		StageMark m(c, ST_BOUNDS, s);
 		CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
-		launch_bounds(n, aabb, ptr<DevStats>(c->stats), s);
+		launch_bounds(n, aabb, ptr<DevStats>(c->stats), c->gp, grid, s);
 	}
 	c->launches += 1;
-	const int grid[3] = {gx, gy, gz};
-	uint64_t P = 0;
-	CC_TRY(bp_core(c, n, aabb, grid, s, &P));
+	enqueue_search(c, n, aabb, s);
+	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
+	const uint64_t cap = pairs ? pairs_cap : 0;
+	if (cap) enqueue_emit(c, n, out, cap, s);
+	CC_TRY(check_launch(c));
+	CC_TRY(read_stats(c, s));
+	CC_TRY(device_err(c));
+	CC_TRY(settle(c, n, aabb, cap ? out : nullptr, cap, nullptr, s));
+	remember(c);
+	const uint64_t P = c->h_stats->pairs;
 	*n_pairs = P;
-	if (!pairs || P > pairs_cap) {
-		c->retained = true;
-		c->retained_n = n;
-		c->retained_P = P;
-		if (P == 0) return CC_OK;
+	if (P > cap) {
+		retain(c, n, P);
 		return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries, capacity %llu", (unsigned long long)P,
-		               (unsigned long long)pairs_cap);
+		               (unsigned long long)cap);
 	}
-	return bp_emit(c, n, P, reinterpret_cast<unsigned long long *>(pairs), s);
+	if (c->h_stats->err & kErrSegmentTooLong) CC_TRY(sort_fallback(c, n, P, out, s));
+	return CC_OK;
 }
 
 cc_status cc_broadphase_fetch(cc_ctx *c, int64_t *pairs, uint64_t pairs_cap, void *stream) {
@@ -611,9 +694,11 @@ cc_status cc_broadphase_fetch(cc_ctx *c, int64_t *pairs, uint64_t pairs_cap, voi
 	if (c->retained_P > pairs_cap || (!pairs && c->retained_P))
 		return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries", (unsigned long long)c->retained_P);
 	CC_CUDA(c, cudaSetDevice(c->device));
-	c->retained = false;
-	return bp_emit(c, c->retained_n, c->retained_P, reinterpret_cast<unsigned long long *>(pairs),
-	               (cudaStream_t)stream);
+	if (c->retained_P == 0) {
+		c->retained = false;
+		return CC_OK;
+	}
+	return emit_retained(c, reinterpret_cast<unsigned long long *>(pairs), pairs_cap, (cudaStream_t)stream);
 }
 
 cc_status cc_broadphase_bins(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy, int gz, uint32_t *bin_number,
@@ -630,14 +715,14 @@ cc_status cc_broadphase_bins(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy,
 	if (!aabb) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb");
 	CC_CUDA(c, cudaSetDevice(c->device));
 	cudaStream_t s = (cudaStream_t)stream;
-	CC_TRY(bp_prepare(c, n));
+	CC_TRY(prepare(c, n, 0));
 	StageMark bins_mark(c, ST_BINS, s);
 	BpBuffers b = bp_buffers(c);
-	CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
-	launch_bounds(n, aabb, b.stats, s);
-	CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * c->gp.g_max, s));
 	const int grid[3] = {gx, gy, gz};
-	launch_count(n, aabb, c->gp, grid, b, s);  // plan + in-place shift
+	CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
+	launch_bounds(n, aabb, b.stats, c->gp, grid, s);  // + plan
+	CC_CUDA(c, cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * c->gp.g_max, s));
+	launch_count(n, aabb, b, s);  // in-place shift
 	// per-body bin counts -> offsets
 	CC_TRY(ensure(c, c->ref_cnt, sizeof(uint32_t) * n));
 	CC_TRY(ensure(c, c->ref_off, sizeof(unsigned long long) * (n + 1)));
@@ -708,8 +793,19 @@ cc_status cc_narrowphase(cc_ctx *c, uint64_t n, const int32_t *T, const float *A
 	if (n_pairs && (!pairs || !norm || !cpta || !cptb || !depth || !bids || !active))
 		return set_err(c, CC_ERR_INVALID_ARGUMENT, "null pair/contact/active array");
 	CC_CUDA(c, cudaSetDevice(c->device));
-	return np_run(c, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, n_pairs, norm, cpta, cptb, depth,
-	              bids, n_contacts, (cudaStream_t)stream);
+	if (n_pairs == 0) return CC_OK;
+	cudaStream_t s = (cudaStream_t)stream;
+	CC_TRY(np_prepare(c, n_pairs));
+	CC_CUDA(c, cudaMemsetAsync(c->stats.p, 0, sizeof(DevStats), s));
+	const NpArgs a = {n, nb, T, A, B, C, R, ID, active, pos, rot, envelope, pairs, norm, cpta, cptb, depth, bids};
+	enqueue_np(c, a, n_pairs, nullptr, s);
+	CC_TRY(check_launch(c));
+	CC_TRY(read_stats(c, s));
+	if (c->h_stats->err & kErrBadIndex)
+		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is >= nb");
+	if (c->h_stats->err & kErrSpinLimit) return set_err(c, CC_ERR_INTERNAL, "device-side look-back wait gave up");
+	*n_contacts = c->h_stats->contacts;
+	return CC_OK;
 }
 
 cc_status cc_collide(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz, float envelope, cc_result *res,

@@ -35,6 +35,10 @@ struct DevStats {
 	unsigned long long contacts;
 	unsigned long long big_segments;
 	unsigned long long max_segment;
+	unsigned long long cells;     // plan.G as a 64-bit scan count
+	unsigned long long np_n;      // pairs handed to the narrowphase (0 if an output was too small)
+	uint32_t blocks_done;         // last-block detection of the bounds reduction
+	uint32_t pad_;
 	Plan plan;
 };
 
@@ -51,13 +55,15 @@ struct GridParams {
 // ------------------------------------------------------------------ scan
 // Exclusive scan of `n` uint32 counts into uint64 offsets out[0..n] (out[n] =
 // total) with one decoupled look-back pass. status: >= scan_tiles(n) words.
+// With n_dev the count is min(n, *n_dev), read on the device; total_out
+// (optional) receives the sum.
 size_t scan_tiles(uint64_t n);
 void launch_scan_u32_to_u64(const uint32_t *in, uint64_t n, unsigned long long *out, uint64_t *status,
-                            uint32_t *ticket, uint32_t *err, cudaStream_t s);
-// Same, 32-bit output (caller guarantees total < 2^32). With n_dev the count
-// is min(n, *n_dev), read on the device; total_out (optional) receives the sum.
+                            uint32_t *ticket, uint32_t *err, cudaStream_t s,
+                            const unsigned long long *n_dev = nullptr, unsigned long long *total_out = nullptr);
+// Same, 32-bit output (caller guarantees total < 2^32).
 void launch_scan_u32_to_u32(const uint32_t *in, uint64_t n, uint32_t *out, uint64_t *status, uint32_t *ticket,
-                            uint32_t *err, cudaStream_t s, const uint32_t *n_dev = nullptr,
+                            uint32_t *err, cudaStream_t s, const unsigned long long *n_dev = nullptr,
                             unsigned long long *total_out = nullptr);
 
 // ------------------------------------------------------------------ radix sort
@@ -71,11 +77,12 @@ void radix_sort_u64(unsigned long long *keys, unsigned long long *tmp, uint64_t 
 
 // ------------------------------------------------------------------ AABB
 // GenerateAABB. With `stats` non-null the kernel also accumulates the scene
-// bounds, extent sums and validity (the broadphase's first pass).
+// bounds, extent sums and validity (the broadphase's first pass) and its last
+// block writes the grid plan (stats->plan) for grid dims `grid` and tuning gp.
 // Body ids >= nb set kErrBadIndex in *err and leave that shape's AABB unwritten.
 void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
-                 uint32_t *err, cudaStream_t s);
+                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s);
 
 // ------------------------------------------------------------------ broadphase
 struct BpBuffers {
@@ -95,16 +102,21 @@ struct BpBuffers {
 	uint64_t big_cap;
 };
 
-void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, cudaStream_t s);
-void launch_count(uint64_t n, float *aabb, const GridParams &gp, const int grid[3], const BpBuffers &b,
-                  cudaStream_t s);
+// Bounds pass over caller AABBs; its last block writes stats->plan.
+void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridParams &gp, const int grid[3],
+                   cudaStream_t s);
+// In-place shift + per-cell counts on the plan's search grid.
+void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
-void launch_owner_scatter(uint64_t P, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+// Device-driven emission: P is read from stats->pairs. If P exceeds the
+// scratch (pair_cap) or out_cap nothing is written and stats->np_n = 0, else
+// stats->np_n = P.
+void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
-void launch_segsort_big(uint64_t nbig, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 
 // Reference-grid bin list (the reference's internal sorted (bin, body) list).
 void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s);
@@ -127,14 +139,27 @@ struct NpScratch {
 	uint64_t *status;       // look-back tiles of the flag scan
 	uint32_t *ticket;
 	uint32_t *err;
+	uint32_t *order;        // P: pair indices grouped by (type A, type B)
+	uint32_t *classes;      // 2 * kNpClasses counters + the work-queue counter (zeroed per call)
 };
+constexpr int kNpClasses = 64;  // 7 x 7 shape-type combinations + one for invalid keys
 
 // Pair indices >= n and body ids >= nb set kErrBadIndex in *sc.err; such a
-// pair is reported as no contact.
-void launch_mpr(uint64_t P, uint64_t n, const int32_t *T, const float *A, const float *B, const float *C,
-                const float *R, const uint32_t *ID, uint64_t nb, const uint8_t *active, const float *pos,
-                const float *rot, float envelope, const long long *pairs, const NpScratch &sc, cudaStream_t s);
-void launch_np_compact(uint64_t P, const NpScratch &sc, long long *pairs, float *norm, float *cpta, float *cptb,
-                       float *depth, int32_t *bids, cudaStream_t s);
+// pair is reported as no contact. precision: 0 exact (the reference's FP64
+// arithmetic), 1 fp64 (pair-local frame), 2 mixed (FP32 support maps).
+// P_cap: host bound on the pair count; with P_dev the count is min(P_cap,
+// *P_dev), read on the device. P_hint sizes the persistent grid.
+void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, const int32_t *T, const float *A,
+                const float *B, const float *C, const float *R, const uint32_t *ID, uint64_t nb,
+                const uint8_t *active, const float *pos, const float *rot, float envelope, const long long *pairs,
+                const NpScratch &sc, int precision, uint64_t P_hint, cudaStream_t s);
+// The exact variant lives in its own -fmad=false translation unit.
+void launch_mpr_exact(unsigned grid, uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, const int32_t *T,
+                      const float *A, const float *B, const float *C, const float *R, const uint32_t *ID, uint64_t nb,
+                      const uint8_t *active, const float *pos, const float *rot, float envelope,
+                      const long long *pairs, const NpScratch &sc, cudaStream_t s);
+void launch_np_compact(uint64_t P_cap, const unsigned long long *P_dev, const NpScratch &sc, long long *pairs,
+                       float *norm, float *cpta, float *cptb, float *depth, int32_t *bids,
+                       unsigned long long *contacts_out, cudaStream_t s);
 
 }  // namespace cc

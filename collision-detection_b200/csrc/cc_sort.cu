@@ -12,7 +12,8 @@ constexpr uint64_t kScanTile = (uint64_t)kScanNT * kScanIPT;
 
 template <class OutT>
 __global__ void __launch_bounds__(kScanNT) k_scan(const uint32_t *__restrict__ in, uint64_t n_host,
-                                                  const uint32_t *__restrict__ n_dev, OutT *__restrict__ out,
+                                                  const unsigned long long *__restrict__ n_dev,
+                                                  OutT *__restrict__ out,
                                                   unsigned long long *total_out, uint64_t *status, uint32_t *ticket,
                                                   uint32_t *err) {
 	__shared__ uint32_t s_tile;
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(kScanNT) k_scan(const uint32_t *__restrict__ i
 
 template <class OutT>
 void scan_impl(const uint32_t *in, uint64_t n, OutT *out, uint64_t *status, uint32_t *ticket, uint32_t *err,
-               cudaStream_t s, const uint32_t *n_dev = nullptr, unsigned long long *total_out = nullptr) {
+               cudaStream_t s, const unsigned long long *n_dev = nullptr, unsigned long long *total_out = nullptr) {
 	const uint64_t tiles = n / kScanTile + 1;
 	cudaMemsetAsync(status, 0, tiles * sizeof(uint64_t), s);
 	cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s);
@@ -73,11 +74,13 @@ void scan_impl(const uint32_t *in, uint64_t n, OutT *out, uint64_t *status, uint
 size_t scan_tiles(uint64_t n) { return (size_t)(n / kScanTile + 1); }
 
 void launch_scan_u32_to_u64(const uint32_t *in, uint64_t n, unsigned long long *out, uint64_t *status,
-                            uint32_t *ticket, uint32_t *err, cudaStream_t s) {
-	scan_impl(in, n, out, status, ticket, err, s);
+                            uint32_t *ticket, uint32_t *err, cudaStream_t s, const unsigned long long *n_dev,
+                            unsigned long long *total_out) {
+	scan_impl(in, n, out, status, ticket, err, s, n_dev, total_out);
 }
 void launch_scan_u32_to_u32(const uint32_t *in, uint64_t n, uint32_t *out, uint64_t *status, uint32_t *ticket,
-                            uint32_t *err, cudaStream_t s, const uint32_t *n_dev, unsigned long long *total_out) {
+                            uint32_t *err, cudaStream_t s, const unsigned long long *n_dev,
+                            unsigned long long *total_out) {
 	scan_impl(in, n, out, status, ticket, err, s, n_dev, total_out);
 }
 

@@ -162,8 +162,8 @@ extern "C" cc_status cc_broadphase_noalloc(uint64_t n, float *aabb, int gx, int 
 	// everything that accumulates starts at zero (the array keeps the last call's contents)
 	NA_CUDA(cudaMemsetAsync(b.stats, 0, sizeof(DevStats), s));
 	NA_CUDA(cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * b.g_max, s));
-	launch_bounds(n, aabb, b.stats, s);
-	launch_count(n, aabb, gp, grid, b, s);
+	launch_bounds(n, aabb, b.stats, gp, grid, s);  // + the grid plan
+	launch_count(n, aabb, b, s);
 	launch_scan_cells(b, b.g_max, s);
 	NA_CUDA(cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * b.g_max, s));
 	launch_scatter(n, aabb, b, s);
@@ -182,12 +182,11 @@ extern "C" cc_status cc_broadphase_noalloc(uint64_t n, float *aabb, int gx, int 
 	if (P == 0) return CC_OK;
 
 	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
-	launch_owner_scatter(P, out, b, s);
+	launch_owner_scatter(pairs_cap, out, b, s);
 	launch_segsort(n, out, b, s);
+	launch_segsort_big(out, b, s);
 	NA_CUDA(cudaGetLastError());
 	if ((st = read_stats(b.stats, s)) != CC_OK) return st;
-	const uint64_t nbig = g_host_stats.big_segments < kBigCap ? g_host_stats.big_segments : kBigCap;
-	if (nbig) launch_segsort_big(nbig, out, b, s);
 	if (g_host_stats.err & kErrSegmentTooLong) {
 		int bits = 1;
 		while (bits < 32 && ((uint64_t)1 << bits) < n) bits++;

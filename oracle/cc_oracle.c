@@ -23,6 +23,7 @@
 #include <string.h>
 
 #define CCO_API __attribute__((visibility("default")))
+#define CCO_API_DEFINED
 
 /* shape_type, collision_detection.h:57 */
 enum { CCO_SPHERE, CCO_ELLIPSOID, CCO_BOX, CCO_CYLINDER, CCO_RECT, CCO_CONE, CCO_TRIANGLEMESH };

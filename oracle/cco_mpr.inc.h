@@ -128,6 +128,12 @@ static V3 F(support)(int type, V3 A, V3 B, V3 C, Q4 R, V3 b) {
 #define SUP_B(d) F(support)(tB, BX, BY, BZ, BR, (d))
 #define SWAP3(a, b) do { V3 t_ = (a); (a) = (b); (b) = t_; } while (0)
 
+/* Optional iteration record (test diagnostics): when set, each MPR call
+ * stores phase1 * 1000 + phase2 at the sink's cursor. */
+static int32_t *F(g_iter_sink) = 0;
+static uint64_t F(g_iter_n) = 0;
+#define CCO_ITERS(p1, p2) do { if (F(g_iter_sink)) F(g_iter_sink)[F(g_iter_n)++] = (p1) * 1000 + (p2); } while (0)
+
 /* Minkowski portal refinement: Narrowphase.cu:122-314. Returns hit. */
 static int F(mpr)(int tA, V3 AX, V3 AY, V3 AZ, Q4 AR, int tB, V3 BX, V3 BY, V3 BZ, Q4 BR, V3 *rn, V3 *pt, CCO_R *depth) {
 	V3 v01 = F(center)(tA, AX, AY, AZ), v02 = F(center)(tB, BX, BY, BZ);
@@ -158,11 +164,11 @@ static int F(mpr)(int tA, V3 AX, V3 AY, V3 AZ, Q4 AR, int tB, V3 BX, V3 BY, V3 B
 	int hit = 0, phase1 = 0, phase2 = 0;
 	const int max_iterations = 34;
 	for (;;) {
-		if (phase1 > max_iterations) return 0;
+		if (phase1 > max_iterations) { CCO_ITERS(phase1, phase2); return 0; }
 		phase1++;
 		v31 = SUP_A(F(neg)(n)); v32 = SUP_B(n);
 		v3 = F(sub)(v32, v31);
-		if (F(dot)(v3, n) <= 0.0) return 0;
+		if (F(dot)(v3, n) <= 0.0) { CCO_ITERS(phase1, phase2); return 0; }
 		if (F(dot)(F(cross)(v1, v3), v0) < 0.0) {
 			v2 = v3; v21 = v31; v22 = v32;
 			n = F(cross)(F(sub)(v1, v0), F(sub)(v3, v0));
@@ -202,6 +208,7 @@ static int F(mpr)(int tA, V3 AX, V3 AY, V3 AZ, Q4 AR, int tB, V3 BX, V3 BY, V3 B
 					*pt = F(muls)(F(muls)(F(add)(p, q), inv), (CCO_R).5);
 					*rn = F(normalize)(n);
 				}
+				CCO_ITERS(phase1, phase2);
 				return hit;
 			}
 			if (F(dot)(F(cross)(v4, v1), v0) < 0) {
@@ -217,6 +224,10 @@ static int F(mpr)(int tA, V3 AX, V3 AY, V3 AZ, Q4 AR, int tB, V3 BX, V3 BY, V3 B
 #undef SUP_A
 #undef SUP_B
 #undef SWAP3
+#undef CCO_ITERS
+
+CCO_API void F(cco_iter_sink)(int32_t *buf) { F(g_iter_sink) = buf; F(g_iter_n) = 0; }
+CCO_API uint64_t F(cco_iter_count)(void) { return F(g_iter_n); }
 
 static inline V3 F(ld3)(const float *p, uint64_t i) { return F(v3)(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
 static inline Q4 F(ld4)(const float *p, uint64_t i) {

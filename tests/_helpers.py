@@ -45,9 +45,13 @@ def contact_errors(gpu, ref, scale):
     gn, rn = np.asarray(gpu["norm"], np.float64)[gi], ref["norm"][ri]
     out["normal"] = np.linalg.norm(gn - rn, axis=1)
     out["depth"] = np.abs(np.asarray(gpu["depth"], np.float64)[gi] - ref["depth"][ri]) / scale
+    # contact points are float32 world coordinates: errors relative to the
+    # point's magnitude (what a float32 output can resolve), at least `scale`
     pa = np.linalg.norm(np.asarray(gpu["cpta"], np.float64)[gi] - ref["cpta"][ri], axis=1)
     pb = np.linalg.norm(np.asarray(gpu["cptb"], np.float64)[gi] - ref["cptb"][ri], axis=1)
-    out["point"] = np.maximum(pa, pb) / scale
+    mag = np.maximum(np.maximum(np.linalg.norm(ref["cpta"][ri], axis=1), np.linalg.norm(ref["cptb"][ri], axis=1)),
+                     scale)
+    out["point"] = np.maximum(pa, pb) / mag
     out["only_gpu"] = np.setdiff1d(gk, rk)
     out["only_ref"] = np.setdiff1d(rk, gk)
     return out

@@ -1,11 +1,15 @@
 """GPU narrowphase against the FP64 MPR oracle (the reference's
 CollideAndFindPoint restated in double) and the pipeline entry points.
 
-Tolerances (written here, measured on B200): on pairs both report as
-contacts, unit normals agree to NORMAL_TOL (max) / NORMAL_P99 (99th pct),
-depths and contact points to DEPTH_TOL / POINT_TOL in units of the pair's
-length scale (the larger shape size). Contacts reported by only one side
-must be grazing (|depth| below GRAZE of the length scale)."""
+Errors are measured on the pairs both report as contacts: unit-normal
+difference, depth difference in units of the scene's largest shape size,
+contact-point difference relative to the point's magnitude (the outputs are
+float32 world coordinates).
+
+* exact mode (default): the contact set must be identical and every error at
+  float32 output rounding (EXACT_TOL).
+* fp64 / mixed modes: max and p99 bounds measured on B200 at the 1M scene,
+  with margin (FAST_BOUNDS)."""
 import numpy as np
 import pytest
 import torch
@@ -16,31 +20,30 @@ from collide_b200 import scenes as S
 
 pytestmark = pytest.mark.gpu
 
-NORMAL_TOL, NORMAL_P99 = 1e-3, 1e-5
-DEPTH_TOL, POINT_TOL = 1e-3, 1e-3
-DEPTH_P99, POINT_P99 = 1e-5, 1e-5
-GRAZE = 1e-4
+EXACT_TOL = dict(normal=1e-6, depth=1e-6, point=1e-6)
+FAST_BOUNDS = {  # (max, p99)
+    "fp64": dict(normal=(2e-2, 5e-5), depth=(5e-3, 5e-6), point=(1e-5, 1e-6)),
+    "mixed": dict(normal=(5e-2, 2e-3), depth=(5e-3, 2e-4), point=(1e-4, 1e-6)),
+}
 
 
-def run_np(cb, scene, pairs, envelope=0.0):
+def run_np(cb, scene, pairs, envelope=0.0, precision="exact"):
     ds = cb.DeviceScene(scene)
     pk = torch.from_numpy(np.ascontiguousarray(pairs, np.int64)).cuda()
-    npc = cb.Narrowphase()
+    ctx = cb.Context()
+    ctx.set_narrowphase_precision(precision)
+    npc = cb.Narrowphase(ctx)
     npc.SetCollisionEnvelope(envelope)
     norm, ca, cb_, d, ids, k = npc.DoNarrowphase(ds.T, ds.A, ds.B, ds.C, ds.R, ds.ID, ds.active, ds.pos, ds.rot, pk)
     return dict(norm=norm.cpu().numpy(), cpta=ca.cpu().numpy(), cptb=cb_.cpu().numpy(), depth=d.cpu().numpy(),
                 bids=ids.cpu().numpy(), n=k, pairs=pk.cpu().numpy(), contact_pairs=pk[:k].cpu().numpy())
 
 
-def check_errors(err, depth_ref_only, depth_gpu_only):
+def check_exact(err):
     assert err["n_common"] > 0
-    assert err["normal"].max() <= NORMAL_TOL, err["normal"].max()
-    assert np.quantile(err["normal"], 0.99) <= NORMAL_P99
-    assert err["depth"].max() <= DEPTH_TOL
-    assert np.quantile(err["depth"], 0.99) <= DEPTH_P99
-    assert err["point"].max() <= POINT_TOL
-    assert np.quantile(err["point"], 0.99) <= POINT_P99
-    assert np.all(np.abs(depth_ref_only) <= GRAZE) and np.all(np.abs(depth_gpu_only) <= GRAZE)
+    assert len(err["only_gpu"]) == 0 and len(err["only_ref"]) == 0, (err["only_gpu"], err["only_ref"])
+    for k, tol in EXACT_TOL.items():
+        assert err[k].max() <= tol, (k, err[k].max())
 
 
 def scale_of(scene):
@@ -54,21 +57,28 @@ def test_narrowphase_vs_fp64_golden(cb, name):
     r = run_np(cb, s, g["pairs"])
     ref = dict(n=len(g["np_f64_depth"]), pairs=g["np_f64_pairs"], norm=g["np_f64_norm"], depth=g["np_f64_depth"],
                cpta=g["np_f64_cpta"], cptb=g["np_f64_cptb"])
-    err = contact_errors(r, ref, scale_of(s))
-    ro = np.isin(ref["pairs"][: ref["n"]], err["only_ref"])
-    go = np.isin(r["contact_pairs"], err["only_gpu"])
-    check_errors(err, ref["depth"][ro] / scale_of(s), r["depth"][go] / scale_of(s))
+    check_exact(contact_errors(r, ref, scale_of(s)))
 
 
-def test_narrowphase_1m_mixed_vs_fp64(cb):
+@pytest.fixture(scope="module")
+def scene_1m():
     m = S.mixed_slab(1 << 20, seed=0)
     _, p = O.broadphase(O.aabb(m), (200, 200, 10))
-    r = run_np(cb, m, p)
-    ref = O.narrowphase(m, p, 0.0, "f64")
-    err = contact_errors(r, ref, scale_of(m))
-    ro = np.isin(ref["pairs"][: ref["n"]], err["only_ref"])
-    go = np.isin(r["contact_pairs"], err["only_gpu"])
-    check_errors(err, ref["depth"][ro] / scale_of(m), r["depth"][go] / scale_of(m))
+    return m, p, O.narrowphase(m, p, 0.0, "f64")
+
+
+def test_narrowphase_1m_exact_equals_fp64_oracle(cb, scene_1m):
+    m, p, ref = scene_1m
+    check_exact(contact_errors(run_np(cb, m, p), ref, scale_of(m)))
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_narrowphase_1m_fast_modes_within_bounds(cb, scene_1m, mode):
+    m, p, ref = scene_1m
+    err = contact_errors(run_np(cb, m, p, precision=mode), ref, scale_of(m))
+    assert err["n_common"] >= 0.999 * ref["n"]
+    for k, (mx, p99) in FAST_BOUNDS[mode].items():
+        assert err[k].max() <= mx and np.quantile(err[k], 0.99) <= p99, (k, err[k].max(), np.quantile(err[k], .99))
 
 
 def test_contacts_come_first_in_pair_order(cb):
