@@ -4,6 +4,8 @@
 // extent sums and input validation) so the pipeline reads each shape once.
 // Compiled with -fmad=false: results are bit-identical to the reference's
 // host build.
+#include <algorithm>
+
 #include "cc_common.cuh"
 #include "cc_internal.h"
 #include "cc_math.cuh"
@@ -39,8 +41,14 @@ __device__ __forceinline__ bool shape_aabb(uint64_t i, const int32_t *T, const f
 	const float3 position = ld3(pos, id);
 	const float4 brot = ld4(rot, id);
 	const float4 lrot = ld4(R, i);
+	// A zero local offset rotates to (+-0, +-0, +-0) and an identity local
+	// rotation leaves body_rot unchanged up to the sign of zero terms; neither
+	// sign survives (p +- r rounds the same, |R| drops it), so skipping that
+	// arithmetic gives bit-identical boxes.
+	const bool a_zero = a.x == 0.f && a.y == 0.f && a.z == 0.f;
+	const bool r_ident = lrot.x == 1.f && lrot.y == 0.f && lrot.z == 0.f && lrot.w == 0.f;
 	if (type == SPHERE) {  // :96-98, ComputeAABBSphere :11-14
-		const float3 p = qrot(a, brot) + position;
+		const float3 p = a_zero ? position : qrot(a, brot) + position;
 		const float3 r = f3(b.x, b.x, b.x);
 		mn = p - r;
 		mx = p + r;
@@ -57,9 +65,9 @@ __device__ __forceinline__ bool shape_aabb(uint64_t i, const int32_t *T, const f
 		return true;
 	}
 	if (type == ELLIPSOID || type == BOX || type == CYLINDER) {  // :108-109, ComputeAABBBox :25-35
-		const Rot m = rot_rows(qmul(brot, lrot));
+		const Rot m = rot_rows(r_ident ? brot : qmul(brot, lrot));
 		const float3 half = f3(dot(abs3(m.r0), b), dot(abs3(m.r1), b), dot(abs3(m.r2), b));
-		const float3 p = qrot(a, brot) + position;
+		const float3 p = a_zero ? position : qrot(a, brot) + position;
 		mn = p - half;
 		mx = p + half;
 		return true;
@@ -67,6 +75,8 @@ __device__ __forceinline__ bool shape_aabb(uint64_t i, const int32_t *T, const f
 	return false;
 }
 
+// Persistent: each thread walks shapes blockIdx*kNT + tid, step gridDim*kNT,
+// keeping its share of the bounds in registers, so the block reduces once.
 template <bool kStats>
 __global__ void __launch_bounds__(kNT) k_aabb(uint64_t n, const int32_t *__restrict__ T, const float *__restrict__ A,
                                                const float *__restrict__ B, const float *__restrict__ C,
@@ -74,10 +84,12 @@ __global__ void __launch_bounds__(kNT) k_aabb(uint64_t n, const int32_t *__restr
                                                uint64_t nb, const float *__restrict__ pos,
                                                const float *__restrict__ rot, float *__restrict__ aabb,
                                                DevStats *stats, uint32_t *err, PlanArgs pa) {
-	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
-	float3 mn = f3(INFINITY, INFINITY, INFINITY), mx = f3(-INFINITY, -INFINITY, -INFINITY);
+	float3 bmn = f3(INFINITY, INFINITY, INFINITY), bmx = f3(-INFINITY, -INFINITY, -INFINITY);
+	float3 esum = f3(0.f, 0.f, 0.f);  // extent sum for the grid tuner's mean box size
 	bool have = false;
-	if (i < n) {
+	uint32_t e = 0, ecnt = 0;
+	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kNT) {
+		float3 mn, mx;
 		if (shape_aabb(i, T, A, B, C, R, ID, nb, pos, rot, mn, mx, err)) {
 			float *o = aabb + 3 * i, *o2 = aabb + 3 * (i + n);
 			o[0] = mn.x; o[1] = mn.y; o[2] = mn.z;
@@ -87,9 +99,23 @@ __global__ void __launch_bounds__(kNT) k_aabb(uint64_t n, const int32_t *__restr
 			mn = f3(o[0], o[1], o[2]);
 			mx = f3(o2[0], o2[1], o2[2]);
 		}
-		have = true;
+		if constexpr (kStats) {
+			if (!finite3(mn) || !finite3(mx)) e |= kErrNonFinite;
+			if (mn.x > mx.x || mn.y > mx.y || mn.z > mx.z) e |= kErrInverted;
+			bmn = f3(fminf(bmn.x, mn.x), fminf(bmn.y, mn.y), fminf(bmn.z, mn.z));
+			bmx = f3(fmaxf(bmx.x, mx.x), fmaxf(bmx.y, mx.y), fmaxf(bmx.z, mx.z));
+			esum = esum + (mx - mn);
+			ecnt++;
+			have = true;
+		}
 	}
-	if constexpr (kStats) accumulate_stats<kNT>(mn, mx, have, stats, pa);
+	if constexpr (kStats) accumulate_stats<kNT>(bmn, bmx, have, stats, pa, e, esum, ecnt);
+}
+template <class K>
+int resident_blocks(K kernel) {
+	int b = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kNT, 0) != cudaSuccess || b < 1) b = 1;
+	return b;
 }
 }  // namespace
 
@@ -97,7 +123,10 @@ void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, c
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
                  uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s) {
 	if (n == 0) return;
-	const unsigned blocks = (unsigned)((n + kNT - 1) / kNT);
+	// persistent grid: as many blocks as are resident at once
+	static const int per_sm[2] = {resident_blocks(k_aabb<false>), resident_blocks(k_aabb<true>)};
+	const unsigned blocks =
+	    (unsigned)std::min<uint64_t>((n + kNT - 1) / kNT, (uint64_t)kNumSMs * per_sm[stats ? 1 : 0]);
 	PlanArgs pa;
 	pa.gp = gp;
 	pa.gx = grid ? grid[0] : 1;

@@ -42,8 +42,49 @@ namespace {
 constexpr int kNT = 256;
 
 __device__ __forceinline__ float3 ld3p(const float *p, uint64_t i) { return f3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
-__device__ __forceinline__ void st3p(float *p, uint64_t i, float3 v) {
-	p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z;
+
+// A block's kNT boxes, staged through shared memory with 16-byte loads: the
+// min corners of boxes [i0, i0+kNT) are 3*kNT contiguous floats at aabb+3*i0
+// and the max corners the same at aabb+3*(n+i0). stage[0..3kNT) = mins,
+// stage[3kNT..6kNT) = maxs. Vector accesses are used when both runs are
+// 16-byte aligned and complete; otherwise scalar ones.
+__device__ __forceinline__ bool tile_vec_ok(const float *aabb, uint64_t n, uint64_t i0) {
+	return i0 + kNT <= n && ((reinterpret_cast<uintptr_t>(aabb + 3 * i0) & 15) == 0) &&
+	       ((reinterpret_cast<uintptr_t>(aabb + 3 * (n + i0)) & 15) == 0);
+}
+__device__ __forceinline__ void load_tile_aabb(const float *__restrict__ aabb, uint64_t n, uint64_t i0, float *stage) {
+	if (tile_vec_ok(aabb, n, i0)) {
+		const float4 *lo = reinterpret_cast<const float4 *>(aabb + 3 * i0);
+		const float4 *hi = reinterpret_cast<const float4 *>(aabb + 3 * (n + i0));
+		float4 *st = reinterpret_cast<float4 *>(stage);
+		for (int k = threadIdx.x; k < 3 * kNT / 4; k += kNT) {
+			st[k] = lo[k];
+			st[3 * kNT / 4 + k] = hi[k];
+		}
+	} else {
+		const uint64_t m = i0 < n ? min((uint64_t)kNT, n - i0) : 0;
+		for (int k = threadIdx.x; k < 3 * (int)m; k += kNT) {
+			stage[k] = aabb[3 * i0 + k];
+			stage[3 * kNT + k] = aabb[3 * (n + i0) + k];
+		}
+	}
+}
+__device__ __forceinline__ void store_tile_aabb(float *__restrict__ aabb, uint64_t n, uint64_t i0, const float *stage) {
+	if (tile_vec_ok(aabb, n, i0)) {
+		float4 *lo = reinterpret_cast<float4 *>(aabb + 3 * i0);
+		float4 *hi = reinterpret_cast<float4 *>(aabb + 3 * (n + i0));
+		const float4 *st = reinterpret_cast<const float4 *>(stage);
+		for (int k = threadIdx.x; k < 3 * kNT / 4; k += kNT) {
+			lo[k] = st[k];
+			hi[k] = st[3 * kNT / 4 + k];
+		}
+	} else {
+		const uint64_t m = i0 < n ? min((uint64_t)kNT, n - i0) : 0;
+		for (int k = threadIdx.x; k < 3 * (int)m; k += kNT) {
+			aabb[3 * i0 + k] = stage[k];
+			aabb[3 * (n + i0) + k] = stage[3 * kNT + k];
+		}
+	}
 }
 
 // Search-grid cell of a shifted coordinate: monotone in v.
@@ -78,22 +119,29 @@ __global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restr
 		mn = ld3p(aabb, i);
 		mx = ld3p(aabb, i + n);
 	}
-	accumulate_stats<kNT>(mn, mx, have, stats, pa);
+	accumulate_stats_one<kNT>(mn, mx, have, stats, pa);
 }
 
 __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, const DevStats *stats,
                                                 uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count) {
 	__shared__ Plan sp;
+	__shared__ float stage[6 * kNT];
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	if (!sp.valid) return;  // invalid input: nothing is modified
-	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
+	load_tile_aabb(aabb, n, i0, stage);
+	__syncthreads();
+	// in-place shift by fabs(min) (:382-386), element by element
+	for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
+	__syncthreads();
+	store_tile_aabb(aabb, n, i0, stage);
+	const uint64_t i = i0 + threadIdx.x;
 	if (i >= n) return;
-	const float3 o = f3(sp.origin[0], sp.origin[1], sp.origin[2]);
-	const float3 mn = ld3p(aabb, i) + o, mx = ld3p(aabb, i + n) + o;  // :382-386
-	st3p(aabb, i, mn);
-	st3p(aabb, i + n, mx);
+	const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
+	const float *hs = stage + 3 * kNT;
+	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
 	owner_count[i] = 0u;
 	const CellRange r = cell_range(sp, mn, mx);
 	for (int z = r.c0[2]; z <= r.c1[2]; z++)
@@ -102,17 +150,23 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
 				atomicAdd(&cell_count[(uint32_t)x + (uint32_t)sp.dim[0] * ((uint32_t)y + (uint32_t)sp.dim[1] * z)], 1u);
 }
 
+// Cell-ordered entries: one thread per body, a cursor atomic per covered cell.
 __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
                                                   const uint32_t *__restrict__ cell_start,
                                                   uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
                                                   uint64_t cap, uint32_t *err) {
 	__shared__ Plan sp;
+	__shared__ float stage[6 * kNT];
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
+	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
+	load_tile_aabb(aabb, n, i0, stage);
 	__syncthreads();
-	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
+	const uint64_t i = i0 + threadIdx.x;
 	if (!sp.valid || i >= n) return;
-	const float3 mn = ld3p(aabb, i), mx = ld3p(aabb, i + n);
+	const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
+	const float *hs = stage + 3 * kNT;
+	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
 	const CellRange r = cell_range(sp, mn, mx);
 	bool over = false;
 	for (int z = r.c0[2]; z <= r.c1[2]; z++)
@@ -131,30 +185,42 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 }
 
 // One lane per entry; each lane tests its entry against the later entries of
-// the same cell. Loops are warp-uniform so the emission can be warp-aggregated.
+// the same cell. A warp's 32 entries and the kWin - 32 that follow them are
+// staged in shared memory with coalesced 16-byte loads (cells hold a handful
+// of entries, so the inner loop almost never leaves the window); loops are
+// warp-uniform so the emission can be warp-aggregated.
+constexpr int kWin = 96;
+
 __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const uint32_t *__restrict__ cell_start,
                                                     const float4 *__restrict__ entries,
                                                     uint64_t entry_cap, uint32_t *__restrict__ owner_count,
                                                     unsigned long long *__restrict__ pairs, uint64_t pair_cap,
                                                     unsigned long long *pair_counter) {
 	__shared__ Plan sp;
+	__shared__ float4 win_all[kNT / 32][2 * kWin];
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	if (!sp.valid) return;
+	float4 *win = win_all[threadIdx.x >> 5];
 	const uint64_t E = min((uint64_t)stats->entries, entry_cap);
 	const uint32_t lane = threadIdx.x & 31;
 	const uint32_t lt = (1u << lane) - 1u;
 	const uint64_t warps = (uint64_t)gridDim.x * (kNT / 32);
 	for (uint64_t base = ((uint64_t)blockIdx.x * (kNT / 32) + (threadIdx.x >> 5)) * 32; base < E; base += warps * 32) {
+		// stage entries [base, base + kWin) of this warp
+		const uint32_t nwin = (uint32_t)min((uint64_t)kWin, E - base);
+		__syncwarp();
+		for (uint32_t k = lane; k < 2 * nwin; k += 32) win[k] = entries[2 * base + k];
+		__syncwarp();
 		const uint64_t e = base + lane;
 		const bool valid = e < E;
 		float4 alo = make_float4(0.f, 0.f, 0.f, 0.f), ahi = alo;
 		int my_n = 0;
 		int cx = 0, cy = 0, cz = 0;
 		if (valid) {
-			alo = entries[2 * e];
-			ahi = entries[2 * e + 1];
+			alo = win[2 * lane];
+			ahi = win[2 * lane + 1];
 			const uint32_t pc = __float_as_uint(ahi.w);
 			cx = pc & 1023; cy = (pc >> 10) & 1023; cz = (pc >> 20) & 1023;
 			const uint32_t c = (uint32_t)cx + (uint32_t)sp.dim[0] * ((uint32_t)cy + (uint32_t)sp.dim[1] * cz);
@@ -174,8 +240,16 @@ __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const 
 			unsigned long long key = 0;
 			uint32_t other_owner = 0xffffffffu;
 			if (t < my_n) {
-				const uint64_t q = e + 1 + t;
-				const float4 blo = entries[2 * q], bhi = entries[2 * q + 1];
+				const uint32_t loc = lane + 1 + t;  // position of the partner in the window
+				float4 blo, bhi;
+				if (loc < nwin) {
+					blo = win[2 * loc];
+					bhi = win[2 * loc + 1];
+				} else {
+					const uint64_t q = e + 1 + t;
+					blo = entries[2 * q];
+					bhi = entries[2 * q + 1];
+				}
 				if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
 				    blo.z <= ahi.z) {
 					const bool hx = ax || cell_of(blo.x, sp.lo[0], sp.inv[0], sp.dim[0]) == cx;
@@ -407,8 +481,8 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
 }
 
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
-	k_scatter<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries, b.entry_cap,
-	                                        &b.stats->err);
+	if (n) k_scatter<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
+	                                               b.entry_cap, &b.stats->err);
 }
 
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s) {

@@ -28,7 +28,8 @@ struct DevStats {
 	uint32_t bmax[3];      // f2ord(max) accumulated with atomicMax (0 = neutral)
 	uint32_t err;          // DeviceError bits
 	uint32_t max_bin;      // largest reference bin id emitted (bin-list path)
-	double ext_sum[3];     // sum of AABB extents per axis (tuner input)
+	double ext_sum[3];     // sum of sampled AABB extents per axis (tuner input)
+	unsigned long long ext_count;  // number of sampled boxes
 	unsigned long long pairs;     // unique pairs emitted by the tile test (may exceed capacity)
 	unsigned long long entries;   // (cell, body) entries of the search grid
 	unsigned long long ref_entries;

@@ -14,7 +14,7 @@ __device__ __forceinline__ bool finite3(float3 v) { return isfinite(v.x) && isfi
 // Grid parameters from the reduced bounds: the reference's shift and inverse
 // bin size (Broadphase.cu:377-381) and the search grid of the pair test.
 __device__ inline Plan make_plan(const uint32_t bmin_inv[3], const uint32_t bmax[3], uint32_t err,
-                                 const double ext_sum[3], const GridParams &gp, int gx, int gy, int gz, uint64_t n) {
+                                 const double ext_mean[3], const GridParams &gp, int gx, int gy, int gz, uint64_t n) {
 	Plan p;
 	const int grid[3] = {gx, gy, gz};
 	float mn[3], mx[3];
@@ -32,7 +32,7 @@ __device__ inline Plan make_plan(const uint32_t bmin_inv[3], const uint32_t bmax
 	for (int d = 0; d < 3; d++) {
 		const float hi = mx[d] + p.origin[d];
 		ext[d] = hi - p.lo[d];
-		mean_max = fmaxf(mean_max, (float)(ext_sum[d] / (double)(n ? n : 1)));
+		mean_max = fmaxf(mean_max, (float)ext_mean[d]);
 	}
 	int dim[3];
 	if (gp.user_dim[0] > 0) {
@@ -68,57 +68,64 @@ struct PlanArgs {
 	uint64_t n;
 };
 
-// Every thread of the block calls this once; `have` marks threads that own a
-// box. Block size NT (multiple of 32, <= 1024).
+// Every thread of the block calls this once with the bounds of the boxes it
+// saw (mn/mx; `have` false if none), its error bits, and the sum of those
+// boxes' extents (esum) over ecnt boxes for the grid tuner's mean extent.
+// Block size NT (multiple of 32, <= 1024).
 template <int NT>
 __device__ __forceinline__ void accumulate_stats(float3 mn, float3 mx, bool have, DevStats *stats,
-                                                 const PlanArgs &pa) {
-	uint32_t e = 0;
-	float3 ext = f3(0.f, 0.f, 0.f);
-	if (have) {
-		if (!finite3(mn) || !finite3(mx)) e |= kErrNonFinite;
-		if (mn.x > mx.x || mn.y > mx.y || mn.z > mx.z) e |= kErrInverted;
-		ext = mx - mn;
-	} else {
-		mn = f3(INFINITY, INFINITY, INFINITY);
-		mx = f3(-INFINITY, -INFINITY, -INFINITY);
+                                                 const PlanArgs &pa, uint32_t e, float3 esum, uint32_t ecnt) {
+	// warp reductions on order-preserving keys: one REDUX instruction each
+	uint32_t k[6];
+	k[0] = have ? f2ord(mn.x) : 0xffffffffu;
+	k[1] = have ? f2ord(mn.y) : 0xffffffffu;
+	k[2] = have ? f2ord(mn.z) : 0xffffffffu;
+	k[3] = have ? f2ord(mx.x) : 0u;
+	k[4] = have ? f2ord(mx.y) : 0u;
+	k[5] = have ? f2ord(mx.z) : 0u;
+#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		k[d] = __reduce_min_sync(0xffffffffu, k[d]);
+		k[d + 3] = __reduce_max_sync(0xffffffffu, k[d + 3]);
 	}
-	float v[6] = {mn.x, mn.y, mn.z, mx.x, mx.y, mx.z};
-	float es[3] = {ext.x, ext.y, ext.z};
+	e = __reduce_or_sync(0xffffffffu, e);
+	ecnt = __reduce_add_sync(0xffffffffu, ecnt);
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-		for (int d = 0; d < 3; d++) {
-			v[d] = fminf(v[d], __shfl_xor_sync(0xffffffffu, v[d], o));
-			v[d + 3] = fmaxf(v[d + 3], __shfl_xor_sync(0xffffffffu, v[d + 3], o));
-			es[d] += __shfl_xor_sync(0xffffffffu, es[d], o);
-		}
-		e |= __shfl_xor_sync(0xffffffffu, e, o);
+		esum.x += __shfl_xor_sync(0xffffffffu, esum.x, o);
+		esum.y += __shfl_xor_sync(0xffffffffu, esum.y, o);
+		esum.z += __shfl_xor_sync(0xffffffffu, esum.z, o);
 	}
-	__shared__ float sv[NT / 32][9];
-	__shared__ uint32_t se[NT / 32];
+	__shared__ uint32_t sk[NT / 32][6];
+	__shared__ float sext[NT / 32][3];
+	__shared__ uint32_t se[NT / 32], sc[NT / 32];
 	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 	if (l == 0) {
 #pragma unroll
-		for (int d = 0; d < 6; d++) sv[w][d] = v[d];
-#pragma unroll
-		for (int d = 0; d < 3; d++) sv[w][6 + d] = es[d];
+		for (int d = 0; d < 6; d++) sk[w][d] = k[d];
+		sext[w][0] = esum.x;
+		sext[w][1] = esum.y;
+		sext[w][2] = esum.z;
 		se[w] = e;
+		sc[w] = ecnt;
 	}
 	__syncthreads();
 	if (threadIdx.x < 3) {
 		const int d = threadIdx.x;
-		float lo = sv[0][d], hi = sv[0][d + 3];
+		uint32_t lo = sk[0][d], hi = sk[0][d + 3];
 		double s = 0.0;
+		uint32_t cnt = 0;
 		for (int ww = 0; ww < NT / 32; ww++) {
-			lo = fminf(lo, sv[ww][d]);
-			hi = fmaxf(hi, sv[ww][d + 3]);
-			s += (double)sv[ww][6 + d];
+			lo = min(lo, sk[ww][d]);
+			hi = max(hi, sk[ww][d + 3]);
+			s += (double)sext[ww][d];
+			cnt += sc[ww];
 		}
-		if (lo <= hi) {  // the block saw at least one box
-			atomicMax(&stats->bmin_inv[d], ~f2ord(lo));
-			atomicMax(&stats->bmax[d], f2ord(hi));
+		if (lo != 0xffffffffu) {  // the block saw at least one box
+			atomicMax(&stats->bmin_inv[d], ~lo);
+			atomicMax(&stats->bmax[d], hi);
 			atomicAdd(&stats->ext_sum[d], s);
+			if (d == 0) atomicAdd(&stats->ext_count, (unsigned long long)cnt);
 		}
 	} else if (threadIdx.x == 32) {
 		uint32_t ee = 0;
@@ -135,17 +142,30 @@ __device__ __forceinline__ void accumulate_stats(float3 mn, float3 mx, bool have
 	if (s_last && threadIdx.x == 0) {
 		__threadfence();
 		uint32_t bmin_inv[3], bmax[3];
-		double ext_sum[3];
+		double ext_mean[3];
+		const unsigned long long cnt = __ldcg(&stats->ext_count);
 		for (int d = 0; d < 3; d++) {
 			bmin_inv[d] = __ldcg(&stats->bmin_inv[d]);
 			bmax[d] = __ldcg(&stats->bmax[d]);
-			ext_sum[d] = __ldcg(&stats->ext_sum[d]);
+			ext_mean[d] = __ldcg(&stats->ext_sum[d]) / (double)(cnt ? cnt : 1);
 		}
 		const uint32_t err = __ldcg(&stats->err);
-		const Plan p = make_plan(bmin_inv, bmax, err, ext_sum, pa.gp, pa.gx, pa.gy, pa.gz, pa.n);
+		const Plan p = make_plan(bmin_inv, bmax, err, ext_mean, pa.gp, pa.gx, pa.gy, pa.gz, pa.n);
 		stats->plan = p;
 		stats->cells = p.G;
 	}
+}
+
+// One box per thread (k_bounds).
+template <int NT>
+__device__ __forceinline__ void accumulate_stats_one(float3 mn, float3 mx, bool have, DevStats *stats,
+                                                     const PlanArgs &pa) {
+	uint32_t e = 0;
+	if (have) {
+		if (!finite3(mn) || !finite3(mx)) e |= kErrNonFinite;
+		if (mn.x > mx.x || mn.y > mx.y || mn.z > mx.z) e |= kErrInverted;
+	}
+	accumulate_stats<NT>(mn, mx, have, stats, pa, e, have ? mx - mn : f3(0.f, 0.f, 0.f), have ? 1u : 0u);
 }
 
 }  // namespace cc
