@@ -93,6 +93,11 @@ class Context:
     def launches(self):
         return int(lib.cc_last_launch_count(self.h))
 
+    def set_graph_replay(self, on=True):
+        """Replay cc_collide as one CUDA graph once a configuration repeats
+        (default on; results are identical)."""
+        self.check(lib.cc_set_graph_replay(self.h, int(bool(on))), "cc_set_graph_replay")
+
     def set_profiling(self, on=True):
         self.check(lib.cc_set_profiling(self.h, int(bool(on))), "cc_set_profiling")
 

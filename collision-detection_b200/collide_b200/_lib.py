@@ -56,6 +56,7 @@ SIGNATURES = {
     "cc_collide_host": (I32, [P, P, I32, I32, I32, F32, P, P]),
     "cc_last_launch_count": (U64, [P]),
     "cc_set_profiling": (I32, [P, I32]),
+    "cc_set_graph_replay": (I32, [P, I32]),
     "cc_stage_count": (I32, []),
     "cc_stage_name": (ctypes.c_char_p, [I32]),
     "cc_stage_times": (I32, [P, ctypes.POINTER(ctypes.c_double), PU64, I32]),

@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(kNT) k_aabb(uint64_t n, const int32_t *__restr
                                                const float *__restrict__ R, const uint32_t *__restrict__ ID,
                                                uint64_t nb, const float *__restrict__ pos,
                                                const float *__restrict__ rot, float *__restrict__ aabb,
-                                               DevStats *stats, uint32_t *err, PlanArgs pa) {
+                                               DevStats *stats, uint32_t *err, PlanArgs pa, ZeroList zero) {
+	zero_ranges(zero);
 	float3 bmn = f3(INFINITY, INFINITY, INFINITY), bmx = f3(-INFINITY, -INFINITY, -INFINITY);
 	float3 esum = f3(0.f, 0.f, 0.f);  // extent sum for the grid tuner's mean box size
 	bool have = false;
@@ -121,7 +122,7 @@ int resident_blocks(K kernel) {
 
 void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
-                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s) {
+                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s, const ZeroList &zero) {
 	if (n == 0) return;
 	// persistent grid: as many blocks as are resident at once
 	static const int per_sm[2] = {resident_blocks(k_aabb<false>), resident_blocks(k_aabb<true>)};
@@ -134,9 +135,9 @@ void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, c
 	pa.gz = grid ? grid[2] : 1;
 	pa.n = n;
 	if (stats)
-		k_aabb<true><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, stats, err, pa);
+		k_aabb<true><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, stats, err, pa, zero);
 	else
-		k_aabb<false><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, pa);
+		k_aabb<false><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, pa, zero);
 }
 
 }  // namespace cc

@@ -111,7 +111,8 @@ __device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
 }
 
 __global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
-                                                 PlanArgs pa) {
+                                                 PlanArgs pa, ZeroList zero) {
+	zero_ranges(zero);
 	const uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x;
 	float3 mn = f3(0.f, 0.f, 0.f), mx = mn;
 	const bool have = i < n;
@@ -461,14 +462,14 @@ inline unsigned blocks_for(uint64_t n) { return (unsigned)((n + kNT - 1) / kNT);
 }  // namespace
 
 void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridParams &gp, const int grid[3],
-                   cudaStream_t s) {
+                   cudaStream_t s, const ZeroList &zero) {
 	PlanArgs pa;
 	pa.gp = gp;
 	pa.gx = grid[0];
 	pa.gy = grid[1];
 	pa.gz = grid[2];
 	pa.n = n;
-	if (n) k_bounds<<<blocks_for(n), kNT, 0, s>>>(n, aabb, stats, pa);
+	if (n) k_bounds<<<blocks_for(n), kNT, 0, s>>>(n, aabb, stats, pa, zero);
 }
 
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
@@ -476,8 +477,9 @@ void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
 }
 
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
+	// the scan leaves the counts zeroed: they are the scatter's cursors
 	launch_scan_u32_to_u32(b.cell_count, g_max, b.cell_start, b.status, b.ticket, &b.stats->err, s, &b.stats->cells,
-	                       &b.stats->entries);
+	                       &b.stats->entries, b.pre_zeroed, b.cell_count);
 }
 
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
@@ -494,7 +496,8 @@ void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cud
 }
 
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s) {
-	launch_scan_u32_to_u64(b.owner_count, n, b.owner_off, b.status, b.ticket, &b.stats->err, s);
+	launch_scan_u32_to_u64(b.owner_count, n, b.owner_off, b.status2 ? b.status2 : b.status,
+	                       b.ticket2 ? b.ticket2 : b.ticket, &b.stats->err, s, nullptr, nullptr, b.pre_zeroed);
 }
 
 void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -54,6 +55,23 @@ struct cc_ctx {
 	int last_dim[3] = {0, 0, 0};
 	uint64_t launches = 0;
 	int np_precision = CC_NP_EXACT;
+	// scratch generation: bumped whenever ensure() moves a buffer
+	uint64_t buf_gen = 0;
+	// look-back status regions (words) of the cell, owner and contact-flag
+	// scans, laid out back to back in `status`
+	uint64_t st_words[3] = {0, 0, 0};
+	// the current pass's first kernel zeroed the scan control words, the
+	// narrowphase class counters and the cell counts (ZeroList)
+	bool pass_zeroed = false;
+	// CUDA graph of the whole device pipeline (cc_collide), replayed while its
+	// configuration (GraphKey) is unchanged
+	cudaStream_t cap_stream = nullptr;
+	cudaGraphExec_t gexec = nullptr;
+	bool graph_off = false;
+	unsigned char gkey[sizeof(void *) * 40] = {};
+	unsigned char pending_key[sizeof(void *) * 40] = {};
+	bool have_pending = false;
+	uint64_t glaunches = 0;
 	// stage profiler
 	bool prof = false;
 	cudaEvent_t ev[2 * kMaxMarks] = {};
@@ -102,6 +120,7 @@ cc_status ensure(cc_ctx *c, Buf &b, size_t bytes) {
 	}
 	CC_CUDA(c, cudaMalloc(&b.p, nb));
 	b.bytes = nb;
+	c->buf_gen++;
 	return CC_OK;
 }
 
@@ -197,12 +216,20 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.pair_cap = c->pairs_tmp.bytes / sizeof(unsigned long long);
 	b.status = ptr<uint64_t>(c->status);
 	b.ticket = ptr<uint32_t>(c->ticket);
+	b.status2 = b.status + c->st_words[0];
+	b.ticket2 = b.ticket + 4;
 	b.big_list = ptr<uint32_t>(c->big_list);
 	b.big_cap = c->big_list.bytes / sizeof(uint32_t);
+	b.pre_zeroed = c->pass_zeroed;
 	return b;
 }
 
-size_t status_words_for(uint64_t n) { return scan_tiles(n) + 8; }
+// Words of a look-back status region for a scan over n elements (rounded to
+// 256 bytes).
+size_t status_words_for(uint64_t n) { return (scan_tiles(n) + 8 + 31) & ~size_t(31); }
+cc_status ensure_status(cc_ctx *c) {
+	return ensure(c, c->status, sizeof(uint64_t) * (c->st_words[0] + c->st_words[1] + c->st_words[2]));
+}
 
 // Narrowphase scratch for up to P pairs.
 cc_status np_prepare(cc_ctx *c, uint64_t P) {
@@ -218,7 +245,8 @@ cc_status np_prepare(cc_ctx *c, uint64_t P) {
 	CC_TRY(ensure(c, c->np_order, 4 * P));
 	CC_TRY(ensure(c, c->np_classes, (2 * kNpClasses + 32) * sizeof(uint32_t)));
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
-	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(P + 1)));
+	c->st_words[2] = std::max<uint64_t>(c->st_words[2], status_words_for(P + 1));
+	CC_TRY(ensure_status(c));
 	CC_TRY(ensure(c, c->ticket, 64));
 	return CC_OK;
 }
@@ -237,7 +265,9 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap) {
 	CC_TRY(ensure(c, c->entries, 2 * sizeof(float4) * e_guess));
 	const uint64_t p_guess = std::max<uint64_t>(c->last_P + c->last_P / 4, n / 4 + 1024);
 	CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * p_guess));
-	CC_TRY(ensure(c, c->status, sizeof(uint64_t) * status_words_for(std::max<uint64_t>(c->gp.g_max, n + 1))));
+	c->st_words[0] = std::max<uint64_t>(c->st_words[0], status_words_for(c->gp.g_max));
+	c->st_words[1] = std::max<uint64_t>(c->st_words[1], status_words_for(n + 1));
+	CC_TRY(ensure_status(c));
 	CC_TRY(ensure(c, c->ticket, 64));
 	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * std::max<uint64_t>(1024, n / 16)));
 	if (np_cap) CC_TRY(np_prepare(c, np_cap));
@@ -254,11 +284,12 @@ NpScratch np_scratch(cc_ctx *c) {
 	sc.pairs = ptr<unsigned long long>(c->np_pairs);
 	sc.flag = ptr<uint32_t>(c->np_flag);
 	sc.pos = ptr<unsigned long long>(c->np_pos);
-	sc.status = ptr<uint64_t>(c->status);
-	sc.ticket = ptr<uint32_t>(c->ticket);
+	sc.status = ptr<uint64_t>(c->status) + c->st_words[0] + c->st_words[1];
+	sc.ticket = ptr<uint32_t>(c->ticket) + 8;
 	sc.err = &ptr<DevStats>(c->stats)->err;
 	sc.order = ptr<uint32_t>(c->np_order);
 	sc.classes = ptr<uint32_t>(c->np_classes);
+	sc.pre_zeroed = c->pass_zeroed;
 	return sc;
 }
 
@@ -276,13 +307,24 @@ struct NpArgs {
 	int32_t *bids;
 };
 
+// Launch-shape hints from the previous call's sizes, rounded up to a power of
+// two so that a captured graph stays valid while sizes drift (every kernel
+// loops over the device-side count, so any launch shape is correct).
+uint64_t pow2ceil(uint64_t v) {
+	uint64_t p = 1;
+	while (p < v) p <<= 1;
+	return p;
+}
+uint64_t hint_E(const cc_ctx *c, uint64_t n) { return pow2ceil(std::max<uint64_t>(c->last_E, n)); }
+uint64_t hint_P(const cc_ctx *c) { return pow2ceil(std::max<uint64_t>(c->last_P, 1)); }
+
 // count .. owner scan: needs stats zeroed and the plan from the bounds pass.
 void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s) {
 	BpBuffers b = bp_buffers(c);
 	const uint32_t gmax = c->gp.g_max;
 	{
 		StageMark m(c, ST_COUNT, s);
-		cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
+		if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
 		launch_count(n, aabb, b, s);
 	}
 	{
@@ -291,12 +333,11 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s) {
 	}
 	{
 		StageMark m(c, ST_SCATTER, s);
-		cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
-		launch_scatter(n, aabb, b, s);
+		launch_scatter(n, aabb, b, s);  // the cell scan left the counts zeroed
 	}
 	{
 		StageMark m(c, ST_PAIR_TEST, s);
-		launch_pair_test(n, b, std::max<uint64_t>(c->last_E, n), s);
+		launch_pair_test(n, b, hint_E(c, n), s);
 	}
 	{
 		StageMark m(c, ST_SCAN_OWNER, s);
@@ -329,7 +370,7 @@ void enqueue_np(cc_ctx *c, const NpArgs &a, uint64_t P_cap, const unsigned long 
 		StageMark m(c, ST_MPR, s);
 		launch_mpr(P_cap, P_dev, a.n, a.T, a.A, a.B, a.C, a.R, a.ID, a.nb, a.active, a.pos, a.rot, a.envelope,
 		           reinterpret_cast<const long long *>(a.pairs), sc, c->np_precision,
-		           P_dev ? std::max<uint64_t>(c->last_P, 1) : P_cap, s);
+		           P_dev ? hint_P(c) : P_cap, s);
 	}
 	{
 		StageMark m(c, ST_NP_COMPACT, s);
@@ -456,19 +497,102 @@ cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, flo
 	CC_TRY(prepare(c, n, pairs_cap));
 	DevStats *d = ptr<DevStats>(c->stats);
 	const int grid[3] = {gx, gy, gz};
-	{
-		StageMark m(c, ST_AABB, s);
-		CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), s));
-		launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb, d, &d->err, c->gp,
-		            grid, s);
-	}
-	c->launches += 1;
-	enqueue_search(c, n, aabb, s);
 	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
-	enqueue_emit(c, n, out, pairs_cap, s);
 	const NpArgs a = {n, sc.nb, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, envelope,
 	                  pairs, norm, cpta, cptb, depth, bids};
-	enqueue_np(c, a, pairs_cap, &d->np_n, s);
+	// the AABB kernel also zeroes the pass's scan control words, class
+	// counters and cell counts
+	ZeroList zero;
+	zero.p[0] = ptr<uint32_t>(c->status);
+	zero.words[0] = 2 * (c->st_words[0] + c->st_words[1] + c->st_words[2]);
+	zero.p[1] = ptr<uint32_t>(c->ticket);
+	zero.words[1] = 16;
+	zero.p[2] = ptr<uint32_t>(c->np_classes);
+	zero.words[2] = 2 * kNpClasses + 1;
+	zero.p[3] = ptr<uint32_t>(c->cell_count);
+	zero.words[3] = c->gp.g_max;
+	for (int r = 0; r < 4; r++)
+		if (!zero.p[r]) zero.words[r] = 0;
+	auto enqueue_all = [&](cudaStream_t st) -> cc_status {
+		{
+			StageMark m(c, ST_AABB, st);
+			CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), st));
+			launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb, d, &d->err,
+			            c->gp, grid, st, zero);
+		}
+		c->launches += 1;
+		c->pass_zeroed = true;
+		enqueue_search(c, n, aabb, st);
+		enqueue_emit(c, n, out, pairs_cap, st);
+		enqueue_np(c, a, pairs_cap, &d->np_n, st);
+		c->pass_zeroed = false;
+		return CC_OK;
+	};
+	bool replayed = false;
+	if (!c->prof && !c->graph_off) {
+		// everything the captured launches depend on
+		struct {
+			uint64_t n, nb, pairs_cap, hE, hP, gen, st[3];
+			const void *p[18];
+			int dims[3], prec;
+			float env;
+			GridParams gp;
+		} k;
+		memset(&k, 0, sizeof(k));
+		k.n = n; k.nb = sc.nb; k.pairs_cap = pairs_cap; k.hE = hint_E(c, n); k.hP = hint_P(c); k.gen = c->buf_gen;
+		for (int r = 0; r < 3; r++) k.st[r] = c->st_words[r];
+		const void *ps[18] = {sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, aabb,
+		                      pairs, norm, cpta, cptb, depth, bids, nullptr, nullptr};
+		memcpy(k.p, ps, sizeof(ps));
+		k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.env = envelope; k.gp = c->gp;
+		static_assert(sizeof(k) <= sizeof(c->gkey), "graph key");
+		if (c->gexec && memcmp(&k, c->gkey, sizeof(k)) == 0) {
+			replayed = true;
+		} else if (c->have_pending && memcmp(&k, c->pending_key, sizeof(k)) == 0) {
+			// the same configuration twice in a row: capture it
+			if (!c->cap_stream) CC_CUDA(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+			const uint64_t l0 = c->launches;
+			cudaGraph_t g = nullptr;
+			cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed);
+			cc_status st = CC_OK;
+			if (e == cudaSuccess) {
+				st = enqueue_all(c->cap_stream);
+				e = cudaStreamEndCapture(c->cap_stream, &g);
+			}
+			if (st != CC_OK) {
+				if (g) cudaGraphDestroy(g);
+				c->launches = l0;
+				c->have_pending = false;
+				return st;
+			}
+			c->glaunches = c->launches - l0;
+			c->launches = l0;
+			if (c->gexec) {
+				cudaGraphExecDestroy(c->gexec);
+				c->gexec = nullptr;
+			}
+			if (e == cudaSuccess) e = cudaGraphInstantiate(&c->gexec, g, 0);
+			if (g) cudaGraphDestroy(g);
+			if (e == cudaSuccess) {
+				memcpy(c->gkey, &k, sizeof(k));
+				replayed = true;
+			} else {  // not capturable here: stay on stream launches
+				cudaGetLastError();
+				c->gexec = nullptr;
+				c->graph_off = true;
+			}
+			c->have_pending = false;
+		} else {
+			memcpy(c->pending_key, &k, sizeof(k));
+			c->have_pending = true;
+		}
+	}
+	if (replayed) {
+		CC_CUDA(c, cudaGraphLaunch(c->gexec, s));
+		c->launches += c->glaunches;
+	} else {
+		CC_TRY(enqueue_all(s));
+	}
 	CC_TRY(check_launch(c));
 	CC_TRY(read_stats(c, s));
 	CC_TRY(device_err(c));
@@ -509,6 +633,7 @@ cc_status cc_ctx_create(cc_ctx **out, int device) {
 	c->gp.k_target = 4.0f;
 	c->gp.min_ratio = 2.0f;
 	c->gp.user_dim[0] = c->gp.user_dim[1] = c->gp.user_dim[2] = 0;
+	if (const char *v = getenv("CC_GRAPH_REPLAY")) c->graph_off = v[0] == '0';
 	if (cudaSetDevice(device) != cudaSuccess || cudaMallocHost(&c->h_stats, sizeof(DevStats)) != cudaSuccess ||
 	    cudaMallocHost(&c->h_word, 64) != cudaSuccess) {
 		delete c;
@@ -530,6 +655,8 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->out_pairs, &c->out_norm,  &c->out_pa,     &c->out_pb,   &c->out_depth,   &c->out_bids};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
+	if (c->gexec) cudaGraphExecDestroy(c->gexec);
+	if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
 	if (c->h_stats) cudaFreeHost(c->h_stats);
 	if (c->h_word) cudaFreeHost(c->h_word);
 	for (int i = 0; i < 2 * kMaxMarks; i++)
@@ -587,6 +714,17 @@ cc_status cc_get_last_grid(const cc_ctx *c, int *dims3, uint64_t *entries) {
 }
 
 uint64_t cc_last_launch_count(const cc_ctx *c) { return c ? c->launches : 0; }
+
+cc_status cc_set_graph_replay(cc_ctx *c, int on) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	c->graph_off = !on;
+	c->have_pending = false;
+	if (!on && c->gexec) {
+		cudaGraphExecDestroy(c->gexec);
+		c->gexec = nullptr;
+	}
+	return CC_OK;
+}
 
 cc_status cc_set_profiling(cc_ctx *c, int on) {
 	if (!c) return CC_ERR_INVALID_ARGUMENT;

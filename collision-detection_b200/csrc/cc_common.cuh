@@ -135,4 +135,14 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint32_t t
 	return excl;
 }
 
+// Grid-stride zeroing of the ranges of a ZeroList (called by every thread of
+// a pass's first kernel).
+template <class ZL>
+__device__ __forceinline__ void zero_ranges(const ZL &z) {
+	const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, step = (uint64_t)gridDim.x * blockDim.x;
+#pragma unroll
+	for (int r = 0; r < 4; r++)
+		for (uint64_t i = t; i < z.words[r]; i += step) z.p[r][i] = 0u;
+}
+
 }  // namespace cc

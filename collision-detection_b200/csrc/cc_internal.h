@@ -53,6 +53,13 @@ struct GridParams {
 	uint32_t g_max;   // capacity of the per-cell arrays
 };
 
+// Word ranges the first kernel of a pass zeroes (scan control words, class
+// counters, cell counts), replacing a chain of memset launches.
+struct ZeroList {
+	uint32_t *p[4] = {nullptr, nullptr, nullptr, nullptr};
+	uint64_t words[4] = {0, 0, 0, 0};
+};
+
 // ------------------------------------------------------------------ scan
 // Exclusive scan of `n` uint32 counts into uint64 offsets out[0..n] (out[n] =
 // total) with one decoupled look-back pass. status: >= scan_tiles(n) words.
@@ -61,11 +68,15 @@ struct GridParams {
 size_t scan_tiles(uint64_t n);
 void launch_scan_u32_to_u64(const uint32_t *in, uint64_t n, unsigned long long *out, uint64_t *status,
                             uint32_t *ticket, uint32_t *err, cudaStream_t s,
-                            const unsigned long long *n_dev = nullptr, unsigned long long *total_out = nullptr);
-// Same, 32-bit output (caller guarantees total < 2^32).
+                            const unsigned long long *n_dev = nullptr, unsigned long long *total_out = nullptr,
+                            bool pre_zeroed = false);
+// Same, 32-bit output (caller guarantees total < 2^32). zero_in: the scan
+// stores 0 over every input word it read (the cell counts become the
+// scatter's cursors without a memset).
 void launch_scan_u32_to_u32(const uint32_t *in, uint64_t n, uint32_t *out, uint64_t *status, uint32_t *ticket,
                             uint32_t *err, cudaStream_t s, const unsigned long long *n_dev = nullptr,
-                            unsigned long long *total_out = nullptr);
+                            unsigned long long *total_out = nullptr, bool pre_zeroed = false,
+                            uint32_t *zero_in = nullptr);
 
 // ------------------------------------------------------------------ radix sort
 // Stable LSD radix sort of 64-bit keys on bits [bit_lo, bit_hi). `keys` and
@@ -83,7 +94,8 @@ void radix_sort_u64(unsigned long long *keys, unsigned long long *tmp, uint64_t 
 // Body ids >= nb set kErrBadIndex in *err and leave that shape's AABB unwritten.
 void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
-                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s);
+                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s,
+                 const ZeroList &zero = ZeroList());
 
 // ------------------------------------------------------------------ broadphase
 struct BpBuffers {
@@ -97,15 +109,18 @@ struct BpBuffers {
 	unsigned long long *owner_off;  // n + 1
 	unsigned long long *pairs_tmp;  // pair_cap
 	uint64_t pair_cap;
-	uint64_t *status;        // look-back tiles
-	uint32_t *ticket;        // 4 counters
+	uint64_t *status;        // look-back tiles of the cell scan
+	uint32_t *ticket;        // its tile counter
 	uint32_t *big_list;      // big segment owners
 	uint64_t big_cap;
+	uint64_t *status2 = nullptr;  // look-back tiles of the owner scan (null: shares status)
+	uint32_t *ticket2 = nullptr;
+	bool pre_zeroed = false;      // status/ticket regions were zeroed by the pass's first kernel
 };
 
 // Bounds pass over caller AABBs; its last block writes stats->plan.
 void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridParams &gp, const int grid[3],
-                   cudaStream_t s);
+                   cudaStream_t s, const ZeroList &zero = ZeroList());
 // In-place shift + per-cell counts on the plan's search grid.
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
@@ -142,6 +157,7 @@ struct NpScratch {
 	uint32_t *err;
 	uint32_t *order;        // P: pair indices grouped by (type A, type B)
 	uint32_t *classes;      // 2 * kNpClasses counters + the work-queue counter (zeroed per call)
+	bool pre_zeroed = false;  // classes, status and ticket already zeroed for this pass
 };
 constexpr int kNpClasses = 64;  // 7 x 7 shape-type combinations + one for invalid keys
 
@@ -155,6 +171,8 @@ void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, con
                 const uint8_t *active, const float *pos, const float *rot, float envelope, const long long *pairs,
                 const NpScratch &sc, int precision, uint64_t P_hint, cudaStream_t s);
 // The exact variant lives in its own -fmad=false translation unit.
+// Blocks of the exact MPR kernel resident per SM.
+int mpr_exact_resident_blocks();
 void launch_mpr_exact(unsigned grid, uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, const int32_t *T,
                       const float *A, const float *B, const float *C, const float *R, const uint32_t *ID, uint64_t nb,
                       const uint8_t *active, const float *pos, const float *rot, float envelope,

@@ -158,10 +158,11 @@ __device__ __forceinline__ vec<S> support_local(int type, vec<S> B, vec<S> n) {
 	return mk<S>(S(0), S(0), S(0));
 }
 
-// TransformSupportVert (:19-52) along direction d.
+// TransformSupportVert (:19-52) along direction d. The reference normalizes
+// d first (exact variant); the caller does that once for both shapes of the
+// pair, since d / |d| for -d is exactly -(d / |d|) in IEEE arithmetic.
 template <class S, bool kExact>
 __device__ __forceinline__ vec<S> support(const Shape<S> &s, vec<S> d) {
-	if constexpr (kExact) d = unit<S, true>(d);
 	if (s.type == TRIANGLEMESH) {  // SupportFunctions.cuh:14-29, world frame
 		S dist = dotp(s.X, d);
 		vec<S> p = s.X;
@@ -508,7 +509,8 @@ __device__ __forceinline__ void run(uint64_t P_cap, const unsigned long long *P_
 			continue;
 		}
 		// the support pair: support(A, -n), support(B, n)
-		const vec<S> d = cvt<S>(L.n);
+		vec<S> d = cvt<S>(L.n);
+		if constexpr (kExact) d = unit<S, true>(d);
 		const vec<S> pa = support<S, kExact>(L.A, neg(d));
 		const vec<S> pb = support<S, kExact>(L.B, d);
 		if (!post_step(L, pa, pb, sc, ida, idb)) L.st = kIdle;

@@ -24,6 +24,15 @@ __global__ void __launch_bounds__(kNT) k_mpr_exact(uint64_t P_cap, const unsigne
 }
 }  // namespace
 
+int mpr_exact_resident_blocks() {
+	static const int b = [] {
+		int v = 0;
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_mpr_exact, kNT, 0) != cudaSuccess || v < 1) v = 1;
+		return v;
+	}();
+	return b;
+}
+
 void launch_mpr_exact(unsigned grid, uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, const int32_t *T,
                       const float *A, const float *B, const float *C, const float *R, const uint32_t *ID, uint64_t nb,
                       const uint8_t *active, const float *pos, const float *rot, float envelope,

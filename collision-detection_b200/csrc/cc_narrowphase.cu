@@ -52,6 +52,26 @@ __device__ __forceinline__ uint32_t pair_class(uint64_t i, uint64_t n, const int
 	return (uint32_t)(ta * 7 + tb);
 }
 
+// Relative MPR cost of a shape type: smooth surfaces refine longest.
+__device__ __forceinline__ int type_cost(int t) {
+	switch (t) {
+	case SPHERE: return 1;
+	case BOX: return 2;
+	case CYLINDER: return 3;
+	case ELLIPSOID: return 4;
+	default: return 2;
+	}
+}
+constexpr int kMaxClassCost = 8;
+// Sphere-sphere pairs take the analytic path and invalid pairs do nothing:
+// cost 0.
+__device__ __forceinline__ int class_cost(int c) {
+	if (c >= 49) return 0;
+	const int ta = c / 7, tb = c % 7;
+	if (ta == SPHERE && tb == SPHERE) return 0;
+	return type_cost(ta) + type_cost(tb);
+}
+
 __global__ void __launch_bounds__(256) k_np_class_count(uint64_t P, const unsigned long long *P_dev, uint64_t n,
                                                          const int32_t *__restrict__ T,
                                                          const long long *__restrict__ pairs, uint32_t *classes) {
@@ -70,12 +90,14 @@ __global__ void __launch_bounds__(256) k_np_class_scatter(uint64_t P, const unsi
                                                            const long long *__restrict__ pairs, uint32_t *classes,
                                                            uint32_t *__restrict__ order) {
 	__shared__ uint32_t off[kNpClasses];
-	if (threadIdx.x == 0) {
+	if (threadIdx.x == 0) {  // classes in order of descending class_cost, so the longest pairs start first
 		uint32_t acc = 0;
-		for (int c = 0; c < kNpClasses; c++) {
-			off[c] = acc;
-			acc += classes[c];
-		}
+		for (int cost = kMaxClassCost; cost >= 0; cost--)
+			for (int c = 0; c < kNpClasses; c++)
+				if (class_cost(c) == cost) {
+					off[c] = acc;
+					acc += classes[c];
+				}
 	}
 	__syncthreads();
 	uint32_t *cursor = classes + kNpClasses;
@@ -123,6 +145,20 @@ __device__ __forceinline__ void compact_one(uint64_t i, uint64_t P, const NpScra
 }
 }  // namespace
 
+namespace {
+template <class K>
+int resident(K kernel) {
+	int v = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kernel, kNT, 0) != cudaSuccess || v < 1) v = 1;
+	return v;
+}
+// Blocks of the MPR kernel of a precision mode resident per SM.
+int mpr_resident_blocks(int precision) {
+	static const int b[3] = {mpr_exact_resident_blocks(), resident(k_mpr<double>), resident(k_mpr<float>)};
+	return b[precision == 0 ? 0 : (precision == 2 ? 2 : 1)];
+}
+}  // namespace
+
 void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, const int32_t *T, const float *A,
                 const float *B, const float *C, const float *R, const uint32_t *ID, uint64_t nb,
                 const uint8_t *active, const float *pos, const float *rot, float envelope, const long long *pairs,
@@ -130,13 +166,16 @@ void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, con
 	if (!P_cap) return;
 	{  // group the pairs by shape-type combination; the last word is the work queue
 		const unsigned g = (unsigned)std::min<uint64_t>((P_cap + 255) / 256, (uint64_t)kNumSMs * 4);
-		cudaMemsetAsync(sc.classes, 0, (2 * kNpClasses + 1) * sizeof(uint32_t), s);
+		if (!sc.pre_zeroed) cudaMemsetAsync(sc.classes, 0, (2 * kNpClasses + 1) * sizeof(uint32_t), s);
 		k_np_class_count<<<g, 256, 0, s>>>(P_cap, P_dev, n, T, pairs, sc.classes);
 		k_np_class_scatter<<<g, 256, 0, s>>>(P_cap, P_dev, n, T, pairs, sc.classes, sc.order);
 	}
-	// persistent lanes, about two pairs per lane (the queue balances the rest)
-	const uint64_t want = (std::min<uint64_t>(P_hint ? P_hint : P_cap, P_cap) + 2 * kNT - 1) / (2 * kNT);
-	const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(want, kNumSMs), (uint64_t)kNumSMs * 16);
+	// persistent lanes: one per pair up to the resident limit, so that every
+	// pair starts at once (the kernel is latency-bound: its time is the
+	// longest pair's dependency chain); beyond that the queue balances
+	const uint64_t want = (std::min<uint64_t>(P_hint ? P_hint : P_cap, P_cap) + kNT - 1) / kNT;
+	const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(want, kNumSMs),
+	                                                   (uint64_t)kNumSMs * mpr_resident_blocks(precision));
 	if (precision == 0)
 		launch_mpr_exact(grid, P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, sc, s);
 	else if (precision == 2)
@@ -150,7 +189,8 @@ void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, con
 void launch_np_compact(uint64_t P_cap, const unsigned long long *P_dev, const NpScratch &sc, long long *pairs,
                        float *norm, float *cpta, float *cptb, float *depth, int32_t *bids,
                        unsigned long long *contacts_out, cudaStream_t s) {
-	launch_scan_u32_to_u64(sc.flag, P_cap, sc.pos, sc.status, sc.ticket, sc.err, s, P_dev, contacts_out);
+	launch_scan_u32_to_u64(sc.flag, P_cap, sc.pos, sc.status, sc.ticket, sc.err, s, P_dev, contacts_out,
+	                       sc.pre_zeroed);
 	if (!P_cap) return;
 	const unsigned grid = (unsigned)std::min<uint64_t>((P_cap + 255) / 256, (uint64_t)kNumSMs * 16);
 	k_np_compact<<<grid, 256, 0, s>>>(P_cap, P_dev, sc, pairs, norm, cpta, cptb, depth, bids);

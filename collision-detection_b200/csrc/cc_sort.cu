@@ -15,7 +15,7 @@ __global__ void __launch_bounds__(kScanNT) k_scan(const uint32_t *__restrict__ i
                                                   const unsigned long long *__restrict__ n_dev,
                                                   OutT *__restrict__ out,
                                                   unsigned long long *total_out, uint64_t *status, uint32_t *ticket,
-                                                  uint32_t *err) {
+                                                  uint32_t *err, uint32_t *zero_in) {
 	__shared__ uint32_t s_tile;
 	__shared__ unsigned long long s_pre;
 	__shared__ unsigned long long sm[40];
@@ -35,9 +35,20 @@ __global__ void __launch_bounds__(kScanNT) k_scan(const uint32_t *__restrict__ i
 			uint4 t = __ldcs(p + q);
 			v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
 		}
+		if (zero_in && (reinterpret_cast<uintptr_t>(zero_in) & 15) == 0) {
+			uint4 *z = reinterpret_cast<uint4 *>(zero_in + i0);
+#pragma unroll
+			for (int q = 0; q < kScanIPT / 4; q++) z[q] = make_uint4(0u, 0u, 0u, 0u);
+		} else if (zero_in) {
+#pragma unroll
+			for (int j = 0; j < kScanIPT; j++) zero_in[i0 + j] = 0u;
+		}
 	} else {
 #pragma unroll
 		for (int j = 0; j < kScanIPT; j++) v[j] = (i0 + j < n) ? in[i0 + j] : 0u;
+		if (zero_in)
+			for (int j = 0; j < kScanIPT; j++)
+				if (i0 + j < n) zero_in[i0 + j] = 0u;
 	}
 	unsigned long long sum = 0;
 #pragma unroll
@@ -63,11 +74,14 @@ __global__ void __launch_bounds__(kScanNT) k_scan(const uint32_t *__restrict__ i
 
 template <class OutT>
 void scan_impl(const uint32_t *in, uint64_t n, OutT *out, uint64_t *status, uint32_t *ticket, uint32_t *err,
-               cudaStream_t s, const unsigned long long *n_dev = nullptr, unsigned long long *total_out = nullptr) {
+               cudaStream_t s, const unsigned long long *n_dev, unsigned long long *total_out, bool pre_zeroed,
+               uint32_t *zero_in) {
 	const uint64_t tiles = n / kScanTile + 1;
-	cudaMemsetAsync(status, 0, tiles * sizeof(uint64_t), s);
-	cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s);
-	k_scan<OutT><<<(unsigned)tiles, kScanNT, 0, s>>>(in, n, n_dev, out, total_out, status, ticket, err);
+	if (!pre_zeroed) {
+		cudaMemsetAsync(status, 0, tiles * sizeof(uint64_t), s);
+		cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s);
+	}
+	k_scan<OutT><<<(unsigned)tiles, kScanNT, 0, s>>>(in, n, n_dev, out, total_out, status, ticket, err, zero_in);
 }
 }  // namespace
 
@@ -75,13 +89,13 @@ size_t scan_tiles(uint64_t n) { return (size_t)(n / kScanTile + 1); }
 
 void launch_scan_u32_to_u64(const uint32_t *in, uint64_t n, unsigned long long *out, uint64_t *status,
                             uint32_t *ticket, uint32_t *err, cudaStream_t s, const unsigned long long *n_dev,
-                            unsigned long long *total_out) {
-	scan_impl(in, n, out, status, ticket, err, s, n_dev, total_out);
+                            unsigned long long *total_out, bool pre_zeroed) {
+	scan_impl(in, n, out, status, ticket, err, s, n_dev, total_out, pre_zeroed, (uint32_t *)nullptr);
 }
 void launch_scan_u32_to_u32(const uint32_t *in, uint64_t n, uint32_t *out, uint64_t *status, uint32_t *ticket,
                             uint32_t *err, cudaStream_t s, const unsigned long long *n_dev,
-                            unsigned long long *total_out) {
-	scan_impl(in, n, out, status, ticket, err, s, n_dev, total_out);
+                            unsigned long long *total_out, bool pre_zeroed, uint32_t *zero_in) {
+	scan_impl(in, n, out, status, ticket, err, s, n_dev, total_out, pre_zeroed, zero_in);
 }
 
 // --------------------------------------------------------------------------
@@ -168,7 +182,8 @@ void radix_sort_u64(unsigned long long *keys, unsigned long long *tmp, uint64_t 
 	unsigned long long *src = keys, *dst = tmp;
 	for (int sh = bit_lo; sh < bit_hi; sh += 8) {
 		k_radix_hist<<<ntiles, kRxNT, 0, s>>>(src, n, sh, ntiles, hist);
-		scan_impl(hist, (uint64_t)256 * ntiles, hoff, status, ticket, err, s);
+		scan_impl(hist, (uint64_t)256 * ntiles, hoff, status, ticket, err, s, (const unsigned long long *)nullptr,
+		          (unsigned long long *)nullptr, false, (uint32_t *)nullptr);
 		k_radix_scatter<<<ntiles, kRxNT, 0, s>>>(src, n, sh, ntiles, hoff, dst);
 		unsigned long long *t = src; src = dst; dst = t;
 	}

@@ -164,8 +164,7 @@ extern "C" cc_status cc_broadphase_noalloc(uint64_t n, float *aabb, int gx, int 
 	NA_CUDA(cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * b.g_max, s));
 	launch_bounds(n, aabb, b.stats, gp, grid, s);  // + the grid plan
 	launch_count(n, aabb, b, s);
-	launch_scan_cells(b, b.g_max, s);
-	NA_CUDA(cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * b.g_max, s));
+	launch_scan_cells(b, b.g_max, s);  // leaves the counts zeroed for the scatter
 	launch_scatter(n, aabb, b, s);
 	launch_pair_test(n, b, n, s);
 	launch_scan_owner(n, b, s);

@@ -94,6 +94,13 @@ CC_API cc_status cc_set_tuning(cc_ctx *ctx, float cell_target, float min_ratio);
  *  CC_NP_MIXED: as CC_NP_FP64 but FP32 support maps. */
 enum { CC_NP_EXACT = 0, CC_NP_FP64 = 1, CC_NP_MIXED = 2 };
 CC_API cc_status cc_set_narrowphase_precision(cc_ctx *ctx, int mode);
+/* CUDA-graph replay of cc_collide (default on; environment CC_GRAPH_REPLAY=0
+ * turns it off at context creation). When the same configuration (sizes,
+ * pointers, grid, precision, envelope, tuning) reaches cc_collide twice in a
+ * row, its launches are captured once and replayed by one graph launch per
+ * call from then on. Results are identical either way. No reference
+ * counterpart. */
+CC_API cc_status cc_set_graph_replay(cc_ctx *ctx, int on);
 /* The grid the last broadphase searched on, and its entry count. */
 CC_API cc_status cc_get_last_grid(const cc_ctx *ctx, int *dims3, uint64_t *entries);
 
