@@ -189,8 +189,24 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 // the same cell. A warp's 32 entries and the kWin - 32 that follow them are
 // staged in shared memory with coalesced 16-byte loads (cells hold a handful
 // of entries, so the inner loop almost never leaves the window); loops are
-// warp-uniform so the emission can be warp-aggregated.
+// warp-uniform so the emission can be warp-aggregated: found pairs collect in
+// a per-warp shared buffer that is flushed with one counter atomic per
+// kOutBuf - 31 pairs or more (dense scenes emit billions of pairs).
 constexpr int kWin = 96;
+constexpr int kOutBuf = 128;
+
+__device__ __forceinline__ void flush_pairs(unsigned long long *buf, uint32_t cnt, uint32_t lane,
+                                            unsigned long long *pair_counter, unsigned long long *pairs,
+                                            uint64_t pair_cap) {
+	unsigned long long start = 0;
+	if (lane == 0) start = atomicAdd(pair_counter, (unsigned long long)cnt);
+	start = __shfl_sync(0xffffffffu, start, 0);
+	for (uint32_t k = lane; k < cnt; k += 32) {
+		const unsigned long long pos = start + k;
+		if (pos < pair_cap) pairs[pos] = buf[k];
+	}
+	__syncwarp();
+}
 
 __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const uint32_t *__restrict__ cell_start,
                                                     const float4 *__restrict__ entries,
@@ -199,11 +215,14 @@ __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const 
                                                     unsigned long long *pair_counter) {
 	__shared__ Plan sp;
 	__shared__ float4 win_all[kNT / 32][2 * kWin];
+	__shared__ unsigned long long out_all[kNT / 32][kOutBuf];
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
 	if (!sp.valid) return;
 	float4 *win = win_all[threadIdx.x >> 5];
+	unsigned long long *obuf = out_all[threadIdx.x >> 5];
+	uint32_t ocnt = 0;  // pairs in obuf (warp-uniform)
 	const uint64_t E = min((uint64_t)stats->entries, entry_cap);
 	const uint32_t lane = threadIdx.x & 31;
 	const uint32_t lt = (1u << lane) - 1u;
@@ -268,19 +287,22 @@ __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const 
 			}
 			const uint32_t b = __ballot_sync(0xffffffffu, emit);
 			if (b) {
-				unsigned long long start = 0;
-				const int leader = __ffs(b) - 1;
-				if ((int)lane == leader) start = atomicAdd(pair_counter, (unsigned long long)__popc(b));
-				start = __shfl_sync(0xffffffffu, start, leader);
+				const uint32_t nb = __popc(b);
+				if (ocnt + nb > kOutBuf) {
+					flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);
+					ocnt = 0;
+				}
 				if (emit) {
-					const unsigned long long pos = start + __popc(b & lt);
-					if (pos < pair_cap) pairs[pos] = key;
+					obuf[ocnt + __popc(b & lt)] = key;
 					if (other_owner != 0xffffffffu) atomicAdd(&owner_count[other_owner], 1u);
 				}
+				ocnt += nb;
+				__syncwarp();
 			}
 		}
 		if (owned) atomicAdd(&owner_count[ida], owned);
 	}
+	if (ocnt) flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);
 }
 
 // Bucket the unsorted pairs by owner (the smaller index). P comes from the
@@ -303,8 +325,13 @@ __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t
 }
 
 constexpr int kSmallSeg = 32;
-constexpr int kBigSeg = 4096;
+constexpr int kMidSeg = 1024;
+constexpr int kBigSeg = 16384;
 
+// Sorts each owner bucket (all keys share the owner in the high half):
+// <= 32 keys by one thread in place; longer buckets are listed for
+// k_segsort_mid (<= 1024 keys, from the front of big_list) or k_segsort_big
+// (<= 16384, from the back).
 __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long long *__restrict__ owner_off,
                                                   unsigned long long *__restrict__ out, uint32_t *big_list,
                                                   uint64_t big_cap, DevStats *stats) {
@@ -330,40 +357,81 @@ __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long
 		atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
 		return;
 	}
-	const unsigned long long slot = atomicAdd(&stats->big_segments, 1ull);
-	if (slot < big_cap) big_list[slot] = (uint32_t)a;
+	const bool mid = len <= kMidSeg;
+	const unsigned long long slot = atomicAdd(mid ? &stats->big_segments : &stats->seg_big, 1ull);
+	if (slot < big_cap) big_list[mid ? slot : big_cap - 1 - slot] = (uint32_t)a;
 	else atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
 }
 
-// Segments of 33..4096 keys: one block per segment (grid-stride over the
-// device-side count), bitonic sort in shared memory.
+// In-place bitonic sort of m (a power of two) 32-bit keys in shared memory by
+// `nt` cooperating threads (thread t of them); sync() separates the steps.
+template <class Sync>
+__device__ __forceinline__ void bitonic_u32(uint32_t *s, int m, int t, int nt, Sync sync) {
+	for (int k = 2; k <= m; k <<= 1) {
+		for (int j = k >> 1; j > 0; j >>= 1) {
+			for (int i = t; i < m; i += nt) {
+				const int p = i ^ j;
+				if (p > i) {
+					const bool up = (i & k) == 0;
+					const uint32_t x = s[i], y = s[p];
+					if ((x > y) == up) {
+						s[i] = y;
+						s[p] = x;
+					}
+				}
+			}
+			sync();
+		}
+	}
+}
+
+// Buckets of 33..1024 keys: one warp per bucket, the partner halves sorted in
+// shared memory (4 KB per warp).
+constexpr int kMidNT = 256;
+__global__ void __launch_bounds__(kMidNT) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
+                                                         const uint32_t *__restrict__ big_list,
+                                                         const unsigned long long *__restrict__ owner_off,
+                                                         unsigned long long *__restrict__ out) {
+	__shared__ uint32_t s_all[kMidNT / 32][kMidSeg];
+	if (stats->np_n != stats->pairs) return;
+	const uint64_t nmid = min((uint64_t)stats->big_segments, big_cap);
+	uint32_t *s = s_all[threadIdx.x >> 5];
+	const int lane = threadIdx.x & 31;
+	const uint64_t warps = (uint64_t)gridDim.x * (kMidNT / 32);
+	for (uint64_t g = (uint64_t)blockIdx.x * (kMidNT / 32) + (threadIdx.x >> 5); g < nmid; g += warps) {
+		const uint32_t a = big_list[g];
+		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
+		int m = 64;
+		while ((uint64_t)m < len) m <<= 1;
+		for (int i = lane; i < m; i += 32) s[i] = (uint64_t)i < len ? (uint32_t)out[beg + i] : 0xffffffffu;
+		__syncwarp();
+		bitonic_u32(s, m, lane, 32, [] { __syncwarp(); });
+		const unsigned long long hi = (unsigned long long)a << 32;
+		for (int i = lane; (uint64_t)i < len; i += 32) out[beg + i] = hi | s[i];
+		__syncwarp();
+	}
+}
+
+// Buckets of 1025..16384 keys: one block per bucket (grid-stride over the
+// device-side count), bitonic sort of the partner halves in 64 KB of
+// dynamic shared memory.
 __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint64_t big_cap,
                                                       const uint32_t *__restrict__ big_list,
                                                       const unsigned long long *__restrict__ owner_off,
                                                       unsigned long long *__restrict__ out) {
-	__shared__ unsigned long long s[kBigSeg];
-	const uint64_t nbig = min((uint64_t)stats->big_segments, big_cap);
+	extern __shared__ uint32_t s[];
+	if (stats->np_n != stats->pairs) return;
+	const uint64_t nbig = min((uint64_t)stats->seg_big, big_cap);
 	for (uint64_t g = blockIdx.x; g < nbig; g += gridDim.x) {
-		const uint32_t a = big_list[g];
+		const uint32_t a = big_list[big_cap - 1 - g];
 		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
 		int m = 1;
 		while ((uint64_t)m < len) m <<= 1;
-		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? out[beg + i] : ~0ull;
+		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? (uint32_t)out[beg + i] : 0xffffffffu;
 		__syncthreads();
-		for (int k = 2; k <= m; k <<= 1) {
-			for (int j = k >> 1; j > 0; j >>= 1) {
-				for (int i = threadIdx.x; i < m; i += blockDim.x) {
-					const int p = i ^ j;
-					if (p > i) {
-						const bool up = (i & k) == 0;
-						const unsigned long long x = s[i], y = s[p];
-						if ((x > y) == up) { s[i] = y; s[p] = x; }
-					}
-				}
-				__syncthreads();
-			}
-		}
-		for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = s[i];
+		bitonic_u32(s, m, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+		const unsigned long long hi = (unsigned long long)a << 32;
+		for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = hi | s[i];
 		__syncthreads();
 	}
 }
@@ -511,7 +579,13 @@ void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cud
 }
 
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
-	k_segsort_big<<<kNumSMs, 512, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
+	static const bool attr = [] {
+		return cudaFuncSetAttribute(k_segsort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                            kBigSeg * (int)sizeof(uint32_t)) == cudaSuccess;
+	}();
+	(void)attr;
+	k_segsort_mid<<<kNumSMs * 6, kMidNT, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
+	k_segsort_big<<<kNumSMs, 512, kBigSeg * sizeof(uint32_t), s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
 }
 
 void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s) {

@@ -269,7 +269,7 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap) {
 	c->st_words[1] = std::max<uint64_t>(c->st_words[1], status_words_for(n + 1));
 	CC_TRY(ensure_status(c));
 	CC_TRY(ensure(c, c->ticket, 64));
-	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * std::max<uint64_t>(1024, n / 16)));
+	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * (n + 1024)));
 	if (np_cap) CC_TRY(np_prepare(c, np_cap));
 	return CC_OK;
 }
@@ -357,9 +357,9 @@ void enqueue_emit(cc_ctx *c, uint64_t n, unsigned long long *out, uint64_t out_c
 	{
 		StageMark m(c, ST_SEGSORT, s);
 		launch_segsort(n, out, b, s);
-		launch_segsort_big(out, b, s);
+		launch_segsort_big(out, b, s);  // the warp and block tiers
 	}
-	c->launches += 3;
+	c->launches += 4;
 }
 
 // Narrowphase over min(P_cap, *P_dev) pairs (P_dev null: exactly P_cap).
@@ -388,7 +388,7 @@ cc_status reset_pass_counters(cc_ctx *c, uint64_t n, cudaStream_t s) {
 	CC_CUDA(c, cudaMemsetAsync(&d->err, 0, sizeof(uint32_t), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->pairs, 0, sizeof(unsigned long long), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
-	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 2 * sizeof(unsigned long long), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 3 * sizeof(unsigned long long), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->np_n, 0, sizeof(unsigned long long), s));
 	return CC_OK;
 }
@@ -459,7 +459,7 @@ cc_status emit_retained(cc_ctx *c, unsigned long long *out, uint64_t cap, cudaSt
 	DevStats *d = ptr<DevStats>(c->stats);
 	c->h_word[0] = c->retained_P;
 	CC_CUDA(c, cudaMemcpyAsync(&d->pairs, c->h_word, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 2 * sizeof(unsigned long long), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 3 * sizeof(unsigned long long), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->err, 0, sizeof(uint32_t), s));
 	enqueue_emit(c, c->retained_n, out, cap, s);
 	CC_TRY(check_launch(c));

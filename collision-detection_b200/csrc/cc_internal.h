@@ -34,8 +34,9 @@ struct DevStats {
 	unsigned long long entries;   // (cell, body) entries of the search grid
 	unsigned long long ref_entries;
 	unsigned long long contacts;
-	unsigned long long big_segments;
+	unsigned long long big_segments;  // owner buckets of 33..1024 pairs (listed from the front)
 	unsigned long long max_segment;
+	unsigned long long seg_big;       // owner buckets of 1025..16384 pairs (listed from the back)
 	unsigned long long cells;     // plan.G as a 64-bit scan count
 	unsigned long long np_n;      // pairs handed to the narrowphase (0 if an output was too small)
 	uint32_t blocks_done;         // last-block detection of the bounds reduction

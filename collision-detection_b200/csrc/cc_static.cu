@@ -38,7 +38,7 @@ constexpr uint64_t kMaxBodies = CC_NOALLOC_MAX_BODIES;
 constexpr uint64_t kMaxEntries = CC_NOALLOC_MAX_ENTRIES;
 constexpr uint64_t kMaxPairs = CC_NOALLOC_MAX_PAIRS;
 constexpr uint32_t kGMax = (uint32_t)kMaxBodies;  // per-cell arrays (>= 4096)
-constexpr uint64_t kBigCap = 1024;
+constexpr uint64_t kBigCap = kMaxBodies + 1024;
 constexpr size_t kScratchBytes = CC_NOALLOC_SCRATCH_BYTES;
 
 // The scratch. In host code `g_scratch` is only a stand-in symbol, never a
