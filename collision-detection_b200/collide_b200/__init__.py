@@ -221,7 +221,9 @@ class Broadphase:
         """Shifts aabb_data ((2N,3) float32, CUDA) in place and returns the
         sorted unique int64 pair keys."""
         n = int(aabb_data.shape[0]) // 2
-        cap = max(1024, n // 4)
+        # capacity: the previous call's pair count with some slack, so a
+        # steady scene needs one library call (else cc_broadphase_fetch)
+        cap = max(1024, n // 4, self.number_of_contacts_possible + self.number_of_contacts_possible // 16)
         out = torch.empty(cap, dtype=torch.int64, device=aabb_data.device)
         np_ = ctypes.c_uint64()
         st = lib.cc_broadphase(self.ctx.h, n, _ptr(aabb_data, torch.float32, "aabb_data"), *self.grid_size,
@@ -425,3 +427,66 @@ class DevicePipeline:
             self.ctx.check(st, "cc_collide")
             self.n_pairs, self.n_contacts = int(self.res.n_pairs), int(self.res.n_contacts)
             return self.n_pairs, self.n_contacts
+
+
+class DeviceBatch:
+    """Independent scenes resident on the device as one concatenated scene
+    (cc_batch): shapes [shape_offsets[s], shape_offsets[s+1]) and bodies
+    [body_offsets[s], body_offsets[s+1]) belong to scene s."""
+
+    def __init__(self, scenes, device="cuda"):
+        from . import scenes as _sc
+        cat, self.shape_offsets, self.body_offsets = _sc.concat(list(scenes))
+        self.ds = DeviceScene(cat, device=device)
+        self.num_scenes = len(self.shape_offsets) - 1
+        self.n, self.nb = self.ds.n, self.ds.nb
+
+    def c_batch(self):
+        b = _lib.Batch()
+        b.num_scenes = self.num_scenes
+        b.shape_offsets = self.shape_offsets.ctypes.data
+        b.body_offsets = self.body_offsets.ctypes.data
+        b.scene = self.ds.c_scene()
+        return b
+
+
+class BatchPipeline:
+    """cc_collide_batch with preallocated outputs: run() collides every scene
+    of a DeviceBatch in one pass. After run(): scene_pairs[s] pairs and
+    contacts [contact_offsets[s], contact_offsets[s+1]) for scene s; pair keys
+    and bids use the concatenated numbering."""
+
+    def __init__(self, db: DeviceBatch, grid=(16, 16, 16), envelope=0.0, ctx: Context | None = None, pairs_cap=None):
+        self.db, self.ds, self.ctx = db, db.ds, ctx or default_context()
+        self.grid, self.envelope = tuple(int(g) for g in grid), float(envelope)
+        dev = db.ds.T.device
+        self.aabb = torch.zeros((2 * db.n, 3), dtype=torch.float32, device=dev)
+        self.batch = db.c_batch()
+        self.scene_pairs = np.zeros(db.num_scenes, np.uint64)
+        self.contact_offsets = np.zeros(db.num_scenes + 1, np.uint64)
+        self._alloc(int(pairs_cap or max(1024, db.n // 4)))
+        self.n_pairs = self.n_contacts = 0
+
+    _alloc = DevicePipeline._alloc
+
+    def run(self):
+        while True:
+            st = lib.cc_collide_batch(self.ctx.h, ctypes.byref(self.batch), *self.grid, self.envelope,
+                                      ctypes.byref(self.res), self.scene_pairs.ctypes.data,
+                                      self.contact_offsets.ctypes.data, _stream())
+            if st == _lib.CC_ERR_CAPACITY and self.res.n_pairs > self.cap:
+                self._alloc(int(self.res.n_pairs * 5 // 4))
+                continue
+            self.ctx.check(st, "cc_collide_batch")
+            self.n_pairs, self.n_contacts = int(self.res.n_pairs), int(self.res.n_contacts)
+            return self.n_pairs, self.n_contacts
+
+
+def collide_batch(db: DeviceBatch, grid=(16, 16, 16), envelope=0.0, ctx: Context | None = None, pairs_cap=None):
+    """cc_collide_batch once; returns device tensors (concatenated numbering)
+    plus per-scene pair counts and contact offsets (numpy)."""
+    bp = BatchPipeline(db, grid, envelope, ctx, pairs_cap)
+    P, k = bp.run()
+    return dict(aabb=bp.aabb, pairs=bp.pairs[:P], contact_pairs=bp.pairs[:k], norm=bp.norm[:k], cpta=bp.cpta[:k],
+                cptb=bp.cptb[:k], depth=bp.depth[:k], bids=bp.bids[:k], n_pairs=P, n_contacts=k,
+                scene_pairs=bp.scene_pairs.copy(), contact_offsets=bp.contact_offsets.copy())

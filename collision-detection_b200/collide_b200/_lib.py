@@ -54,6 +54,7 @@ SIGNATURES = {
     "cc_narrowphase": (I32, [P, U64, P, P, P, P, P, P, U64, P, P, P, F32, P, U64, P, P, P, P, P, PU64, P]),
     "cc_collide": (I32, [P, P, I32, I32, I32, F32, P, P]),
     "cc_collide_host": (I32, [P, P, I32, I32, I32, F32, P, P]),
+    "cc_collide_batch": (I32, [P, P, I32, I32, I32, F32, P, P, P, P]),
     "cc_last_launch_count": (U64, [P]),
     "cc_set_profiling": (I32, [P, I32]),
     "cc_set_graph_replay": (I32, [P, I32]),
@@ -74,6 +75,11 @@ class Scene(ctypes.Structure):
     """struct cc_scene."""
     _fields_ = [("n", U64), ("T", P), ("A", P), ("B", P), ("C", P), ("R", P), ("ID", P), ("nb", U64),
                 ("body_pos", P), ("body_rot", P), ("active", P)]
+
+
+class Batch(ctypes.Structure):
+    """struct cc_batch."""
+    _fields_ = [("num_scenes", U64), ("shape_offsets", P), ("body_offsets", P), ("scene", Scene)]
 
 
 class Result(ctypes.Structure):

@@ -135,6 +135,35 @@ def mixed_slab(n=1 << 20, seed=0, extent=(10.0, 10.0, 0.5), hmin=0.001, hmax=0.0
     return _one_shape_per_body(T, B, c, q, f"mixed_slab_{n}")
 
 
+def batched_mixed(num_scenes=512, seed=0, nmin=1000, nmax=200_000, dmin=0.2, dmax=1.0):
+    """Independent scenes of uneven size for the batched path.
+
+    Defaults are the 512-scene workload: body counts log-uniform in
+    [1,000, 200,000] (mean about 37.6k, about 19M in total), each scene a
+    mixed_slab (the 1M workload's shape mix, sizes and orientations) with its
+    own fill density d ~ U[0.2, 1.0] read as slab thickness 0.5 / d over the
+    10 x 10 footprint. Returns a list of Scene.
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), size=num_scenes)).round().astype(np.int64)
+    dens = rng.uniform(dmin, dmax, size=num_scenes)
+    return [mixed_slab(int(n), seed=seed * 1_000_003 + 1 + i, extent=(10.0, 10.0, 0.5 / d))
+            for i, (n, d) in enumerate(zip(sizes, dens))]
+
+
+def concat(scenes):
+    """Concatenates scenes for the batched entry point: returns (scene,
+    shape_offsets, body_offsets). ID stays local to each scene."""
+    so = np.zeros(len(scenes) + 1, np.uint64)
+    bo = np.zeros(len(scenes) + 1, np.uint64)
+    so[1:] = np.cumsum([s.n for s in scenes])
+    bo[1:] = np.cumsum([s.nb for s in scenes])
+    cat = lambda f: np.ascontiguousarray(np.concatenate([getattr(s, f) for s in scenes]))
+    sc = Scene(T=cat("T"), A=cat("A"), B=cat("B"), C=cat("C"), R=cat("R"), ID=cat("ID"), pos=cat("pos"),
+               rot=cat("rot"), active=cat("active"), name=f"batch_{len(scenes)}")
+    return sc, so, bo
+
+
 def clustered_spheres(n=1 << 24, seed=0, clusters=64, sigma=0.02, background=0.10,
                       rmin=0.0005, rmax=0.005):
     """Load-imbalanced spheres.

@@ -123,19 +123,48 @@ __global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restr
 	accumulate_stats_one<kNT>(mn, mx, have, stats, pa);
 }
 
+// The plan a shape is searched with: the block's staged plan (one scene) or
+// its scene's plan (batch).
+template <bool kBatch>
+__device__ __forceinline__ const Plan &plan_of(const Plan &sp, const SceneMap &sm, uint64_t shape, uint32_t &base) {
+	if constexpr (kBatch) {
+		const uint32_t s = __ldg(sm.scene_of + shape);
+		base = __ldg(sm.cell_base + s);
+		return sm.plans[s];
+	} else {
+		base = 0;
+		return sp;
+	}
+}
+__device__ __forceinline__ uint32_t cell_index(const Plan &p, uint32_t base, int x, int y, int z) {
+	return base + (uint32_t)x + (uint32_t)p.dim[0] * ((uint32_t)y + (uint32_t)p.dim[1] * z);
+}
+
+template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, const DevStats *stats,
-                                                uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count) {
+                                                uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count,
+                                                SceneMap sm) {
 	__shared__ Plan sp;
 	__shared__ float stage[6 * kNT];
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
-	if (!sp.valid) return;  // invalid input: nothing is modified
+	if (!kBatch && !sp.valid) return;  // invalid input: nothing is modified
 	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
 	load_tile_aabb(aabb, n, i0, stage);
 	__syncthreads();
 	// in-place shift by fabs(min) (:382-386), element by element
-	for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
+	if constexpr (kBatch) {
+		for (int k = threadIdx.x; k < 6 * kNT; k += kNT) {
+			const uint64_t shape = i0 + (uint64_t)((k % (3 * kNT)) / 3);
+			if (shape < n) {
+				const Plan &p = sm.plans[__ldg(sm.scene_of + shape)];
+				if (p.valid) stage[k] = stage[k] + p.origin[k % 3];
+			}
+		}
+	} else {
+		for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
+	}
 	__syncthreads();
 	store_tile_aabb(aabb, n, i0, stage);
 	const uint64_t i = i0 + threadIdx.x;
@@ -144,18 +173,21 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
 	const float *hs = stage + 3 * kNT;
 	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
 	owner_count[i] = 0u;
-	const CellRange r = cell_range(sp, mn, mx);
+	uint32_t base;
+	const Plan &p = plan_of<kBatch>(sp, sm, i, base);
+	if (kBatch && !p.valid) return;
+	const CellRange r = cell_range(p, mn, mx);
 	for (int z = r.c0[2]; z <= r.c1[2]; z++)
 		for (int y = r.c0[1]; y <= r.c1[1]; y++)
-			for (int x = r.c0[0]; x <= r.c1[0]; x++)
-				atomicAdd(&cell_count[(uint32_t)x + (uint32_t)sp.dim[0] * ((uint32_t)y + (uint32_t)sp.dim[1] * z)], 1u);
+			for (int x = r.c0[0]; x <= r.c1[0]; x++) atomicAdd(&cell_count[cell_index(p, base, x, y, z)], 1u);
 }
 
 // Cell-ordered entries: one thread per body, a cursor atomic per covered cell.
+template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
                                                   const uint32_t *__restrict__ cell_start,
                                                   uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
-                                                  uint64_t cap, uint32_t *err) {
+                                                  uint64_t cap, uint32_t *err, SceneMap sm) {
 	__shared__ Plan sp;
 	__shared__ float stage[6 * kNT];
 	if (threadIdx.x < sizeof(Plan) / 4)
@@ -164,16 +196,19 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 	load_tile_aabb(aabb, n, i0, stage);
 	__syncthreads();
 	const uint64_t i = i0 + threadIdx.x;
-	if (!sp.valid || i >= n) return;
+	if ((!kBatch && !sp.valid) || i >= n) return;
 	const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
 	const float *hs = stage + 3 * kNT;
 	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
-	const CellRange r = cell_range(sp, mn, mx);
+	uint32_t base;
+	const Plan &p = plan_of<kBatch>(sp, sm, i, base);
+	if (kBatch && !p.valid) return;
+	const CellRange r = cell_range(p, mn, mx);
 	bool over = false;
 	for (int z = r.c0[2]; z <= r.c1[2]; z++)
 		for (int y = r.c0[1]; y <= r.c1[1]; y++)
 			for (int x = r.c0[0]; x <= r.c1[0]; x++) {
-				const uint32_t c = (uint32_t)x + (uint32_t)sp.dim[0] * ((uint32_t)y + (uint32_t)sp.dim[1] * z);
+				const uint32_t c = cell_index(p, base, x, y, z);
 				const uint64_t slot = (uint64_t)cell_start[c] + atomicAdd(&cursor[c], 1u);
 				if (slot < cap) {
 					entries[2 * slot] = make_float4(mn.x, mn.y, mn.z, __uint_as_float((uint32_t)i));
@@ -208,18 +243,19 @@ __device__ __forceinline__ void flush_pairs(unsigned long long *buf, uint32_t cn
 	__syncwarp();
 }
 
-__global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const uint32_t *__restrict__ cell_start,
+template <bool kBatch>
+__global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, const uint32_t *__restrict__ cell_start,
                                                     const float4 *__restrict__ entries,
                                                     uint64_t entry_cap, uint32_t *__restrict__ owner_count,
                                                     unsigned long long *__restrict__ pairs, uint64_t pair_cap,
-                                                    unsigned long long *pair_counter) {
+                                                    unsigned long long *pair_counter, SceneMap sm) {
 	__shared__ Plan sp;
 	__shared__ float4 win_all[kNT / 32][2 * kWin];
 	__shared__ unsigned long long out_all[kNT / 32][kOutBuf];
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
-	if (!sp.valid) return;
+	if (!kBatch && !sp.valid) return;
 	float4 *win = win_all[threadIdx.x >> 5];
 	unsigned long long *obuf = out_all[threadIdx.x >> 5];
 	uint32_t ocnt = 0;  // pairs in obuf (warp-uniform)
@@ -238,21 +274,26 @@ __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const 
 		float4 alo = make_float4(0.f, 0.f, 0.f, 0.f), ahi = alo;
 		int my_n = 0;
 		int cx = 0, cy = 0, cz = 0;
+		const uint32_t ida = valid ? __float_as_uint(win[2 * lane].w) : 0u;
+		uint32_t cbase;
+		const Plan &pl = plan_of<kBatch>(sp, sm, ida, cbase);
 		if (valid) {
 			alo = win[2 * lane];
 			ahi = win[2 * lane + 1];
 			const uint32_t pc = __float_as_uint(ahi.w);
 			cx = pc & 1023; cy = (pc >> 10) & 1023; cz = (pc >> 20) & 1023;
-			const uint32_t c = (uint32_t)cx + (uint32_t)sp.dim[0] * ((uint32_t)cy + (uint32_t)sp.dim[1] * cz);
+			const uint32_t c = cell_index(pl, cbase, cx, cy, cz);
 			const uint64_t end = min((uint64_t)cell_start[c + 1], entry_cap);
 			my_n = (int)(end > e + 1 ? end - e - 1 : 0);
 		}
-		const uint32_t ida = __float_as_uint(alo.w);
+		const float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
+		const float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
+		const int d0 = pl.dim[0], d1 = pl.dim[1], d2 = pl.dim[2];
 		// home-cell test: the pair belongs to this cell iff, on every axis, one
 		// of the two min corners lies in this cell's slab
-		const bool ax = valid && cell_of(alo.x, sp.lo[0], sp.inv[0], sp.dim[0]) == cx;
-		const bool ay = valid && cell_of(alo.y, sp.lo[1], sp.inv[1], sp.dim[1]) == cy;
-		const bool az = valid && cell_of(alo.z, sp.lo[2], sp.inv[2], sp.dim[2]) == cz;
+		const bool ax = valid && cell_of(alo.x, lo0, iv0, d0) == cx;
+		const bool ay = valid && cell_of(alo.y, lo1, iv1, d1) == cy;
+		const bool az = valid && cell_of(alo.z, lo2, iv2, d2) == cz;
 		const int iters = __reduce_max_sync(0xffffffffu, my_n);
 		uint32_t owned = 0;
 		for (int t = 0; t < iters; t++) {
@@ -272,9 +313,9 @@ __global__ void __launch_bounds__(kNT) k_pair_test(const DevStats *stats, const 
 				}
 				if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
 				    blo.z <= ahi.z) {
-					const bool hx = ax || cell_of(blo.x, sp.lo[0], sp.inv[0], sp.dim[0]) == cx;
-					const bool hy = ay || cell_of(blo.y, sp.lo[1], sp.inv[1], sp.dim[1]) == cy;
-					const bool hz = az || cell_of(blo.z, sp.lo[2], sp.inv[2], sp.dim[2]) == cz;
+					const bool hx = ax || cell_of(blo.x, lo0, iv0, d0) == cx;
+					const bool hy = ay || cell_of(blo.y, lo1, iv1, d1) == cy;
+					const bool hz = az || cell_of(blo.z, lo2, iv2, d2) == cz;
 					if (hx && hy && hz) {
 						const uint32_t idb = __float_as_uint(blo.w);
 						const uint32_t lo = min(ida, idb), hi = max(ida, idb);
@@ -369,15 +410,15 @@ template <class Sync>
 __device__ __forceinline__ void bitonic_u32(uint32_t *s, int m, int t, int nt, Sync sync) {
 	for (int k = 2; k <= m; k <<= 1) {
 		for (int j = k >> 1; j > 0; j >>= 1) {
-			for (int i = t; i < m; i += nt) {
-				const int p = i ^ j;
-				if (p > i) {
-					const bool up = (i & k) == 0;
-					const uint32_t x = s[i], y = s[p];
-					if ((x > y) == up) {
-						s[i] = y;
-						s[p] = x;
-					}
+			// compare-exchange q pairs (i, i + j), i with bit j clear: every thread busy
+			for (int q = t; q < (m >> 1); q += nt) {
+				const int i = ((q & ~(j - 1)) << 1) | (q & (j - 1));
+				const int p = i + j;
+				const bool up = (i & k) == 0;
+				const uint32_t x = s[i], y = s[p];
+				if ((x > y) == up) {
+					s[i] = y;
+					s[p] = x;
 				}
 			}
 			sync();
@@ -541,7 +582,11 @@ void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridPar
 }
 
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
-	k_count<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count);
+	if (!n) return;
+	if (b.sm.plans)
+		k_count<true><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm);
+	else
+		k_count<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm);
 }
 
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
@@ -551,16 +596,25 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
 }
 
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
-	if (n) k_scatter<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
-	                                               b.entry_cap, &b.stats->err);
+	if (!n) return;
+	if (b.sm.plans)
+		k_scatter<true><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
+		                                              b.entry_cap, &b.stats->err, b.sm);
+	else
+		k_scatter<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
+		                                               b.entry_cap, &b.stats->err, b.sm);
 }
 
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s) {
 	(void)n;
 	uint64_t want = (entries_hint + kNT - 1) / kNT;
 	unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(want, 1), (uint64_t)kNumSMs * 8);
-	k_pair_test<<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count, b.pairs_tmp,
-	                                 b.pair_cap, &b.stats->pairs);
+	if (b.sm.plans)
+		k_pair_test<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+		                                       b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm);
+	else
+		k_pair_test<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+		                                        b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm);
 }
 
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s) {

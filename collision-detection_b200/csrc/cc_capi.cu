@@ -46,6 +46,10 @@ struct cc_ctx {
 	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes;
 	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
 	    out_depth, out_bids;
+	// batch scratch: offsets, scene of each shape, global body ids, per-scene
+	// stats and plans, scene cell counts and bases, G-scan control, results
+	Buf b_off, b_scene_of, b_gid, b_sst, b_plans, b_G, b_base, b_status, b_ticket, b_res;
+	SceneMap sm;  // set while a batch call runs
 	DevStats *h_stats = nullptr;  // pinned
 	uint64_t *h_word = nullptr;   // pinned scratch words
 	// retained broadphase result (owner buckets not yet scattered)
@@ -221,6 +225,7 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.big_list = ptr<uint32_t>(c->big_list);
 	b.big_cap = c->big_list.bytes / sizeof(uint32_t);
 	b.pre_zeroed = c->pass_zeroed;
+	b.sm = c->sm;
 	return b;
 }
 
@@ -254,8 +259,8 @@ cc_status np_prepare(cc_ctx *c, uint64_t P) {
 // Allocates the n-dependent broadphase scratch and, if np_cap > 0, the
 // narrowphase scratch for np_cap pairs. Buffers only grow; every public call
 // ends with a synchronize, so nothing in flight uses a buffer replaced here.
-cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap) {
-	c->gp.g_max = g_max_for(n);
+cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 0) {
+	c->gp.g_max = g_override ? (uint32_t)g_override : g_max_for(n);
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
 	CC_TRY(ensure(c, c->cell_count, sizeof(uint32_t) * c->gp.g_max));
 	CC_TRY(ensure(c, c->cell_start, sizeof(uint32_t) * (c->gp.g_max + 1)));
@@ -652,7 +657,9 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->np_norm,  &c->np_pa,      &c->np_pb,      &c->np_depth, &c->np_ids,      &c->np_pairs,
 	               &c->np_flag,  &c->np_pos,     &c->np_order, &c->np_classes, &c->in_T,       &c->in_A,     &c->in_B,        &c->in_C,
 	               &c->in_R,     &c->in_ID,      &c->in_pos,     &c->in_rot,   &c->in_act,      &c->out_aabb,
-	               &c->out_pairs, &c->out_norm,  &c->out_pa,     &c->out_pb,   &c->out_depth,   &c->out_bids};
+	               &c->out_pairs, &c->out_norm,  &c->out_pa,     &c->out_pb,   &c->out_depth,   &c->out_bids,
+	               &c->b_off,    &c->b_scene_of, &c->b_gid,      &c->b_sst,    &c->b_plans,     &c->b_G,
+	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
 	if (c->gexec) cudaGraphExecDestroy(c->gexec);
@@ -943,6 +950,137 @@ cc_status cc_narrowphase(cc_ctx *c, uint64_t n, const int32_t *T, const float *A
 		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is >= nb");
 	if (c->h_stats->err & kErrSpinLimit) return set_err(c, CC_ERR_INTERNAL, "device-side look-back wait gave up");
 	*n_contacts = c->h_stats->contacts;
+	return CC_OK;
+}
+
+cc_status cc_collide_batch(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, float envelope, cc_result *res,
+                           uint64_t *scene_pairs, uint64_t *contact_offsets, void *stream) {
+	if (!c || !bt || !res) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	res->n_pairs = res->n_contacts = 0;
+	c->retained = false;
+	const uint64_t S = bt->num_scenes;
+	if (S == 0) return CC_OK;
+	if (S >= 0xffffffffull || !bt->shape_offsets || !bt->body_offsets)
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "num_scenes out of range or null offsets");
+	const cc_scene &sc = bt->scene;
+	if (bt->shape_offsets[0] != 0 || bt->body_offsets[0] != 0 || bt->shape_offsets[S] != sc.n ||
+	    bt->body_offsets[S] != sc.nb)
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "offsets must start at 0 and end at scene.n / scene.nb");
+	uint64_t g_total = 0;
+	for (uint64_t s = 0; s < S; s++) {
+		if (bt->shape_offsets[s + 1] < bt->shape_offsets[s] || bt->body_offsets[s + 1] < bt->body_offsets[s])
+			return set_err(c, CC_ERR_INVALID_ARGUMENT, "offsets decrease at scene %llu", (unsigned long long)s);
+		g_total += batch_scene_cells(bt->shape_offsets[s + 1] - bt->shape_offsets[s]);
+	}
+	if (g_total >= ((uint64_t)1 << 31))
+		return set_err(c, CC_ERR_CAPACITY, "batch needs %llu grid cells (>= 2^31)", (unsigned long long)g_total);
+	CC_TRY(check_grid(c, gx, gy, gz));
+	CC_TRY(check_scene(c, sc.n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot));
+	const uint64_t n = sc.n;
+	if (n == 0) return CC_OK;
+	if (!res->aabb || !sc.active) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb or active array");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	cudaStream_t s = (cudaStream_t)stream;
+	const uint64_t pairs_cap = res->pairs_cap;
+	CC_TRY(prepare(c, n, pairs_cap, std::max<uint64_t>(g_total, 1)));
+	CC_TRY(ensure(c, c->b_off, sizeof(unsigned long long) * 2 * (S + 1)));
+	CC_TRY(ensure(c, c->b_scene_of, sizeof(uint32_t) * n));
+	CC_TRY(ensure(c, c->b_gid, sizeof(uint32_t) * n));
+	CC_TRY(ensure(c, c->b_sst, sizeof(SceneStats) * S));
+	CC_TRY(ensure(c, c->b_plans, sizeof(Plan) * S));
+	CC_TRY(ensure(c, c->b_G, sizeof(uint32_t) * (S + 1)));
+	CC_TRY(ensure(c, c->b_base, sizeof(uint32_t) * (S + 2)));
+	CC_TRY(ensure(c, c->b_status, sizeof(uint64_t) * status_words_for(S + 1)));
+	CC_TRY(ensure(c, c->b_ticket, 64));
+	CC_TRY(ensure(c, c->b_res, sizeof(unsigned long long) * (2 * S + 2)));
+	unsigned long long *d_shape = ptr<unsigned long long>(c->b_off), *d_body = d_shape + (S + 1);
+	CC_CUDA(c, cudaMemcpyAsync(d_shape, bt->shape_offsets, sizeof(uint64_t) * (S + 1), cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(d_body, bt->body_offsets, sizeof(uint64_t) * (S + 1), cudaMemcpyHostToDevice, s));
+	DevStats *d = ptr<DevStats>(c->stats);
+	const int grid[3] = {gx, gy, gz};
+	uint32_t *scene_of = ptr<uint32_t>(c->b_scene_of), *gid = ptr<uint32_t>(c->b_gid);
+	SceneStats *sst = ptr<SceneStats>(c->b_sst);
+	Plan *plans = ptr<Plan>(c->b_plans);
+	uint32_t *G = ptr<uint32_t>(c->b_G), *base = ptr<uint32_t>(c->b_base);
+	unsigned long long *d_pairs_s = ptr<unsigned long long>(c->b_res), *d_coff = d_pairs_s + S;
+	unsigned long long *out = reinterpret_cast<unsigned long long *>(res->pairs);
+	// the rest of the pipeline sees one scene of n shapes with global body ids
+	struct SmGuard {
+		cc_ctx *c;
+		~SmGuard() {
+			c->sm = SceneMap();
+			c->pass_zeroed = false;
+		}
+	} smg_{c};
+	const NpArgs a = {n, sc.nb, sc.T, sc.A, sc.B, sc.C, sc.R, gid, sc.active, sc.body_pos, sc.body_rot, envelope,
+	                  res->pairs, res->norm, res->cpta, res->cptb, res->depth, res->bids};
+	ZeroList zero;
+	zero.p[0] = ptr<uint32_t>(c->status);
+	zero.words[0] = 2 * (c->st_words[0] + c->st_words[1] + c->st_words[2]);
+	zero.p[1] = ptr<uint32_t>(c->ticket);
+	zero.words[1] = 16;
+	zero.p[2] = ptr<uint32_t>(c->np_classes);
+	zero.words[2] = 2 * kNpClasses + 1;
+	zero.p[3] = ptr<uint32_t>(c->cell_count);
+	zero.words[3] = c->gp.g_max;
+	for (int r = 0; r < 4; r++)
+		if (!zero.p[r]) zero.words[r] = 0;
+	{
+		StageMark m(c, ST_AABB, s);
+		CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), s));
+		CC_CUDA(c, cudaMemsetAsync(sst, 0, sizeof(SceneStats) * S, s));
+		launch_batch_prep(n, (uint32_t)S, d_shape, d_body, sc.ID, scene_of, gid, &d->err, s);
+		launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, gid, sc.nb, sc.body_pos, sc.body_rot, res->aabb, nullptr, &d->err,
+		            c->gp, grid, s, zero);
+	}
+	{
+		StageMark m(c, ST_BOUNDS, s);
+		launch_batch_bounds(n, res->aabb, scene_of, sst, &d->err, s);
+		launch_batch_plan((uint32_t)S, d_shape, sst, c->gp, grid, plans, G, s);
+		launch_scan_u32_to_u32(G, S, base, ptr<uint64_t>(c->b_status), ptr<uint32_t>(c->b_ticket), &d->err, s,
+		                       nullptr, &d->cells);
+	}
+	c->launches += 6;
+	c->sm.scene_of = scene_of;
+	c->sm.plans = plans;
+	c->sm.cell_base = base;
+	c->pass_zeroed = true;
+	enqueue_search(c, n, res->aabb, s);
+	enqueue_emit(c, n, out, pairs_cap, s);
+	enqueue_np(c, a, pairs_cap, &d->np_n, s);
+	c->pass_zeroed = false;
+	CC_TRY(check_launch(c));
+	CC_TRY(read_stats(c, s));
+	CC_TRY(device_err(c));
+	CC_TRY(settle(c, n, res->aabb, out, pairs_cap, &a, s));
+	remember(c);
+	const uint64_t P = c->h_stats->pairs;
+	res->n_pairs = P;
+	if (P > pairs_cap)
+		return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries, capacity %llu", (unsigned long long)P,
+		               (unsigned long long)pairs_cap);
+	if (c->h_stats->err & kErrSegmentTooLong) {
+		CC_TRY(sort_fallback(c, n, P, out, s));
+		CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
+		enqueue_np(c, a, pairs_cap, &d->np_n, s);
+		CC_TRY(check_launch(c));
+		CC_TRY(read_stats(c, s));
+	}
+	if (c->h_stats->err & kErrBadIndex)
+		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is outside its scene");
+	res->n_contacts = c->h_stats->contacts;
+	if (scene_pairs || contact_offsets) {
+		launch_batch_offsets((uint32_t)S, d_shape, ptr<unsigned long long>(c->owner_off),
+		                     ptr<unsigned long long>(c->np_pos), d, d_pairs_s, d_coff, s);
+		CC_TRY(check_launch(c));
+		if (scene_pairs)
+			CC_CUDA(c, cudaMemcpyAsync(scene_pairs, d_pairs_s, sizeof(uint64_t) * S, cudaMemcpyDeviceToHost, s));
+		if (contact_offsets)
+			CC_CUDA(c, cudaMemcpyAsync(contact_offsets, d_coff, sizeof(uint64_t) * (S + 1), cudaMemcpyDeviceToHost, s));
+		CC_CUDA(c, cudaStreamSynchronize(s));
+	}
 	return CC_OK;
 }
 

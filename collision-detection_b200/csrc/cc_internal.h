@@ -99,6 +99,16 @@ void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, c
                  const ZeroList &zero = ZeroList());
 
 // ------------------------------------------------------------------ broadphase
+// A batch of independent scenes laid out as one concatenated scene: every
+// scene has its own bounds, reference shift and search grid (plans[s]); the
+// grids occupy disjoint global cell ranges starting at cell_base[s]. Null
+// pointers: a single scene whose plan is DevStats::plan.
+struct SceneMap {
+	const uint32_t *scene_of = nullptr;   // n: scene of every shape
+	const Plan *plans = nullptr;          // per scene
+	const uint32_t *cell_base = nullptr;  // per scene + 1
+};
+
 struct BpBuffers {
 	DevStats *stats;
 	uint32_t *cell_count;    // g_max
@@ -117,6 +127,7 @@ struct BpBuffers {
 	uint64_t *status2 = nullptr;  // look-back tiles of the owner scan (null: shares status)
 	uint32_t *ticket2 = nullptr;
 	bool pre_zeroed = false;      // status/ticket regions were zeroed by the pass's first kernel
+	SceneMap sm;                  // batch layout (empty: one scene)
 };
 
 // Bounds pass over caller AABBs; its last block writes stats->plan.
@@ -134,6 +145,32 @@ void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
 void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+
+// ------------------------------------------------------------------ batches
+// Per-scene accumulators of the batch bounds pass (zeroed per call).
+struct SceneStats {
+	uint32_t bmin_inv[3];  // ~f2ord(min), atomicMax
+	uint32_t bmax[3];      // f2ord(max), atomicMax
+	uint32_t err;
+	uint32_t pad_;
+	double ext_sum[3];
+	unsigned long long count;
+};
+// Cells a scene of n_s shapes may use (the single-scene g_max rule).
+__host__ __device__ inline uint32_t batch_scene_cells(uint64_t n_s) {
+	if (n_s == 0) return 0;
+	const uint64_t g = n_s > 4096 ? n_s : 4096;
+	return (uint32_t)(g < ((uint64_t)1 << 28) ? g : ((uint64_t)1 << 28));
+}
+void launch_batch_prep(uint64_t n, uint32_t S, const unsigned long long *shape_off, const unsigned long long *body_off,
+                       const uint32_t *ID, uint32_t *scene_of, uint32_t *gid, uint32_t *err, cudaStream_t s);
+void launch_batch_bounds(uint64_t n, const float *aabb, const uint32_t *scene_of, SceneStats *sst, uint32_t *err,
+                         cudaStream_t s);
+void launch_batch_plan(uint32_t S, const unsigned long long *shape_off, const SceneStats *sst, const GridParams &gp,
+                       const int grid[3], Plan *plans, uint32_t *G, cudaStream_t s);
+void launch_batch_offsets(uint32_t S, const unsigned long long *shape_off, const unsigned long long *owner_off,
+                          const unsigned long long *np_pos, const DevStats *stats, unsigned long long *scene_pairs,
+                          unsigned long long *contact_off, cudaStream_t s);
 
 // Reference-grid bin list (the reference's internal sorted (bin, body) list).
 void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s);

@@ -187,6 +187,35 @@ typedef struct cc_result {
 CC_API cc_status cc_collide(cc_ctx *ctx, const cc_scene *scene, int gx, int gy, int gz, float envelope, cc_result *res,
                      void *stream);
 
+/* A batch of independent scenes in one call. The scenes are concatenated:
+ * shapes [shape_offsets[s], shape_offsets[s+1]) and bodies
+ * [body_offsets[s], body_offsets[s+1]) belong to scene s, and ID holds body
+ * indices local to each scene. Offsets are HOST arrays of num_scenes + 1
+ * entries starting at 0 and ending at scene.n / scene.nb; all other arrays
+ * are on the device. No reference counterpart: it replaces one
+ * GenerateAABB -> detectPossibleCollisions -> DoNarrowphase sequence
+ * (AABBGenerator.cuh:21-30, Broadphase.cuh:17, Narrowphase.cuh:19-34) per
+ * scene. Every scene gets its own bounds, shift and grid, exactly as a
+ * separate cc_collide would, and no pair crosses scenes. */
+typedef struct cc_batch {
+	uint64_t num_scenes;
+	const uint64_t *shape_offsets; /* host, num_scenes + 1 */
+	const uint64_t *body_offsets;  /* host, num_scenes + 1 */
+	cc_scene scene;                /* the concatenated scenes (device) */
+} cc_batch;
+
+/* cc_collide over a batch. Outputs use the concatenated numbering:
+ * res->aabb holds the mins of all shapes then their maxs (each scene shifted
+ * by its own origin), pair keys are (global a << 32 | global b) with
+ * a = shape_offsets[s] + local index, bids are global body indices. The pair
+ * list is sorted, so it is grouped by scene; contacts come first (stable), so
+ * scene s's contacts are [contact_offsets[s], contact_offsets[s+1]).
+ * scene_pairs (host, num_scenes) receives each scene's pair count;
+ * scene_pairs and contact_offsets (host, num_scenes + 1) may be NULL. On
+ * CC_ERR_CAPACITY res->n_pairs is the size needed (call again). */
+CC_API cc_status cc_collide_batch(cc_ctx *ctx, const cc_batch *batch, int gx, int gy, int gz, float envelope,
+                                  cc_result *res, uint64_t *scene_pairs, uint64_t *contact_offsets, void *stream);
+
 /* Same with HOST pointers in `scene` and `res` (pinned memory recommended):
  * the inputs are copied to context-owned device buffers, the pipeline runs,
  * and aabb (if non-NULL), pairs and contacts are copied back. */
