@@ -65,7 +65,78 @@ def parse():
     ap.add_argument("--n", type=int, default=N_BODIES, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-scene batched measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
     return ap.parse_args()
+
+
+BATCH_WORKLOAD = ("batched_mixed: 512 independent scenes, bodies log-uniform [1,000, 200,000], the 1M workload's "
+                  "shape mix, slab thickness 0.5/d with d ~ U[0.2,1.0] over a 10x10 footprint")
+
+
+def bench_batched(cb, ctx, dev, steps=10):
+    """512 uneven scenes: one cc_collide_batch pass against cc_collide per scene."""
+    import torch
+    from collide_b200 import scenes as S
+    scenes = S.batched_mixed(512, seed=0)
+    N = sum(s.n for s in scenes)
+    db = cb.DeviceBatch(scenes, device=dev)
+    bp = cb.BatchPipeline(db, grid=BINS, ctx=ctx)
+    for _ in range(3):
+        bp.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        bp.run()
+    e1.record()
+    torch.cuda.synchronize()
+    tb = e0.elapsed_time(e1) / steps
+    P, C = bp.n_pairs, bp.n_contacts
+    del bp, db
+    pipes = [cb.DevicePipeline(cb.DeviceScene(s, device=dev), grid=BINS, ctx=ctx) for s in scenes]
+    for p in pipes:
+        p.run()
+    torch.cuda.synchronize()
+    e0.record()
+    for p in pipes:
+        p.run()
+    e1.record()
+    torch.cuda.synchronize()
+    tl = e0.elapsed_time(e1)
+    del pipes
+    torch.cuda.empty_cache()
+    return {"workload": BATCH_WORKLOAD, "scenes": 512, "bodies": N, "pairs": P, "contacts": C,
+            "ms_per_batch": tb, "value": N / (tb / 1000.0), "unit": "bodies/s",
+            "per_scene_launch": {"ms": tl, "value": N / (tl / 1000.0), "unit": "bodies/s",
+                                 "how": "cc_collide once per scene, in order, outputs preallocated"},
+            "speedup_vs_per_scene": tl / tb, "steps": steps}
+
+
+def bench_served(cb, dev, seconds):
+    """Poisson stream (2,000 queries/s, 70% updates / 30% new scenes) on
+    device-resident scenes: continuous batching against the per-query path,
+    plus the capacity of both with about 1,000 queries queued at once."""
+    from collide_b200 import serving as SV
+    pool = [SV.PinnedScene(s) for s in SV.scene_pool(64, seed=0)]
+    out = {"workload": "scene_pool: 64 mixed_slab scenes, bodies log-uniform [2,000, 500,000]; 256 resident at "
+                       "start; updates move bodies by N(0,1e-4^2) and turn them by <= 1e-3 rad; new scenes come "
+                       "from pinned host memory; HBM budget 150 GB",
+           "rate_qps": 2000.0, "duration_s": seconds}
+    for mode in ("batched", "plain"):
+        srv = SV.Server(pool, resident=256, budget_bytes=150e9, max_batch=256, grid=BINS, device=dev)
+        srv.serve(SV.poisson_stream(2000.0, 0.1, resident=256, pool=64, seed=99), mode=mode)  # warm-up
+        r = srv.serve(SV.poisson_stream(2000.0, seconds, resident=256, pool=64, seed=1), mode=mode)
+        cap = srv.serve(SV.poisson_stream(1e6, 1e-3, resident=256, pool=64, seed=2), mode=mode)
+        r["capacity_queries_per_s"] = cap["queries_per_s"]
+        r["capacity_queries"] = cap["queries"]
+        out[mode] = r
+        del srv
+    out["p99_ratio_plain_over_batched"] = out["plain"]["p99_ms"] / out["batched"]["p99_ms"]
+    out["capacity_ratio_batched_over_plain"] = (out["batched"]["capacity_queries_per_s"] /
+                                                 out["plain"]["capacity_queries_per_s"])
+    return out
 
 
 def scene_for(rank, n):
@@ -346,6 +417,10 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and not args.no_batch:
+        line["batched"] = bench_batched(cb, ctx, dev)
+    if rank == 0 and world == 1 and not args.no_serve:
+        line["served"] = bench_served(cb, dev, args.serve_seconds)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(scene, args.cpu_seconds)

@@ -403,8 +403,8 @@ class DevicePipeline:
         self._alloc(int(pairs_cap or max(1024, ds.n // 4)))
         self.n_pairs = self.n_contacts = 0
 
-    def _alloc(self, cap):
-        dev = self.ds.T.device
+    def _alloc(self, cap, dev=None):
+        dev = dev or self.ds.T.device
         self.cap = cap
         self.pairs = torch.empty(cap, dtype=torch.int64, device=dev)
         self.norm = torch.empty((cap, 3), dtype=torch.float32, device=dev)
@@ -490,3 +490,44 @@ def collide_batch(db: DeviceBatch, grid=(16, 16, 16), envelope=0.0, ctx: Context
     return dict(aabb=bp.aabb, pairs=bp.pairs[:P], contact_pairs=bp.pairs[:k], norm=bp.norm[:k], cpta=bp.cpta[:k],
                 cptb=bp.cptb[:k], depth=bp.depth[:k], bids=bp.bids[:k], n_pairs=P, n_contacts=k,
                 scene_pairs=bp.scene_pairs.copy(), contact_offsets=bp.contact_offsets.copy())
+
+
+class ScenesPipeline:
+    """cc_collide_scenes: one batched pass over scenes that stay in their own
+    device allocations (a list of DeviceScene). Outputs as BatchPipeline, in
+    the concatenated numbering of the list's order."""
+
+    def __init__(self, ctx: Context | None = None, grid=(16, 16, 16), envelope=0.0, pairs_cap=1 << 16):
+        self.ctx = ctx or default_context()
+        self.grid, self.envelope = tuple(int(g) for g in grid), float(envelope)
+        self.cap = 0
+        self.aabb = None
+        self._want_cap = int(pairs_cap)
+        self.n_pairs = self.n_contacts = 0
+
+    _alloc = DevicePipeline._alloc
+
+    def run(self, scenes):
+        k = len(scenes)
+        arr = (_lib.Scene * max(k, 1))()
+        for i, d in enumerate(scenes):
+            arr[i] = d.c_scene()
+        n = sum(d.n for d in scenes)
+        dev = scenes[0].T.device if k else torch.device("cuda")
+        if self.aabb is None or self.aabb.shape[0] < 2 * n:
+            self.aabb = torch.empty((max(2 * n, 2), 3), dtype=torch.float32, device=dev)
+        if self.cap < self._want_cap:
+            self._alloc(self._want_cap, dev)
+        self.res.aabb = self.aabb.data_ptr()
+        self.scene_pairs = np.zeros(max(k, 1), np.uint64)
+        self.contact_offsets = np.zeros(k + 1, np.uint64)
+        while True:
+            st = lib.cc_collide_scenes(self.ctx.h, k, arr, *self.grid, self.envelope, ctypes.byref(self.res),
+                                       self.scene_pairs.ctypes.data, self.contact_offsets.ctypes.data, _stream())
+            if st == _lib.CC_ERR_CAPACITY and self.res.n_pairs > self.cap:
+                self._alloc(int(self.res.n_pairs * 5 // 4), dev)
+                self.res.aabb = self.aabb.data_ptr()
+                continue
+            self.ctx.check(st, "cc_collide_scenes")
+            self.n_pairs, self.n_contacts = int(self.res.n_pairs), int(self.res.n_contacts)
+            return self.n_pairs, self.n_contacts

@@ -55,6 +55,8 @@ SIGNATURES = {
     "cc_collide": (I32, [P, P, I32, I32, I32, F32, P, P]),
     "cc_collide_host": (I32, [P, P, I32, I32, I32, F32, P, P]),
     "cc_collide_batch": (I32, [P, P, I32, I32, I32, F32, P, P, P, P]),
+    "cc_collide_scenes": (I32, [P, U64, P, I32, I32, I32, F32, P, P, P, P]),
+    "cc_perturb_bodies": (I32, [P, U64, P, P, U64, F32, F32, P]),
     "cc_last_launch_count": (U64, [P]),
     "cc_set_profiling": (I32, [P, I32]),
     "cc_set_graph_replay": (I32, [P, I32]),

@@ -1,0 +1,230 @@
+"""Serving: a request loop over device-resident scenes with continuous batching.
+
+Scenes stay on the device between queries (one DeviceScene each). A query is
+either a time-step update of a resident scene (positions moved by N(0, s^2),
+orientations turned by a random-axis rotation of at most a given angle: one
+cc_perturb_bodies launch on the device) or a new scene (copied from pinned
+host memory, then admitted). Admission is by byte accounting against an HBM
+budget: a new scene is admitted when its bytes fit, after evicting idle
+scenes least recently used first; otherwise the query is rejected (and
+counted).
+
+Server.serve() runs an arrival stream against the wall clock. In batched
+mode every loop iteration takes ALL queries that have arrived (up to
+max_batch), applies their updates / uploads, and collides their scenes in ONE
+cc_collide_scenes pass, so queries that arrive while a pass is on the GPU
+join the next pass. In plain mode each query runs alone through cc_collide,
+in arrival order (the per-query path). Latency is completion minus arrival;
+the results of a scene are identical alone and in a batch (every scene gets
+its own bounds, shift and grid).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from collections import OrderedDict
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import Context, DevicePipeline, DeviceScene, ScenesPipeline, _stream, lib
+from . import scenes as S
+
+
+def scene_bytes(scene) -> int:
+    """Device bytes a resident scene holds: its inputs plus its AABBs."""
+    return int(scene.nbytes() + 24 * scene.n)
+
+
+def perturb_(ctx: Context, ds: DeviceScene, seed: int, sigma=1e-4, max_angle=1e-3):
+    """Time-step update of a device-resident scene (cc_perturb_bodies)."""
+    ctx.check(lib.cc_perturb_bodies(ctx.h, ds.nb, ds.pos.data_ptr(), ds.rot.data_ptr(), ctypes.c_uint64(seed),
+                                    float(sigma), float(max_angle), _stream()), "cc_perturb_bodies")
+
+
+class PinnedScene:
+    """A host scene in pinned memory, uploaded without a staging copy."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self.n, self.nb = scene.n, scene.nb
+        pin = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).pin_memory()  # noqa: E731
+        self.t = dict(T=pin(scene.T, np.int32), A=pin(scene.A, np.float32), B=pin(scene.B, np.float32),
+                      C=pin(scene.C, np.float32), R=pin(scene.R, np.float32),
+                      ID=pin(np.ascontiguousarray(scene.ID, dtype=np.uint32).view(np.int32), np.int32),
+                      pos=pin(scene.pos, np.float32), rot=pin(scene.rot, np.float32),
+                      active=pin(scene.active, np.uint8))
+
+    def nbytes(self):
+        return self.scene.nbytes()
+
+    def upload(self, device) -> DeviceScene:
+        ds = DeviceScene.__new__(DeviceScene)
+        ds.n, ds.nb = self.n, self.nb
+        for k, v in self.t.items():
+            setattr(ds, k, v.to(device, non_blocking=True))
+        return ds
+
+
+@dataclass
+class Query:
+    arrival: float          # seconds after the stream starts
+    kind: str               # "update" | "new"
+    scene: int              # resident slot (update) or pool index (new)
+    seed: int = 0
+    done: float = math.nan  # completion time, seconds after the start
+    n_pairs: int = 0
+    n_contacts: int = 0
+
+
+@dataclass
+class Stream:
+    queries: list = field(default_factory=list)
+
+
+def poisson_stream(rate=2000.0, duration=1.0, resident=256, pool=64, update_frac=0.7, seed=0) -> Stream:
+    """Poisson arrivals (mean `rate` per second) over `duration` seconds:
+    `update_frac` updates of a random resident scene, the rest new scenes
+    drawn from a pool of `pool` pre-generated scenes."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t, qs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            break
+        if rng.random() < update_frac:
+            qs.append(Query(t, "update", int(rng.integers(0, resident)), int(rng.integers(0, 2**31))))
+        else:
+            qs.append(Query(t, "new", int(rng.integers(0, pool)), int(rng.integers(0, 2**31))))
+    return Stream(qs)
+
+
+def scene_pool(count=64, nmin=2000, nmax=500_000, seed=0):
+    """Scenes of log-uniform size in [nmin, nmax] with the 1M workload's shape
+    mix, for new-scene queries and the initial resident set."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), size=count)).round().astype(np.int64)
+    return [S.mixed_slab(int(n), seed=seed * 7919 + 1 + i, extent=(10.0, 10.0, 0.5)) for i, n in enumerate(sizes)]
+
+
+class Server:
+    def __init__(self, pool, resident=256, budget_bytes=150e9, max_batch=256, grid=(16, 16, 16), precision="exact",
+                 device="cuda"):
+        self.pool = [p if isinstance(p, PinnedScene) else PinnedScene(p) for p in pool]
+        self.device = device
+        self.budget, self.max_batch, self.grid = float(budget_bytes), int(max_batch), tuple(grid)
+        self.ctx = Context()
+        self.ctx.set_narrowphase_precision(precision)
+        self.resident: OrderedDict[int, DeviceScene] = OrderedDict()  # LRU order, oldest first
+        self.bytes = 0
+        self.next_id = 0
+        self.batch = ScenesPipeline(self.ctx, grid=self.grid)
+        self.plain: dict[int, DevicePipeline] = {}
+        self.rejected = 0
+        for i in range(resident):
+            if self.admit(self.pool[i % len(self.pool)]) is None:
+                break
+        self.initial = len(self.resident)
+        self.slots = list(self.resident)  # the scenes update queries address
+        torch.cuda.synchronize()
+
+    # -- residency ------------------------------------------------------
+    def admit(self, ps: PinnedScene, pinned=()):
+        """Makes a pool scene resident; evicts idle scenes (least recently
+        used first, never one in `pinned`) until it fits. Returns its id, or
+        None if it cannot fit."""
+        need = int(ps.nbytes() + 24 * ps.n)
+        if self.bytes + need > self.budget:
+            for sid in [s for s in self.resident if s not in pinned]:
+                if self.bytes + need <= self.budget:
+                    break
+                ds = self.resident.pop(sid)
+                self.bytes -= ds.resident_bytes
+                self.plain.pop(sid, None)
+        if self.bytes + need > self.budget:
+            self.rejected += 1
+            return None
+        ds = ps.upload(self.device)
+        ds.resident_bytes = need
+        sid = self.next_id
+        self.next_id += 1
+        self.resident[sid] = ds
+        self.bytes += need
+        return sid
+
+    def _prepare(self, q: Query, pinned=()):
+        """Applies a query's input; returns its resident scene id (None: the
+        scene is gone or did not fit the budget)."""
+        if q.kind == "new":
+            return self.admit(self.pool[q.scene], pinned)
+        sid = self.slots[q.scene % len(self.slots)]
+        if sid not in self.resident:  # evicted: the update has nothing to move
+            return None
+        self.resident.move_to_end(sid)
+        perturb_(self.ctx, self.resident[sid], q.seed)
+        return sid
+
+    # -- passes ---------------------------------------------------------
+    def collide_batch(self, sids):
+        self.batch.run([self.resident[s] for s in sids])
+        co = self.batch.contact_offsets.astype(np.int64)
+        return [(int(self.batch.scene_pairs[i]), int(co[i + 1] - co[i])) for i in range(len(sids))]
+
+    def collide_one(self, sid):
+        p = self.plain.get(sid)
+        if p is None:
+            p = self.plain[sid] = DevicePipeline(self.resident[sid], grid=self.grid, ctx=self.ctx)
+        return p.run()
+
+    def serve(self, stream: Stream, mode="batched"):
+        qs = stream.queries
+        t0 = time.perf_counter()
+        i = 0  # next query not yet taken
+        passes = []
+        while i < len(qs):
+            now = time.perf_counter() - t0
+            if qs[i].arrival > now:
+                time.sleep(min(qs[i].arrival - now, 2e-4))
+                continue
+            if mode == "plain":
+                q = qs[i]
+                i += 1
+                sid = self._prepare(q)
+                if sid is not None:
+                    q.n_pairs, q.n_contacts = self.collide_one(sid)
+                torch.cuda.synchronize()
+                q.done = time.perf_counter() - t0
+                passes.append(1)
+                continue
+            # batched: everything that has arrived, up to max_batch
+            j = i
+            while j < len(qs) and j - i < self.max_batch and qs[j].arrival <= now:
+                j += 1
+            take = qs[i:j]
+            i = j
+            sids, used = [], set()
+            for q in take:  # scenes already in this pass are not evicted
+                s = self._prepare(q, pinned=used)
+                sids.append(s)
+                if s is not None:
+                    used.add(s)
+            live = [(q, s) for q, s in zip(take, sids) if s is not None]
+            if live:
+                # a scene updated twice in one pass is collided once, after both updates
+                uniq = list(dict.fromkeys(s for _, s in live))
+                res = dict(zip(uniq, self.collide_batch(uniq)))
+                for q, s in live:
+                    q.n_pairs, q.n_contacts = res[s]
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            for q in take:
+                q.done = t
+            passes.append(len(take))
+        wall = time.perf_counter() - t0
+        lat = np.array([q.done - q.arrival for q in qs]) * 1e3
+        return dict(mode=mode, queries=len(qs), wall_s=wall, queries_per_s=len(qs) / wall,
+                    p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
+                    mean_ms=float(lat.mean()), passes=len(passes), mean_pass_queries=float(np.mean(passes)),
+                    rejected=self.rejected, resident=len(self.resident), resident_gb=self.bytes / 1e9)

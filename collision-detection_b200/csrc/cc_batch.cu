@@ -169,7 +169,103 @@ __global__ void __launch_bounds__(kNT) k_batch_offsets(uint32_t S, const unsigne
 	if (s < S) scene_pairs[s] = owner_off[shape_off[s + 1]] - p0;
 	contact_off[s] = np_ok ? np_pos[p0] : 0ull;
 }
+
+// Gathers scenes held in separate allocations into the concatenated layout:
+// one thread per shape (kBodies false) or per body (true).
+template <bool kBodies>
+__global__ void __launch_bounds__(kNT) k_gather(uint64_t n, uint32_t S, const unsigned long long *off,
+                                                 const SceneSrc *src, SceneDst dst) {
+	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kNT) {
+		const uint32_t s = scene_lookup(off, S, i);
+		const uint64_t j = i - __ldg(off + s);
+		const SceneSrc &c = src[s];
+		if constexpr (kBodies) {
+			for (int d = 0; d < 3; d++) dst.pos[3 * i + d] = c.pos[3 * j + d];
+			reinterpret_cast<float4 *>(dst.rot)[i] = reinterpret_cast<const float4 *>(c.rot)[j];
+			dst.active[i] = c.active[j];
+		} else {
+			dst.T[i] = c.T[j];
+			for (int d = 0; d < 3; d++) {
+				dst.A[3 * i + d] = c.A[3 * j + d];
+				dst.B[3 * i + d] = c.B[3 * j + d];
+				dst.C[3 * i + d] = c.C[3 * j + d];
+			}
+			reinterpret_cast<float4 *>(dst.R)[i] = reinterpret_cast<const float4 *>(c.R)[j];
+			dst.ID[i] = c.ID[j];
+		}
+	}
+}
+
+// Counter-based random numbers for the time-step update: SplitMix64's output
+// function (Steele, Lea, Flood 2014) applied to seed + counter, so every body
+// draws the same numbers whatever the launch shape.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+	z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+	z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+	return z ^ (z >> 31);
+}
+__device__ __forceinline__ float unit_open(uint64_t h) {  // (0, 1)
+	return ((float)(h >> 40) + 0.5f) * (1.0f / 16777216.0f);
+}
+// Two standard normals by the Box-Muller transform (Box and Muller, 1958).
+__device__ __forceinline__ float2 normal2(uint64_t key) {
+	const float u1 = unit_open(mix64(key)), u2 = unit_open(mix64(key ^ 0x5851f42d4c957f2dull));
+	const float r = sqrtf(-2.0f * logf(u1));
+	float s, c;
+	sincosf(6.283185307179586f * u2, &s, &c);
+	return make_float2(r * c, r * s);
+}
+
+// pos += N(0, sigma^2); rot = normalize(dq * rot), dq = (cos(a/2), u sin(a/2))
+// with u uniform on the sphere and a ~ U[0, max_angle]. Quaternions (w,x,y,z).
+__global__ void __launch_bounds__(kNT) k_perturb(uint64_t nb, float *__restrict__ pos, float *__restrict__ rot,
+                                                  uint64_t seed, float sigma, float max_angle) {
+	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < nb; i += (uint64_t)gridDim.x * kNT) {
+		const uint64_t key = mix64(seed) + 8 * i;
+		const float2 n01 = normal2(key), n23 = normal2(key + 1), n45 = normal2(key + 2);
+		pos[3 * i] += sigma * n01.x;
+		pos[3 * i + 1] += sigma * n01.y;
+		pos[3 * i + 2] += sigma * n23.x;
+		float ux = n23.y, uy = n45.x, uz = n45.y;
+		const float ul = sqrtf(ux * ux + uy * uy + uz * uz);
+		if (ul > 0.f) {
+			ux /= ul; uy /= ul; uz /= ul;
+		} else {
+			ux = 1.f; uy = 0.f; uz = 0.f;
+		}
+		const float h = 0.5f * max_angle * unit_open(mix64(key + 3));
+		float sh, ch;
+		sincosf(h, &sh, &ch);
+		const float bx = ux * sh, by = uy * sh, bz = uz * sh;
+		float4 q = reinterpret_cast<float4 *>(rot)[i];
+		float4 r;
+		r.x = ch * q.x - bx * q.y - by * q.z - bz * q.w;
+		r.y = ch * q.y + bx * q.x + by * q.w - bz * q.z;
+		r.z = ch * q.z - bx * q.w + by * q.x + bz * q.y;
+		r.w = ch * q.w + bx * q.z - by * q.y + bz * q.x;
+		const float rl = sqrtf(r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w);
+		reinterpret_cast<float4 *>(rot)[i] = make_float4(r.x / rl, r.y / rl, r.z / rl, r.w / rl);
+	}
+}
 }  // namespace
+
+void launch_perturb(uint64_t nb, float *pos, float *rot, uint64_t seed, float sigma, float max_angle, cudaStream_t s) {
+	if (!nb) return;
+	const unsigned g = (unsigned)std::min<uint64_t>((nb + kNT - 1) / kNT, (uint64_t)kNumSMs * 16);
+	k_perturb<<<g, kNT, 0, s>>>(nb, pos, rot, seed, sigma, max_angle);
+}
+
+void launch_gather(uint64_t n, uint64_t nb, uint32_t S, const unsigned long long *shape_off,
+                   const unsigned long long *body_off, const SceneSrc *src, const SceneDst &dst, cudaStream_t s) {
+	if (n) {
+		const unsigned g = (unsigned)std::min<uint64_t>((n + kNT - 1) / kNT, (uint64_t)kNumSMs * 16);
+		k_gather<false><<<g, kNT, 0, s>>>(n, S, shape_off, src, dst);
+	}
+	if (nb) {
+		const unsigned g = (unsigned)std::min<uint64_t>((nb + kNT - 1) / kNT, (uint64_t)kNumSMs * 16);
+		k_gather<true><<<g, kNT, 0, s>>>(nb, S, body_off, src, dst);
+	}
+}
 
 void launch_batch_prep(uint64_t n, uint32_t S, const unsigned long long *shape_off, const unsigned long long *body_off,
                        const uint32_t *ID, uint32_t *scene_of, uint32_t *gid, uint32_t *err, cudaStream_t s) {

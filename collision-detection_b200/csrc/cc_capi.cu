@@ -9,6 +9,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/collide_b200.h"
 #include "cc_common.cuh"
@@ -49,6 +50,8 @@ struct cc_ctx {
 	// batch scratch: offsets, scene of each shape, global body ids, per-scene
 	// stats and plans, scene cell counts and bases, G-scan control, results
 	Buf b_off, b_scene_of, b_gid, b_sst, b_plans, b_G, b_base, b_status, b_ticket, b_res;
+	// gather arena of cc_collide_scenes
+	Buf g_T, g_A, g_B, g_C, g_R, g_ID, g_pos, g_rot, g_act, g_src, g_off;
 	SceneMap sm;  // set while a batch call runs
 	DevStats *h_stats = nullptr;  // pinned
 	uint64_t *h_word = nullptr;   // pinned scratch words
@@ -659,7 +662,9 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->in_R,     &c->in_ID,      &c->in_pos,     &c->in_rot,   &c->in_act,      &c->out_aabb,
 	               &c->out_pairs, &c->out_norm,  &c->out_pa,     &c->out_pb,   &c->out_depth,   &c->out_bids,
 	               &c->b_off,    &c->b_scene_of, &c->b_gid,      &c->b_sst,    &c->b_plans,     &c->b_G,
-	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res};
+	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
+	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
+	               &c->g_act,    &c->g_src,      &c->g_off};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
 	if (c->gexec) cudaGraphExecDestroy(c->gexec);
@@ -953,11 +958,11 @@ cc_status cc_narrowphase(cc_ctx *c, uint64_t n, const int32_t *T, const float *A
 	return CC_OK;
 }
 
-cc_status cc_collide_batch(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, float envelope, cc_result *res,
-                           uint64_t *scene_pairs, uint64_t *contact_offsets, void *stream) {
-	if (!c || !bt || !res) return CC_ERR_INVALID_ARGUMENT;
-	ProfGuard pg_(c, stream);
-	c->launches = 0;
+}  // extern "C"
+
+namespace {
+cc_status batch_impl(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, float envelope, cc_result *res,
+                     uint64_t *scene_pairs, uint64_t *contact_offsets, void *stream) {
 	res->n_pairs = res->n_contacts = 0;
 	c->retained = false;
 	const uint64_t S = bt->num_scenes;
@@ -1082,6 +1087,81 @@ cc_status cc_collide_batch(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz
 		CC_CUDA(c, cudaStreamSynchronize(s));
 	}
 	return CC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+cc_status cc_collide_batch(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, float envelope, cc_result *res,
+                           uint64_t *scene_pairs, uint64_t *contact_offsets, void *stream) {
+	if (!c || !bt || !res) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	return batch_impl(c, bt, gx, gy, gz, envelope, res, scene_pairs, contact_offsets, stream);
+}
+
+cc_status cc_collide_scenes(cc_ctx *c, uint64_t num_scenes, const cc_scene *scenes, int gx, int gy, int gz,
+                            float envelope, cc_result *res, uint64_t *scene_pairs, uint64_t *contact_offsets,
+                            void *stream) {
+	if (!c || !res || (num_scenes && !scenes)) return CC_ERR_INVALID_ARGUMENT;
+	ProfGuard pg_(c, stream);
+	c->launches = 0;
+	res->n_pairs = res->n_contacts = 0;
+	if (num_scenes == 0) return CC_OK;
+	if (num_scenes >= 0xffffffffull) return set_err(c, CC_ERR_INVALID_ARGUMENT, "too many scenes");
+	std::vector<uint64_t> so(num_scenes + 1, 0), bo(num_scenes + 1, 0);
+	std::vector<SceneSrc> src(num_scenes);
+	for (uint64_t s = 0; s < num_scenes; s++) {
+		const cc_scene &x = scenes[s];
+		CC_TRY(check_scene(c, x.n, x.T, x.A, x.B, x.C, x.R, x.ID, x.nb, x.body_pos, x.body_rot));
+		if ((x.n || x.nb) && (!x.active || !x.body_pos || !x.body_rot))
+			return set_err(c, CC_ERR_INVALID_ARGUMENT, "scene %llu: null body arrays", (unsigned long long)s);
+		so[s + 1] = so[s] + x.n;
+		bo[s + 1] = bo[s] + x.nb;
+		src[s] = SceneSrc{x.T, x.A, x.B, x.C, x.R, x.ID, x.body_pos, x.body_rot, x.active};
+	}
+	const uint64_t n = so[num_scenes], nb = bo[num_scenes];
+	CC_CUDA(c, cudaSetDevice(c->device));
+	cudaStream_t s = (cudaStream_t)stream;
+	CC_TRY(ensure(c, c->g_T, 4 * std::max<uint64_t>(n, 1)));
+	CC_TRY(ensure(c, c->g_A, 12 * std::max<uint64_t>(n, 1)));
+	CC_TRY(ensure(c, c->g_B, 12 * std::max<uint64_t>(n, 1)));
+	CC_TRY(ensure(c, c->g_C, 12 * std::max<uint64_t>(n, 1)));
+	CC_TRY(ensure(c, c->g_R, 16 * std::max<uint64_t>(n, 1)));
+	CC_TRY(ensure(c, c->g_ID, 4 * std::max<uint64_t>(n, 1)));
+	CC_TRY(ensure(c, c->g_pos, 12 * std::max<uint64_t>(nb, 1)));
+	CC_TRY(ensure(c, c->g_rot, 16 * std::max<uint64_t>(nb, 1)));
+	CC_TRY(ensure(c, c->g_act, std::max<uint64_t>(nb, 1)));
+	CC_TRY(ensure(c, c->g_src, sizeof(SceneSrc) * num_scenes));
+	CC_TRY(ensure(c, c->g_off, sizeof(unsigned long long) * 2 * (num_scenes + 1)));
+	unsigned long long *d_so = ptr<unsigned long long>(c->g_off), *d_bo = d_so + (num_scenes + 1);
+	CC_CUDA(c, cudaMemcpyAsync(c->g_src.p, src.data(), sizeof(SceneSrc) * num_scenes, cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(d_so, so.data(), sizeof(uint64_t) * (num_scenes + 1), cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, cudaMemcpyAsync(d_bo, bo.data(), sizeof(uint64_t) * (num_scenes + 1), cudaMemcpyHostToDevice, s));
+	SceneDst dst{ptr<int32_t>(c->g_T), ptr<float>(c->g_A), ptr<float>(c->g_B), ptr<float>(c->g_C), ptr<float>(c->g_R),
+	             ptr<uint32_t>(c->g_ID), ptr<float>(c->g_pos), ptr<float>(c->g_rot), ptr<uint8_t>(c->g_act)};
+	{
+		StageMark m(c, ST_COPY_IN, s);
+		launch_gather(n, nb, (uint32_t)num_scenes, d_so, d_bo, ptr<SceneSrc>(c->g_src), dst, s);
+	}
+	c->launches += 2;
+	cc_batch bt;
+	bt.num_scenes = num_scenes;
+	bt.shape_offsets = so.data();
+	bt.body_offsets = bo.data();
+	bt.scene = cc_scene{n, dst.T, dst.A, dst.B, dst.C, dst.R, dst.ID, nb, dst.pos, dst.rot, dst.active};
+	return batch_impl(c, &bt, gx, gy, gz, envelope, res, scene_pairs, contact_offsets, stream);
+}
+
+cc_status cc_perturb_bodies(cc_ctx *c, uint64_t nb, float *body_pos, float *body_rot, uint64_t seed, float sigma,
+                            float max_angle, void *stream) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	if (nb == 0) return CC_OK;
+	if (!body_pos || !body_rot) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null body arrays");
+	if (!aligned16(body_rot)) return set_err(c, CC_ERR_INVALID_ARGUMENT, "body_rot must be 16-byte aligned");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	launch_perturb(nb, body_pos, body_rot, seed, sigma, max_angle, (cudaStream_t)stream);
+	return check_launch(c);
 }
 
 cc_status cc_collide(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz, float envelope, cc_result *res,

@@ -162,6 +162,25 @@ __host__ __device__ inline uint32_t batch_scene_cells(uint64_t n_s) {
 	const uint64_t g = n_s > 4096 ? n_s : 4096;
 	return (uint32_t)(g < ((uint64_t)1 << 28) ? g : ((uint64_t)1 << 28));
 }
+// Device pointers of one scene held in its own allocations, and the
+// concatenated destination (16-byte aligned real4 arrays on both sides).
+struct SceneSrc {
+	const int32_t *T;
+	const float *A, *B, *C, *R;
+	const uint32_t *ID;
+	const float *pos, *rot;
+	const uint8_t *active;
+};
+struct SceneDst {
+	int32_t *T;
+	float *A, *B, *C, *R;
+	uint32_t *ID;
+	float *pos, *rot;
+	uint8_t *active;
+};
+void launch_perturb(uint64_t nb, float *pos, float *rot, uint64_t seed, float sigma, float max_angle, cudaStream_t s);
+void launch_gather(uint64_t n, uint64_t nb, uint32_t S, const unsigned long long *shape_off,
+                   const unsigned long long *body_off, const SceneSrc *src, const SceneDst &dst, cudaStream_t s);
 void launch_batch_prep(uint64_t n, uint32_t S, const unsigned long long *shape_off, const unsigned long long *body_off,
                        const uint32_t *ID, uint32_t *scene_of, uint32_t *gid, uint32_t *err, cudaStream_t s);
 void launch_batch_bounds(uint64_t n, const float *aabb, const uint32_t *scene_of, SceneStats *sst, uint32_t *err,

@@ -216,6 +216,23 @@ typedef struct cc_batch {
 CC_API cc_status cc_collide_batch(cc_ctx *ctx, const cc_batch *batch, int gx, int gy, int gz, float envelope,
                                   cc_result *res, uint64_t *scene_pairs, uint64_t *contact_offsets, void *stream);
 
+/* cc_collide_batch over scenes that live in separate device allocations
+ * (scenes[s] holds scene s's device pointers, IDs local to the scene): the
+ * library gathers them into its own concatenated arena with one kernel, then
+ * runs the batch. Outputs as cc_collide_batch. No reference counterpart. */
+CC_API cc_status cc_collide_scenes(cc_ctx *ctx, uint64_t num_scenes, const cc_scene *scenes, int gx, int gy, int gz,
+                                   float envelope, cc_result *res, uint64_t *scene_pairs, uint64_t *contact_offsets,
+                                   void *stream);
+
+/* A time-step update of device-resident bodies, as a served simulation sends
+ * it: every position component moves by N(0, sigma^2) and every orientation
+ * turns by an angle U[0, max_angle] about a uniform random axis
+ * (rot = normalize(dq * rot)). The random numbers are a pure function of
+ * (seed, body index): the same call gives the same bodies on any launch.
+ * Asynchronous on `stream`. No reference counterpart. */
+CC_API cc_status cc_perturb_bodies(cc_ctx *ctx, uint64_t nb, float *body_pos, float *body_rot, uint64_t seed,
+                                   float sigma, float max_angle, void *stream);
+
 /* Same with HOST pointers in `scene` and `res` (pinned memory recommended):
  * the inputs are copied to context-owned device buffers, the pipeline runs,
  * and aabb (if non-NULL), pairs and contacts are copied back. */

@@ -1,0 +1,97 @@
+"""Serving loop: the arrival stream (CPU), and on the GPU that a scene's
+results are the same alone and inside a batched pass, that admission evicts
+least-recently-used idle scenes and never exceeds the budget, that the
+time-step update is reproducible, and that both serving modes finish a short
+stream."""
+import numpy as np
+import pytest
+import torch
+
+from collide_b200 import scenes as S
+from collide_b200 import serving as SV
+
+
+def test_poisson_stream_rate_and_mix():
+    st = SV.poisson_stream(rate=2000.0, duration=2.0, resident=100, pool=10, update_frac=0.7, seed=3)
+    n = len(st.queries)
+    assert abs(n - 4000) < 4 * np.sqrt(4000)
+    arr = np.array([q.arrival for q in st.queries])
+    assert np.all(np.diff(arr) >= 0) and arr[-1] < 2.0
+    frac = np.mean([q.kind == "update" for q in st.queries])
+    assert abs(frac - 0.7) < 0.05
+    assert all(0 <= q.scene < (100 if q.kind == "update" else 10) for q in st.queries)
+
+
+def test_scene_bytes_counts_inputs_and_boxes():
+    sc = S.mixed_slab(1000, seed=1)
+    assert SV.scene_bytes(sc) == sc.nbytes() + 24 * 1000
+
+
+@pytest.mark.gpu
+def test_results_same_alone_and_in_the_mix(cb):
+    pool = [S.mixed_slab(n, seed=n, extent=(1.0, 1.0, 0.1)) for n in (3000, 12000, 800, 25000)]
+    srv = SV.Server(pool, resident=4, max_batch=16)
+    sids = list(srv.resident)
+    srv.batch.run([srv.resident[s] for s in sids])
+    b = srv.batch
+    co = b.contact_offsets.astype(np.int64)
+    ctx = cb.Context()
+    assert b.n_contacts > 0
+    for i, s in enumerate(sids):
+        alone = cb.DevicePipeline(srv.resident[s], ctx=ctx)
+        P, C = alone.run()
+        assert int(b.scene_pairs[i]) == P and co[i + 1] - co[i] == C
+        sl = slice(co[i], co[i + 1])
+        assert torch.equal(b.norm[sl], alone.norm[:C]) and torch.equal(b.depth[sl], alone.depth[:C])
+        assert torch.equal(b.cpta[sl], alone.cpta[:C]) and torch.equal(b.cptb[sl], alone.cptb[:C])
+
+
+@pytest.mark.gpu
+def test_admission_evicts_lru_within_budget(cb):
+    pool = [S.mixed_slab(1000, seed=i) for i in range(6)]
+    one = SV.scene_bytes(pool[0])
+    srv = SV.Server(pool, resident=3, budget_bytes=3.5 * one)
+    assert srv.initial == 3 and srv.bytes <= srv.budget
+    first = list(srv.resident)[0]
+    srv.resident.move_to_end(first)  # used recently: the second-oldest goes first
+    second = list(srv.resident)[0]
+    sid = srv.admit(srv.pool[4])
+    assert sid is not None and second not in srv.resident and first in srv.resident
+    assert srv.bytes <= srv.budget
+    big = SV.PinnedScene(S.mixed_slab(5000, seed=9))
+    assert srv.admit(big) is None and srv.rejected == 1
+
+
+@pytest.mark.gpu
+def test_time_step_update_is_reproducible_and_small(cb):
+    sc = S.mixed_slab(20000, seed=4)
+    ctx = cb.Context()
+    a, b = cb.DeviceScene(sc), cb.DeviceScene(sc)
+    SV.perturb_(ctx, a, 123)
+    SV.perturb_(ctx, b, 123)
+    torch.cuda.synchronize()
+    assert torch.equal(a.pos, b.pos) and torch.equal(a.rot, b.rot)
+    d = (a.pos.cpu().numpy() - sc.pos).ravel()
+    assert abs(d.std() - 1e-4) < 5e-6 and abs(d.mean()) < 5e-6
+    q = a.rot.cpu().numpy().astype(np.float64)
+    assert np.allclose(np.linalg.norm(q, axis=1), 1.0, atol=1e-6)
+    # rotation angle of q * conj(q0), from its vector part (well conditioned near 0)
+    q0 = sc.rot.astype(np.float64)
+    w0, v0 = q0[:, :1], -q0[:, 1:]
+    w1, v1 = q[:, :1], q[:, 1:]
+    v = w1 * v0 + w0 * v1 + np.cross(v1, v0)
+    w = w1 * w0 - np.sum(v1 * v0, axis=1, keepdims=True)
+    ang = 2 * np.arctan2(np.linalg.norm(v, axis=1), np.abs(w[:, 0]))
+    assert ang.max() <= 1.0e-3 + 1e-6 and ang.mean() > 3e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_serve_short_stream(cb, mode):
+    pool = [S.mixed_slab(n, seed=n, extent=(2.0, 2.0, 0.2)) for n in (2000, 5000, 9000, 3000)]
+    srv = SV.Server(pool, resident=8, max_batch=32)
+    st = SV.poisson_stream(rate=400.0, duration=0.25, resident=8, pool=4, seed=1)
+    r = srv.serve(st, mode=mode)
+    assert r["queries"] == len(st.queries) > 20
+    assert all(np.isfinite(q.done) and q.done >= q.arrival for q in st.queries)
+    assert r["p99_ms"] >= r["p50_ms"] > 0
