@@ -152,11 +152,15 @@ class DeviceScene:
         return (self.T, self.A, self.B, self.C, self.R, self.ID, self.pos, self.rot)
 
     def c_scene(self):
+        c = getattr(self, "_c", None)
+        if c is not None:  # the tensors are only ever updated in place
+            return c
         s = _lib.Scene()
         s.n, s.nb = self.n, self.nb
         s.T, s.A, s.B, s.C = self.T.data_ptr(), self.A.data_ptr(), self.B.data_ptr(), self.C.data_ptr()
         s.R, s.ID = self.R.data_ptr(), self.ID.data_ptr()
         s.body_pos, s.body_rot, s.active = self.pos.data_ptr(), self.rot.data_ptr(), self.active.data_ptr()
+        self._c = s
         return s
 
 

@@ -111,7 +111,14 @@ def scene_pool(count=64, nmin=2000, nmax=500_000, seed=0):
 
 class Server:
     def __init__(self, pool, resident=256, budget_bytes=150e9, max_batch=256, grid=(16, 16, 16), precision="exact",
-                 device="cuda"):
+                 device="cuda", reserve_bytes=None):
+        # reserve the working set up front (torch keeps a freed block cached
+        # and carves later scenes from it): admitting a scene then costs a
+        # copy, not a device allocation
+        reserve = int(min(budget_bytes, 32e9) if reserve_bytes is None else reserve_bytes)
+        if reserve > 0:
+            del_me = torch.empty(reserve, dtype=torch.uint8, device=device)
+            del del_me
         self.pool = [p if isinstance(p, PinnedScene) else PinnedScene(p) for p in pool]
         self.device = device
         self.budget, self.max_batch, self.grid = float(budget_bytes), int(max_batch), tuple(grid)
@@ -128,6 +135,11 @@ class Server:
                 break
         self.initial = len(self.resident)
         self.slots = list(self.resident)  # the scenes update queries address
+        # size the library's scratch once for a full pass over resident scenes
+        # (it only grows, by half at a time, after that)
+        warm = [self.resident[s] for s in self.slots[: self.max_batch]]
+        if warm:
+            self.batch.run(warm)
         torch.cuda.synchronize()
 
     # -- residency ------------------------------------------------------

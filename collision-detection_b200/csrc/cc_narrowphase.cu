@@ -62,7 +62,6 @@ __device__ __forceinline__ int type_cost(int t) {
 	default: return 2;
 	}
 }
-constexpr int kMaxClassCost = 8;
 // Sphere-sphere pairs take the analytic path and invalid pairs do nothing:
 // cost 0.
 __device__ __forceinline__ int class_cost(int c) {
@@ -89,15 +88,22 @@ __global__ void __launch_bounds__(256) k_np_class_scatter(uint64_t P, const unsi
                                                            const int32_t *__restrict__ T,
                                                            const long long *__restrict__ pairs, uint32_t *classes,
                                                            uint32_t *__restrict__ order) {
-	__shared__ uint32_t off[kNpClasses];
-	if (threadIdx.x == 0) {  // classes in order of descending class_cost, so the longest pairs start first
+	// classes in order of descending class_cost (ties by class id), so the
+	// longest pairs start first: class c begins after every class ranked
+	// before it
+	__shared__ uint32_t off[kNpClasses], cnt[kNpClasses];
+	__shared__ int cost[kNpClasses];
+	if (threadIdx.x < kNpClasses) {
+		cnt[threadIdx.x] = classes[threadIdx.x];
+		cost[threadIdx.x] = class_cost(threadIdx.x);
+	}
+	__syncthreads();
+	if (threadIdx.x < kNpClasses) {
+		const int c = threadIdx.x, k = cost[c];
 		uint32_t acc = 0;
-		for (int cost = kMaxClassCost; cost >= 0; cost--)
-			for (int c = 0; c < kNpClasses; c++)
-				if (class_cost(c) == cost) {
-					off[c] = acc;
-					acc += classes[c];
-				}
+		for (int d = 0; d < kNpClasses; d++)
+			if (cost[d] > k || (cost[d] == k && d < c)) acc += cnt[d];
+		off[c] = acc;
 	}
 	__syncthreads();
 	uint32_t *cursor = classes + kNpClasses;

@@ -30,7 +30,7 @@ def test_scene_bytes_counts_inputs_and_boxes():
 @pytest.mark.gpu
 def test_results_same_alone_and_in_the_mix(cb):
     pool = [S.mixed_slab(n, seed=n, extent=(1.0, 1.0, 0.1)) for n in (3000, 12000, 800, 25000)]
-    srv = SV.Server(pool, resident=4, max_batch=16)
+    srv = SV.Server(pool, resident=4, max_batch=16, reserve_bytes=1 << 28)
     sids = list(srv.resident)
     srv.batch.run([srv.resident[s] for s in sids])
     b = srv.batch
@@ -50,7 +50,7 @@ def test_results_same_alone_and_in_the_mix(cb):
 def test_admission_evicts_lru_within_budget(cb):
     pool = [S.mixed_slab(1000, seed=i) for i in range(6)]
     one = SV.scene_bytes(pool[0])
-    srv = SV.Server(pool, resident=3, budget_bytes=3.5 * one)
+    srv = SV.Server(pool, resident=3, budget_bytes=3.5 * one, reserve_bytes=0)
     assert srv.initial == 3 and srv.bytes <= srv.budget
     first = list(srv.resident)[0]
     srv.resident.move_to_end(first)  # used recently: the second-oldest goes first
@@ -89,7 +89,7 @@ def test_time_step_update_is_reproducible_and_small(cb):
 @pytest.mark.parametrize("mode", ["batched", "plain"])
 def test_serve_short_stream(cb, mode):
     pool = [S.mixed_slab(n, seed=n, extent=(2.0, 2.0, 0.2)) for n in (2000, 5000, 9000, 3000)]
-    srv = SV.Server(pool, resident=8, max_batch=32)
+    srv = SV.Server(pool, resident=8, max_batch=32, reserve_bytes=1 << 28)
     st = SV.poisson_stream(rate=400.0, duration=0.25, resident=8, pool=4, seed=1)
     r = srv.serve(st, mode=mode)
     assert r["queries"] == len(st.queries) > 20
