@@ -146,14 +146,14 @@ def scene_for(rank, n):
 
 # ---------------------------------------------------------------------------- clocks
 class Clocks:
-    """nvidia-smi sampling (every 100 ms, with host timestamps) started before
-    the warm-up; samples falling inside the timed window (widened by one
-    interval on each side, since a window shorter than the interval would
-    otherwise hold none) are summarised."""
+    """nvidia-smi sampling (every 25 ms, with host timestamps) started before
+    the warm-up; samples falling inside the timed windows (the device-resident
+    pass through the end of the e2e pass, widened by one interval on each
+    side) are summarised."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-    PERIOD = 0.1
+    PERIOD = 0.025
 
     def __init__(self, index):
         import threading
@@ -283,6 +283,16 @@ def run_reference(args):
         times.append(float(t.sum()))
     ms = 1000.0 * sum(times) / len(times)
     value = scene.n / (ms / 1000.0)
+    # the broadphase as one unit: the single-pass byte model 88N + 56E + 16C + 8P
+    # (C = candidates; the home-cell test emits none twice, so C = P here) over
+    # the summed stage times from the shift/count pass to the sorted list
+    bp_stages = ("count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
+    bp_ms = sum(kern[k][0] / kern[k][1] for k in bp_stages if k in kern)
+    bp_bytes = 88 * scene.n + 56 * E + 16 * P + 8 * P
+    bp_roof = {"bound": "hbm", "stages": list(bp_stages), "ms": bp_ms,
+               "model_bytes": bp_bytes, "achieved": bp_bytes / (bp_ms / 1000.0) / 1e9, "peak": hbm, "unit": "GB/s",
+               "frac": bp_bytes / (bp_ms / 1000.0) / 1e9 / hbm,
+               "floor_bytes": 24 * scene.n + 8 * P, "pairs_per_s": P / (bp_ms / 1000.0)}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -356,8 +366,7 @@ def run_ours(args):
     clocks = Clocks(local)
     clocks.wait_first()
     total_ms, launches, _, window = timed_pass(False)
-    clocks.mark(*window)
-    clk = clocks.stop()
+    t_first = window[0]
     total_ms = dist_max(total_ms, world)
     ms = total_ms / args.steps
     value = world * scene.n / (ms / 1000.0)
@@ -365,7 +374,11 @@ def run_ours(args):
     # event records add host work, so this pass is not the value above)
     prof_ms, _, stage, _ = timed_pass(True)
 
-    # ---- e2e: the host-pointer entry point, copies inside the timed region
+    # ---- e2e: the host-pointer entry points, copies inside the timed region.
+    # Blocking: cc_collide_host per step. Pipelined (the e2e value): steps
+    # submitted two in flight (cc_collide_host_submit / _wait), so the copy of
+    # step k+1's inputs overlaps step k's pipeline; every step still copies all
+    # of its inputs in and its pairs and contacts out.
     hs = cb.HostSession(scene, grid=BINS, ctx=ctx)
     for i in range(2):
         hs.run()
@@ -378,9 +391,32 @@ def run_ours(args):
         hs.run()
         evs2[i][1].record(stream)
     torch.cuda.synchronize()
-    e2e_ms = dist_max(sum(a.elapsed_time(b) for a, b in evs2) / args.steps, world)
+    blocking_ms = dist_max(sum(a.elapsed_time(b) for a, b in evs2) / args.steps, world)
+    hp = cb.HostSession(scene, grid=BINS, ctx=ctx)
+    for i in range(3):
+        hp.submit()
+        hp.wait()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    hp.submit()
+    for i in range(1, args.steps):
+        hp.submit()
+        hp.wait()
+    hp.wait()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks.mark(t_first, time.time())
+    clk = clocks.stop()
+    assert (hp.n_pairs, hp.n_contacts) == (hs.n_pairs, hs.n_contacts)
+    e2e_ms = dist_max(e0.elapsed_time(e1) / args.steps, world)
     e2e = {"value": world * scene.n / (e2e_ms / 1000.0), "unit": UNIT, "ms_per_step": e2e_ms,
-           "h2d_bytes_per_step": hs.input_bytes(), "d2h_bytes_per_step": hs.output_bytes()}
+           "h2d_bytes_per_step": hp.input_bytes(), "d2h_bytes_per_step": hp.output_bytes(),
+           "how": "cc_collide_host_submit/_wait, two steps in flight, pinned host buffers; CUDA events on the "
+                  "caller's stream around all steps",
+           "blocking": {"ms_per_step": blocking_ms, "value": world * scene.n / (blocking_ms / 1000.0),
+                        "how": "cc_collide_host, one step at a time"}}
 
     # ---- roofline of the dominant kernel stage
     peaks = {}
@@ -400,6 +436,16 @@ def run_ours(args):
                          "algorithmic_GBps": STAGE_BYTES[k](scene.n, E, G, P, C) / (v[0] / v[1] / 1000) / 1e9}
                      for k, v in kern.items()}
 
+    # the broadphase as one unit: the single-pass byte model 88N + 56E + 16C + 8P
+    # (C = candidates; the home-cell test emits none twice, so C = P here) over
+    # the summed stage times from the shift/count pass to the sorted list
+    bp_stages = ("count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
+    bp_ms = sum(kern[k][0] / kern[k][1] for k in bp_stages if k in kern)
+    bp_bytes = 88 * scene.n + 56 * E + 16 * P + 8 * P
+    bp_roof = {"bound": "hbm", "stages": list(bp_stages), "ms": bp_ms,
+               "model_bytes": bp_bytes, "achieved": bp_bytes / (bp_ms / 1000.0) / 1e9, "peak": hbm, "unit": "GB/s",
+               "frac": bp_bytes / (bp_ms / 1000.0) / 1e9 / hbm,
+               "floor_bytes": 24 * scene.n + 8 * P, "pairs_per_s": P / (bp_ms / 1000.0)}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -413,6 +459,7 @@ def run_ours(args):
                      "algorithmic_bytes_per_launch": dom_bytes, "traffic": traffic_from_profiles(dom),
                      "timing": "CUDA events around each stage on the launch stream, over a second pass of the "
                                f"same {args.steps} steps ({prof_ms / args.steps:.4f} ms/step with the events)"},
+        "roofline_broadphase": bp_roof,
         "stages": stage_summary,
         "gpu_launches": launches,
         "clocks": clk,

@@ -24,6 +24,7 @@ PyTorch only provides device memory and the current stream here.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -40,6 +41,49 @@ _default_ctx = {}
 
 def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def gpu_local_cpus(device=None):
+    """CPUs on the GPU's own NUMA node (NVML), or None if unknown. Host
+    buffers that feed the GPU belong on that node: a copy from the other
+    socket's memory crosses the inter-socket link first."""
+    try:
+        import pynvml
+        if device is None:
+            device = torch.cuda.current_device()
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(device)
+        try:  # the same GPU as CUDA's device index, whatever CUDA_VISIBLE_DEVICES says
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(device)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, 64)
+        cpus = {64 * i + b for i, w in enumerate(words) for b in range(64) if (w >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+    except Exception:
+        return None
+
+
+class numa_local:
+    """Context manager: the calling thread runs on the GPU's NUMA node while
+    host buffers are allocated (pinned pages are placed where they are first
+    touched), then gets its old CPU set back."""
+
+    def __init__(self, device=None):
+        self.device = device
+
+    def __enter__(self):
+        self.old = os.sched_getaffinity(0)
+        cpus = gpu_local_cpus(self.device)
+        if cpus:
+            os.sched_setaffinity(0, cpus)
+        return self
+
+    def __exit__(self, *exc):
+        os.sched_setaffinity(0, self.old)
+        return False
 
 
 def _ptr(t, dtype=None, name="tensor"):
@@ -337,13 +381,14 @@ class HostSession:
         self.grid, self.envelope = tuple(int(g) for g in grid), float(envelope)
         pin = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).pin_memory()  # noqa: E731
         self.n, self.nb = scene.n, scene.nb
-        self.inputs = [pin(scene.T, np.int32), pin(scene.A, np.float32), pin(scene.B, np.float32),
-                       pin(scene.C, np.float32), pin(scene.R, np.float32),
-                       pin(np.ascontiguousarray(scene.ID, dtype=np.uint32).view(np.int32), np.int32),
-                       pin(scene.pos, np.float32), pin(scene.rot, np.float32), pin(scene.active, np.uint8)]
         self.want_aabb = want_aabb
         self.n_pairs = self.n_contacts = 0
-        self._alloc(int(pairs_cap or max(1024, self.n // 4)))
+        with numa_local(self.ctx.device):  # pinned buffers on the GPU's node
+            self.inputs = [pin(scene.T, np.int32), pin(scene.A, np.float32), pin(scene.B, np.float32),
+                           pin(scene.C, np.float32), pin(scene.R, np.float32),
+                           pin(np.ascontiguousarray(scene.ID, dtype=np.uint32).view(np.int32), np.int32),
+                           pin(scene.pos, np.float32), pin(scene.rot, np.float32), pin(scene.active, np.uint8)]
+            self._alloc(int(pairs_cap or max(1024, self.n // 4)))
 
     def _alloc(self, cap):
         self.cap = cap
@@ -383,6 +428,50 @@ class HostSession:
             self.ctx.check(st, "cc_collide_host")
             self.n_pairs, self.n_contacts = int(res.n_pairs), int(res.n_contacts)
             return self.n_pairs, self.n_contacts
+
+    # -- pipelined steps: submit() returns at once, wait() finishes the oldest
+    def _structs(self):
+        T, A, B, C, R, ID, pos, rot, act = self.inputs
+        sc = _lib.Scene()
+        sc.n, sc.nb = self.n, self.nb
+        sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID = (T.data_ptr(), A.data_ptr(), B.data_ptr(), C.data_ptr(),
+                                                R.data_ptr(), ID.data_ptr())
+        sc.body_pos, sc.body_rot, sc.active = pos.data_ptr(), rot.data_ptr(), act.data_ptr()
+        res = _lib.Result()
+        res.aabb = self.aabb.data_ptr() if self.aabb is not None else None
+        res.pairs, res.pairs_cap = self.pairs.data_ptr(), self.cap
+        res.norm, res.cpta, res.cptb = self.norm.data_ptr(), self.cpta.data_ptr(), self.cptb.data_ptr()
+        res.depth, res.bids = self.depth.data_ptr(), self.bids.data_ptr()
+        # the structs and the buffers they point at stay alive while a step uses them
+        keep = (self.aabb, self.pairs, self.norm, self.cpta, self.cptb, self.depth, self.bids)
+        self._cur = (sc, res, keep)
+
+    def submit(self):
+        """cc_collide_host_submit: enqueue one step (at most two in flight).
+        The host inputs must stay unchanged until the step's wait()."""
+        if getattr(self, "_cur", None) is None:
+            self._structs()
+        if not hasattr(self, "_pending"):
+            self._pending = []
+        sc, res, keep = self._cur
+        self.ctx.check(lib.cc_collide_host_submit(self.ctx.h, ctypes.byref(sc), *self.grid, self.envelope,
+                                                  ctypes.byref(res), _stream()), "cc_collide_host_submit")
+        self._pending.append(self._cur)
+
+    def wait(self):
+        """cc_collide_host_wait: finish the oldest submitted step; its pairs
+        and contacts are in this session's host buffers until the next wait."""
+        sc, res, keep = self._pending.pop(0)
+        st = lib.cc_collide_host_wait(self.ctx.h, ctypes.byref(res), _stream())
+        if st == _lib.CC_ERR_CAPACITY and res.n_pairs > res.pairs_cap:
+            # larger buffers for the steps to come; this one runs again blocking
+            if res.n_pairs > self.cap:
+                self._alloc(int(res.n_pairs) * 5 // 4)
+                self._cur = None
+            return self.run()
+        self.ctx.check(st, "cc_collide_host_wait")
+        self.n_pairs, self.n_contacts = int(res.n_pairs), int(res.n_contacts)
+        return self.n_pairs, self.n_contacts
 
 
 def collide_host(scene, grid=(16, 16, 16), envelope=0.0, ctx: Context | None = None):

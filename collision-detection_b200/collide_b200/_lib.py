@@ -54,6 +54,8 @@ SIGNATURES = {
     "cc_narrowphase": (I32, [P, U64, P, P, P, P, P, P, U64, P, P, P, F32, P, U64, P, P, P, P, P, PU64, P]),
     "cc_collide": (I32, [P, P, I32, I32, I32, F32, P, P]),
     "cc_collide_host": (I32, [P, P, I32, I32, I32, F32, P, P]),
+    "cc_collide_host_submit": (I32, [P, P, I32, I32, I32, F32, P, P]),
+    "cc_collide_host_wait": (I32, [P, P, P]),
     "cc_collide_batch": (I32, [P, P, I32, I32, I32, F32, P, P, P, P]),
     "cc_collide_scenes": (I32, [P, U64, P, I32, I32, I32, F32, P, P, P, P]),
     "cc_perturb_bodies": (I32, [P, U64, P, P, U64, F32, F32, P]),

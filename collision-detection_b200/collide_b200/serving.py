@@ -29,7 +29,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import Context, DevicePipeline, DeviceScene, ScenesPipeline, _stream, lib
+from . import Context, DevicePipeline, DeviceScene, ScenesPipeline, _stream, lib, numa_local
 from . import scenes as S
 
 
@@ -51,11 +51,16 @@ class PinnedScene:
         self.scene = scene
         self.n, self.nb = scene.n, scene.nb
         pin = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).pin_memory()  # noqa: E731
-        self.t = dict(T=pin(scene.T, np.int32), A=pin(scene.A, np.float32), B=pin(scene.B, np.float32),
-                      C=pin(scene.C, np.float32), R=pin(scene.R, np.float32),
-                      ID=pin(np.ascontiguousarray(scene.ID, dtype=np.uint32).view(np.int32), np.int32),
-                      pos=pin(scene.pos, np.float32), rot=pin(scene.rot, np.float32),
-                      active=pin(scene.active, np.uint8))
+        with numa_local():  # pages on the GPU's NUMA node
+            self.t = self._pin(scene, pin)
+
+    @staticmethod
+    def _pin(scene, pin):
+        return dict(T=pin(scene.T, np.int32), A=pin(scene.A, np.float32), B=pin(scene.B, np.float32),
+                    C=pin(scene.C, np.float32), R=pin(scene.R, np.float32),
+                    ID=pin(np.ascontiguousarray(scene.ID, dtype=np.uint32).view(np.int32), np.int32),
+                    pos=pin(scene.pos, np.float32), rot=pin(scene.rot, np.float32),
+                    active=pin(scene.active, np.uint8))
 
     def nbytes(self):
         return self.scene.nbytes()

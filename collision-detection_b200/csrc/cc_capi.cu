@@ -64,6 +64,24 @@ struct cc_ctx {
 	int np_precision = CC_NP_EXACT;
 	// scratch generation: bumped whenever ensure() moves a buffer
 	uint64_t buf_gen = 0;
+	// ensure() in dry-run mode records would_grow instead of reallocating
+	bool dry_run = false, would_grow = false;
+	// pipelined host steps (cc_collide_host_submit / _wait): two slots of
+	// device inputs and outputs; copies in on one stream, the pipeline on
+	// another, copies out on a third
+	struct HostSlot {
+		Buf T, A, B, C, R, ID, pos, rot, act, aabb, pairs, norm, pa, pb, depth, bids;
+		cudaEvent_t in_done = nullptr, done = nullptr;
+		DevStats *h_stats = nullptr;  // pinned copy of the step's counters
+		cc_scene dev{};
+		cc_result *res = nullptr;
+		int grid[3] = {0, 0, 0};
+		float env = 0.f;
+		uint64_t cap = 0, entry_cap = 0, pair_cap = 0;
+	} hs[2];
+	cudaStream_t hs_copy = nullptr, hs_comp = nullptr, hs_out = nullptr;
+	cudaEvent_t hs_user = nullptr, hs_back = nullptr;
+	int hs_next = 0, hs_oldest = 0, hs_inflight = 0;
 	// look-back status regions (words) of the cell, owner and contact-flag
 	// scans, laid out back to back in `status`
 	uint64_t st_words[3] = {0, 0, 0};
@@ -118,6 +136,10 @@ cc_status set_err(cc_ctx *c, cc_status st, const char *fmt, ...) {
 
 cc_status ensure(cc_ctx *c, Buf &b, size_t bytes) {
 	if (bytes <= b.bytes) return CC_OK;
+	if (c->dry_run) {  // only report that this call would reallocate
+		c->would_grow = true;
+		return CC_OK;
+	}
 	size_t nb = std::max(bytes, b.bytes + b.bytes / 2);
 	nb = (nb + 255) & ~size_t(255);
 	if (b.p) {
@@ -492,16 +514,13 @@ cc_status check_grid(cc_ctx *c, int gx, int gy, int gz) {
 	return CC_OK;
 }
 
-// GenerateAABB -> broadphase -> narrowphase on device pointers with one
-// synchronize in the common case.
-cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
-                      int64_t *pairs, uint64_t pairs_cap, float *norm, float *cpta, float *cptb, float *depth,
-                      int32_t *bids, uint64_t *n_pairs, uint64_t *n_contacts, cudaStream_t s) {
-	*n_pairs = 0;
-	*n_contacts = 0;
+// The first half of collide_dev: sizes the scratch and enqueues the whole step
+// on `s` (or replays its graph when `graphs`), without waiting.
+cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
+                          int64_t *pairs, uint64_t pairs_cap, float *norm, float *cpta, float *cptb, float *depth,
+                          int32_t *bids, cudaStream_t s, bool graphs) {
 	c->retained = false;
 	const uint64_t n = sc.n;
-	if (n == 0) return CC_OK;
 	CC_TRY(prepare(c, n, pairs_cap));
 	DevStats *d = ptr<DevStats>(c->stats);
 	const int grid[3] = {gx, gy, gz};
@@ -537,7 +556,7 @@ cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, flo
 		return CC_OK;
 	};
 	bool replayed = false;
-	if (!c->prof && !c->graph_off) {
+	if (graphs && !c->prof && !c->graph_off) {
 		// everything the captured launches depend on
 		struct {
 			uint64_t n, nb, pairs_cap, hE, hP, gen, st[3];
@@ -601,8 +620,19 @@ cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, flo
 	} else {
 		CC_TRY(enqueue_all(s));
 	}
-	CC_TRY(check_launch(c));
-	CC_TRY(read_stats(c, s));
+	return check_launch(c);
+}
+
+// The second half: with c->h_stats current (the step's DevStats), checks
+// errors, redoes passes whose scratch was too small, and reports the counts.
+cc_status collide_finish(cc_ctx *c, const cc_scene &sc, float envelope, float *aabb, int64_t *pairs,
+                         uint64_t pairs_cap, float *norm, float *cpta, float *cptb, float *depth, int32_t *bids,
+                         uint64_t *n_pairs, uint64_t *n_contacts, cudaStream_t s) {
+	const uint64_t n = sc.n;
+	DevStats *d = ptr<DevStats>(c->stats);
+	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
+	const NpArgs a = {n, sc.nb, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, envelope,
+	                  pairs, norm, cpta, cptb, depth, bids};
 	CC_TRY(device_err(c));
 	CC_TRY(settle(c, n, aabb, out, pairs_cap, &a, s));
 	remember(c);
@@ -625,6 +655,22 @@ cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, flo
 		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is >= nb");
 	*n_contacts = c->h_stats->contacts;
 	return CC_OK;
+}
+
+// GenerateAABB -> broadphase -> narrowphase on device pointers with one
+// synchronize in the common case.
+cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
+                      int64_t *pairs, uint64_t pairs_cap, float *norm, float *cpta, float *cptb, float *depth,
+                      int32_t *bids, uint64_t *n_pairs, uint64_t *n_contacts, cudaStream_t s) {
+	*n_pairs = 0;
+	*n_contacts = 0;
+	c->retained = false;
+	if (sc.n == 0) return CC_OK;
+	CC_TRY(collide_enqueue(c, sc, gx, gy, gz, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids, s,
+	                       true));
+	CC_TRY(read_stats(c, s));
+	return collide_finish(c, sc, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids, n_pairs, n_contacts,
+	                      s);
 }
 
 }  // namespace
@@ -669,6 +715,19 @@ void cc_ctx_destroy(cc_ctx *c) {
 		if (b->p) cudaFree(b->p);
 	if (c->gexec) cudaGraphExecDestroy(c->gexec);
 	if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+	for (auto &h : c->hs) {
+		Buf *hb[] = {&h.T, &h.A, &h.B, &h.C, &h.R, &h.ID, &h.pos, &h.rot, &h.act, &h.aabb, &h.pairs, &h.norm, &h.pa,
+		             &h.pb, &h.depth, &h.bids};
+		for (Buf *b : hb)
+			if (b->p) cudaFree(b->p);
+		if (h.in_done) cudaEventDestroy(h.in_done);
+		if (h.done) cudaEventDestroy(h.done);
+		if (h.h_stats) cudaFreeHost(h.h_stats);
+	}
+	for (cudaStream_t t : {c->hs_copy, c->hs_comp, c->hs_out})
+		if (t) cudaStreamDestroy(t);
+	if (c->hs_user) cudaEventDestroy(c->hs_user);
+	if (c->hs_back) cudaEventDestroy(c->hs_back);
 	if (c->h_stats) cudaFreeHost(c->h_stats);
 	if (c->h_word) cudaFreeHost(c->h_word);
 	for (int i = 0; i < 2 * kMaxMarks; i++)
@@ -1176,6 +1235,186 @@ cc_status cc_collide(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz, floa
 	CC_CUDA(c, cudaSetDevice(c->device));
 	return collide_dev(c, *sc, gx, gy, gz, envelope, res->aabb, res->pairs, res->pairs_cap, res->norm, res->cpta,
 	                   res->cptb, res->depth, res->bids, &res->n_pairs, &res->n_contacts, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+namespace {
+// Turns stage profiling off for the scope of a call.
+struct NoProfile {
+	cc_ctx *c;
+	bool was;
+	explicit NoProfile(cc_ctx *c_) : c(c_), was(c_->prof) { c->prof = false; }
+	~NoProfile() { c->prof = was; }
+};
+
+// Copies a finished step's outputs (P pairs, nc contacts) from its slot to the
+// caller's host buffers and waits for them.
+cc_status host_copy_out(cc_ctx *c, cc_ctx::HostSlot &h, cc_result *res, uint64_t P, uint64_t nc, cudaStream_t s) {
+	StageMark m(c, ST_COPY_OUT, s);
+	const uint64_t n = h.dev.n;
+	if (res->aabb) CC_CUDA(c, cudaMemcpyAsync(res->aabb, h.aabb.p, 24 * n, cudaMemcpyDeviceToHost, s));
+	if (res->pairs && P) CC_CUDA(c, cudaMemcpyAsync(res->pairs, h.pairs.p, 8 * P, cudaMemcpyDeviceToHost, s));
+	if (nc) {
+		if (res->norm) CC_CUDA(c, cudaMemcpyAsync(res->norm, h.norm.p, 12 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->cpta) CC_CUDA(c, cudaMemcpyAsync(res->cpta, h.pa.p, 12 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->cptb) CC_CUDA(c, cudaMemcpyAsync(res->cptb, h.pb.p, 12 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->depth) CC_CUDA(c, cudaMemcpyAsync(res->depth, h.depth.p, 4 * nc, cudaMemcpyDeviceToHost, s));
+		if (res->bids) CC_CUDA(c, cudaMemcpyAsync(res->bids, h.bids.p, 8 * nc, cudaMemcpyDeviceToHost, s));
+	}
+	CC_CUDA(c, cudaStreamSynchronize(s));
+	return CC_OK;
+}
+
+// Sizes one slot for a scene of n shapes / nb bodies and cap pairs and points
+// its device view at it.
+cc_status host_slot_prepare(cc_ctx *c, cc_ctx::HostSlot &h, uint64_t n, uint64_t nb, uint64_t cap) {
+	const uint64_t k = std::max<uint64_t>(cap, 1);
+	CC_TRY(ensure(c, h.T, 4 * n));
+	CC_TRY(ensure(c, h.A, 12 * n));
+	CC_TRY(ensure(c, h.B, 12 * n));
+	CC_TRY(ensure(c, h.C, 12 * n));
+	CC_TRY(ensure(c, h.R, 16 * n));
+	CC_TRY(ensure(c, h.ID, 4 * n));
+	CC_TRY(ensure(c, h.pos, 12 * nb));
+	CC_TRY(ensure(c, h.rot, 16 * nb));
+	CC_TRY(ensure(c, h.act, nb));
+	CC_TRY(ensure(c, h.aabb, 24 * n));
+	CC_TRY(ensure(c, h.pairs, 8 * k));
+	CC_TRY(ensure(c, h.norm, 12 * k));
+	CC_TRY(ensure(c, h.pa, 12 * k));
+	CC_TRY(ensure(c, h.pb, 12 * k));
+	CC_TRY(ensure(c, h.depth, 4 * k));
+	CC_TRY(ensure(c, h.bids, 8 * k));
+	h.dev = cc_scene{n, ptr<int32_t>(h.T), ptr<float>(h.A), ptr<float>(h.B), ptr<float>(h.C), ptr<float>(h.R),
+	                 ptr<uint32_t>(h.ID), nb, ptr<float>(h.pos), ptr<float>(h.rot), ptr<uint8_t>(h.act)};
+	return CC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+cc_status cc_collide_host_submit(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz, float envelope,
+                                 cc_result *res, void *stream) {
+	if (!c || !sc || !res) return CC_ERR_INVALID_ARGUMENT;
+	NoProfile np_(c);  // stage events would span three streams: not recorded here
+	c->launches = 0;
+	if (c->hs_inflight == 2)
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "two steps in flight: call cc_collide_host_wait first");
+	CC_TRY(check_grid(c, gx, gy, gz));
+	CC_TRY(check_scene(c, sc->n, sc->T, sc->A, sc->B, sc->C, sc->R, sc->ID, sc->nb, sc->body_pos, sc->body_rot));
+	if (sc->n && !sc->active) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null active array");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	if (!c->hs_copy) {
+		CC_CUDA(c, cudaStreamCreateWithFlags(&c->hs_copy, cudaStreamNonBlocking));
+		CC_CUDA(c, cudaStreamCreateWithFlags(&c->hs_comp, cudaStreamNonBlocking));
+		CC_CUDA(c, cudaStreamCreateWithFlags(&c->hs_out, cudaStreamNonBlocking));
+		CC_CUDA(c, cudaEventCreateWithFlags(&c->hs_user, cudaEventDisableTiming));
+		CC_CUDA(c, cudaEventCreateWithFlags(&c->hs_back, cudaEventDisableTiming));
+		for (auto &h : c->hs) {
+			CC_CUDA(c, cudaEventCreateWithFlags(&h.in_done, cudaEventDisableTiming));
+			CC_CUDA(c, cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming));
+			CC_CUDA(c, cudaMallocHost(&h.h_stats, sizeof(DevStats)));
+		}
+	}
+	cc_ctx::HostSlot &h = c->hs[c->hs_next];
+	const uint64_t n = sc->n, nb = sc->nb, cap = res->pairs_cap;
+	// growing a buffer frees the old one: never while another step may use it
+	if (c->hs_inflight) {
+		c->dry_run = true;
+		c->would_grow = false;
+		const cc_status d1 = host_slot_prepare(c, h, n, nb, cap);
+		const cc_status d2 = n ? prepare(c, n, cap) : CC_OK;
+		c->dry_run = false;
+		if (d1 != CC_OK || d2 != CC_OK || c->would_grow) CC_CUDA(c, cudaStreamSynchronize(c->hs_comp));
+	}
+	CC_TRY(host_slot_prepare(c, h, n, nb, cap));
+	if (n) CC_TRY(prepare(c, n, cap));
+	// after the caller's prior work on `stream`
+	CC_CUDA(c, cudaEventRecord(c->hs_user, (cudaStream_t)stream));
+	CC_CUDA(c, cudaStreamWaitEvent(c->hs_copy, c->hs_user, 0));
+	{
+		StageMark m(c, ST_COPY_IN, c->hs_copy);
+		cudaStream_t t = c->hs_copy;
+		CC_CUDA(c, cudaMemcpyAsync(h.T.p, sc->T, 4 * n, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.A.p, sc->A, 12 * n, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.B.p, sc->B, 12 * n, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.C.p, sc->C, 12 * n, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.R.p, sc->R, 16 * n, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.ID.p, sc->ID, 4 * n, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.pos.p, sc->body_pos, 12 * nb, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.rot.p, sc->body_rot, 16 * nb, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaMemcpyAsync(h.act.p, sc->active, nb, cudaMemcpyHostToDevice, t));
+		if (res->aabb) CC_CUDA(c, cudaMemcpyAsync(h.aabb.p, res->aabb, 24 * n, cudaMemcpyHostToDevice, t));
+		CC_CUDA(c, cudaEventRecord(h.in_done, t));
+	}
+	CC_CUDA(c, cudaStreamWaitEvent(c->hs_comp, h.in_done, 0));
+	if (n) {
+		CC_TRY(collide_enqueue(c, h.dev, gx, gy, gz, envelope, ptr<float>(h.aabb), ptr<int64_t>(h.pairs), cap,
+		                       ptr<float>(h.norm), ptr<float>(h.pa), ptr<float>(h.pb), ptr<float>(h.depth),
+		                       ptr<int32_t>(h.bids), c->hs_comp, false));
+		CC_CUDA(c, cudaMemcpyAsync(h.h_stats, c->stats.p, sizeof(DevStats), cudaMemcpyDeviceToHost, c->hs_comp));
+		const BpBuffers b = bp_buffers(c);
+		h.entry_cap = b.entry_cap;
+		h.pair_cap = b.pair_cap;
+	} else {
+		memset(h.h_stats, 0, sizeof(DevStats));
+	}
+	CC_CUDA(c, cudaEventRecord(h.done, c->hs_comp));
+	h.res = res;
+	h.grid[0] = gx;
+	h.grid[1] = gy;
+	h.grid[2] = gz;
+	h.env = envelope;
+	h.cap = cap;
+	c->hs_next ^= 1;
+	c->hs_inflight++;
+	return CC_OK;
+}
+
+cc_status cc_collide_host_wait(cc_ctx *c, cc_result *res, void *stream) {
+	if (!c || !res) return CC_ERR_INVALID_ARGUMENT;
+	NoProfile np_(c);
+	if (c->hs_inflight == 0) return set_err(c, CC_ERR_NO_RESULT, "no step in flight");
+	cc_ctx::HostSlot &h = c->hs[c->hs_oldest];
+	c->hs_oldest ^= 1;
+	c->hs_inflight--;
+	if (res != h.res) return set_err(c, CC_ERR_INVALID_ARGUMENT, "wait with a different result than the oldest submit");
+	CC_CUDA(c, cudaSetDevice(c->device));
+	CC_CUDA(c, cudaEventSynchronize(h.done));
+	res->n_pairs = res->n_contacts = 0;
+	if (h.dev.n == 0) return CC_OK;
+	const DevStats &st = *h.h_stats;
+	const bool fast = st.err == 0 && st.entries <= h.entry_cap && st.pairs <= h.pair_cap && st.pairs <= h.cap &&
+	                  st.np_n == st.pairs;
+	uint64_t P = st.pairs, nc = st.contacts;
+	if (fast) {
+		memcpy(c->h_stats, h.h_stats, sizeof(DevStats));
+		remember(c);
+	} else {
+		// rare: an error, a scratch overflow or a full output. Let the steps in
+		// flight finish, then run this one again on the blocking path, which
+		// regrows scratch, reports the error or retains the result.
+		CC_CUDA(c, cudaStreamSynchronize(c->hs_comp));
+		// the first run shifted the boxes in place; GenerateAABB keeps the
+		// caller's boxes of RECT/TRIANGLEMESH shapes, so start from them again
+		if (res->aabb)
+			CC_CUDA(c, cudaMemcpy(h.aabb.p, res->aabb, 24 * h.dev.n, cudaMemcpyHostToDevice));
+		const cc_status r = collide_dev(c, h.dev, h.grid[0], h.grid[1], h.grid[2], h.env, ptr<float>(h.aabb),
+		                                ptr<int64_t>(h.pairs), h.cap, ptr<float>(h.norm), ptr<float>(h.pa),
+		                                ptr<float>(h.pb), ptr<float>(h.depth), ptr<int32_t>(h.bids), &P, &nc,
+		                                c->hs_comp);
+		res->n_pairs = P;
+		res->n_contacts = nc;
+		if (r != CC_OK) return r;
+	}
+	res->n_pairs = P;
+	res->n_contacts = nc;
+	CC_TRY(host_copy_out(c, h, res, P, nc, c->hs_out));
+	// the caller's stream sees the step as done
+	CC_CUDA(c, cudaEventRecord(c->hs_back, c->hs_out));
+	CC_CUDA(c, cudaStreamWaitEvent((cudaStream_t)stream, c->hs_back, 0));
+	return CC_OK;
 }
 
 cc_status cc_collide_host(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz, float envelope, cc_result *res,

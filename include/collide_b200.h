@@ -239,6 +239,22 @@ CC_API cc_status cc_perturb_bodies(cc_ctx *ctx, uint64_t nb, float *body_pos, fl
 CC_API cc_status cc_collide_host(cc_ctx *ctx, const cc_scene *scene, int gx, int gy, int gz, float envelope,
                           cc_result *res, void *stream);
 
+/* Pipelined form of cc_collide_host for a stream of time steps: submit
+ * enqueues one step (copies in on one stream, the pipeline on another, the
+ * small counter read-back) and returns at once, so the copy of step k+1 runs
+ * while step k computes; wait finishes the OLDEST submitted step: waits for
+ * it, copies its pairs and contacts into `res` (the same cc_result that was
+ * submitted) and sets res->n_pairs / n_contacts. At most two steps are in
+ * flight per context; host buffers must stay untouched until their wait.
+ * Work is ordered after the caller's `stream` at submit, and `stream` waits
+ * for the step's copies at wait. A step that needs more scratch or more
+ * output than the submit provided is redone on the blocking path inside
+ * wait, with cc_collide_host's results and status. Stage profiling is not
+ * recorded for these calls. No reference counterpart. */
+CC_API cc_status cc_collide_host_submit(cc_ctx *ctx, const cc_scene *scene, int gx, int gy, int gz, float envelope,
+                                        cc_result *res, void *stream);
+CC_API cc_status cc_collide_host_wait(cc_ctx *ctx, cc_result *res, void *stream);
+
 /* Number of kernels the last call on this context launched. */
 CC_API uint64_t cc_last_launch_count(const cc_ctx *ctx);
 
