@@ -220,8 +220,9 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 	if (over) atomicOr(err, (uint32_t)kErrCapacity);
 }
 
-// One lane per entry; each lane tests its entry against the later entries of
-// the same cell. A warp's 32 entries and the kWin - 32 that follow them are
+// Each entry is tested against the later entries of its cell; a warp takes
+// 32 entries and deals their tests out evenly over its lanes (so a warp's
+// rounds follow the SUM of its entries' partner counts, not 32 x the largest). A warp's 32 entries and the kWin - 32 that follow them are
 // staged in shared memory with coalesced 16-byte loads (cells hold a handful
 // of entries, so the inner loop almost never leaves the window); loops are
 // warp-uniform so the emission can be warp-aggregated: found pairs collect in
@@ -252,6 +253,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 	__shared__ Plan sp;
 	__shared__ float4 win_all[kNT / 32][2 * kWin];
 	__shared__ unsigned long long out_all[kNT / 32][kOutBuf];
+	__shared__ uint32_t owned_s[kNT];  // pairs owned by each lane's entry in the current window
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
@@ -286,42 +288,75 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 			const uint64_t end = min((uint64_t)cell_start[c + 1], entry_cap);
 			my_n = (int)(end > e + 1 ? end - e - 1 : 0);
 		}
-		const float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
-		const float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
-		const int d0 = pl.dim[0], d1 = pl.dim[1], d2 = pl.dim[2];
+		float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
+		float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
+		int d0 = pl.dim[0], d1 = pl.dim[1], d2 = pl.dim[2];
 		// home-cell test: the pair belongs to this cell iff, on every axis, one
 		// of the two min corners lies in this cell's slab
-		const bool ax = valid && cell_of(alo.x, lo0, iv0, d0) == cx;
-		const bool ay = valid && cell_of(alo.y, lo1, iv1, d1) == cy;
-		const bool az = valid && cell_of(alo.z, lo2, iv2, d2) == cz;
-		const int iters = __reduce_max_sync(0xffffffffu, my_n);
-		uint32_t owned = 0;
-		for (int t = 0; t < iters; t++) {
+		const uint32_t amask = (valid && cell_of(alo.x, lo0, iv0, d0) == cx ? 1u : 0u) |
+		                       (valid && cell_of(alo.y, lo1, iv1, d1) == cy ? 2u : 0u) |
+		                       (valid && cell_of(alo.z, lo2, iv2, d2) == cz ? 4u : 0u);
+		// the warp's sum(my_n) tests, dealt out 32 per round: test k belongs to
+		// the lane a with pre[a] <= k < pre[a] + my_n[a] (pre: exclusive scan)
+		int pre = my_n;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const int v = __shfl_up_sync(0xffffffffu, pre, o);
+			if ((int)lane >= o) pre += v;
+		}
+		const int total = __shfl_sync(0xffffffffu, pre, 31);
+		pre -= my_n;
+		owned_s[threadIdx.x] = 0;
+		__syncwarp();
+		for (int k0 = 0; k0 < total; k0 += 32) {
+			const int k = k0 + (int)lane;
+			int a = 0;
+#pragma unroll
+			for (int step = 16; step > 0; step >>= 1) {
+				const int v = __shfl_sync(0xffffffffu, pre, a + step);
+				if (v <= k) a += step;
+			}
+			const int t = k - __shfl_sync(0xffffffffu, pre, a);
+			const uint32_t am = __shfl_sync(0xffffffffu, amask, a);
+			if constexpr (kBatch) {  // entries of one warp may come from different scenes
+				lo0 = __shfl_sync(0xffffffffu, pl.lo[0], a);
+				lo1 = __shfl_sync(0xffffffffu, pl.lo[1], a);
+				lo2 = __shfl_sync(0xffffffffu, pl.lo[2], a);
+				iv0 = __shfl_sync(0xffffffffu, pl.inv[0], a);
+				iv1 = __shfl_sync(0xffffffffu, pl.inv[1], a);
+				iv2 = __shfl_sync(0xffffffffu, pl.inv[2], a);
+				d0 = __shfl_sync(0xffffffffu, pl.dim[0], a);
+				d1 = __shfl_sync(0xffffffffu, pl.dim[1], a);
+				d2 = __shfl_sync(0xffffffffu, pl.dim[2], a);
+			}
 			bool emit = false;
 			unsigned long long key = 0;
 			uint32_t other_owner = 0xffffffffu;
-			if (t < my_n) {
-				const uint32_t loc = lane + 1 + t;  // position of the partner in the window
+			if (k < total) {
+				const float4 plo = win[2 * a], phi = win[2 * a + 1];
+				const uint32_t pc = __float_as_uint(phi.w);
+				const int px = pc & 1023, py = (pc >> 10) & 1023, pz = (pc >> 20) & 1023;
+				const uint32_t loc = (uint32_t)a + 1 + (uint32_t)t;  // partner's position in the window
 				float4 blo, bhi;
 				if (loc < nwin) {
 					blo = win[2 * loc];
 					bhi = win[2 * loc + 1];
 				} else {
-					const uint64_t q = e + 1 + t;
+					const uint64_t q = base + loc;
 					blo = entries[2 * q];
 					bhi = entries[2 * q + 1];
 				}
-				if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
-				    blo.z <= ahi.z) {
-					const bool hx = ax || cell_of(blo.x, lo0, iv0, d0) == cx;
-					const bool hy = ay || cell_of(blo.y, lo1, iv1, d1) == cy;
-					const bool hz = az || cell_of(blo.z, lo2, iv2, d2) == cz;
+				if (plo.x <= bhi.x && blo.x <= phi.x && plo.y <= bhi.y && blo.y <= phi.y && plo.z <= bhi.z &&
+				    blo.z <= phi.z) {
+					const bool hx = (am & 1u) || cell_of(blo.x, lo0, iv0, d0) == px;
+					const bool hy = (am & 2u) || cell_of(blo.y, lo1, iv1, d1) == py;
+					const bool hz = (am & 4u) || cell_of(blo.z, lo2, iv2, d2) == pz;
 					if (hx && hy && hz) {
-						const uint32_t idb = __float_as_uint(blo.w);
-						const uint32_t lo = min(ida, idb), hi = max(ida, idb);
+						const uint32_t ia = __float_as_uint(plo.w), idb = __float_as_uint(blo.w);
+						const uint32_t lo = min(ia, idb), hi = max(ia, idb);
 						key = ((unsigned long long)lo << 32) | hi;
 						emit = true;
-						if (lo == ida) owned++;
+						if (lo == ia) atomicAdd(&owned_s[(threadIdx.x & ~31u) + a], 1u);
 						else other_owner = lo;
 					}
 				}
@@ -341,6 +376,8 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 				__syncwarp();
 			}
 		}
+		__syncwarp();
+		const uint32_t owned = owned_s[threadIdx.x];
 		if (owned) atomicAdd(&owner_count[ida], owned);
 	}
 	if (ocnt) flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);

@@ -405,7 +405,7 @@ void enqueue_np(cc_ctx *c, const NpArgs &a, uint64_t P_cap, const unsigned long 
 	{
 		StageMark m(c, ST_NP_COMPACT, s);
 		launch_np_compact(P_cap, P_dev, sc, reinterpret_cast<long long *>(a.pairs), a.norm, a.cpta, a.cptb, a.depth,
-		                  a.bids, &ptr<DevStats>(c->stats)->contacts, s);
+		                  a.bids, &ptr<DevStats>(c->stats)->contacts, P_dev ? hint_P(c) : P_cap, s);
 	}
 	c->launches += 5;
 }

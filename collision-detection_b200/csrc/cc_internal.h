@@ -236,6 +236,6 @@ void launch_mpr_exact(unsigned grid, uint64_t P_cap, const unsigned long long *P
                       const long long *pairs, const NpScratch &sc, cudaStream_t s);
 void launch_np_compact(uint64_t P_cap, const unsigned long long *P_dev, const NpScratch &sc, long long *pairs,
                        float *norm, float *cpta, float *cptb, float *depth, int32_t *bids,
-                       unsigned long long *contacts_out, cudaStream_t s);
+                       unsigned long long *contacts_out, uint64_t P_hint, cudaStream_t s);
 
 }  // namespace cc

@@ -171,7 +171,9 @@ void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, con
                 const NpScratch &sc, int precision, uint64_t P_hint, cudaStream_t s) {
 	if (!P_cap) return;
 	{  // group the pairs by shape-type combination; the last word is the work queue
-		const unsigned g = (unsigned)std::min<uint64_t>((P_cap + 255) / 256, (uint64_t)kNumSMs * 4);
+		// blocks for the expected pair count (the loops stride over the device count)
+		const uint64_t Pe = std::min<uint64_t>(P_hint ? P_hint : P_cap, P_cap);
+		const unsigned g = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((Pe + 255) / 256, (uint64_t)kNumSMs * 4));
 		if (!sc.pre_zeroed) cudaMemsetAsync(sc.classes, 0, (2 * kNpClasses + 1) * sizeof(uint32_t), s);
 		k_np_class_count<<<g, 256, 0, s>>>(P_cap, P_dev, n, T, pairs, sc.classes);
 		k_np_class_scatter<<<g, 256, 0, s>>>(P_cap, P_dev, n, T, pairs, sc.classes, sc.order);
@@ -194,11 +196,12 @@ void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, con
 
 void launch_np_compact(uint64_t P_cap, const unsigned long long *P_dev, const NpScratch &sc, long long *pairs,
                        float *norm, float *cpta, float *cptb, float *depth, int32_t *bids,
-                       unsigned long long *contacts_out, cudaStream_t s) {
+                       unsigned long long *contacts_out, uint64_t P_hint, cudaStream_t s) {
 	launch_scan_u32_to_u64(sc.flag, P_cap, sc.pos, sc.status, sc.ticket, sc.err, s, P_dev, contacts_out,
 	                       sc.pre_zeroed);
 	if (!P_cap) return;
-	const unsigned grid = (unsigned)std::min<uint64_t>((P_cap + 255) / 256, (uint64_t)kNumSMs * 16);
+	const uint64_t Pe = std::min<uint64_t>(P_hint ? P_hint : P_cap, P_cap);
+	const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((Pe + 255) / 256, (uint64_t)kNumSMs * 16));
 	k_np_compact<<<grid, 256, 0, s>>>(P_cap, P_dev, sc, pairs, norm, cpta, cptb, depth, bids);
 }
 
