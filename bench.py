@@ -427,6 +427,12 @@ def run_ours(args):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    # the bucket sort runs as three tiers (thread, warp, block): one stage here
+    stage = dict(stage)
+    for tier in ("segsort_mid", "segsort_big"):
+        if tier in stage and "segsort" in stage:
+            stage["segsort"] = (stage["segsort"][0] + stage[tier][0], stage["segsort"][1])
+            del stage[tier]
     kern = {k: v for k, v in stage.items() if k in STAGE_BYTES}
     dom = max(kern, key=lambda k: kern[k][0])
     dom_ms = kern[dom][0] / kern[dom][1]

@@ -413,32 +413,46 @@ constexpr int kBigSeg = 16384;
 __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long long *__restrict__ owner_off,
                                                   unsigned long long *__restrict__ out, uint32_t *big_list,
                                                   uint64_t big_cap, DevStats *stats) {
+	if (stats->np_n != stats->pairs) return;  // the pairs were not emitted (uniform over the grid)
 	const uint64_t a = (uint64_t)blockIdx.x * kNT + threadIdx.x;
-	if (a >= n || stats->np_n != stats->pairs) return;  // the pairs were not emitted
-	const uint64_t beg = owner_off[a], end = owner_off[a + 1];
-	const uint64_t len = end - beg;
-	if (len <= 1) return;
-	if (len <= kSmallSeg) {  // insertion sort in place
-		for (uint64_t i = beg + 1; i < end; i++) {
-			const unsigned long long k = out[i];
-			uint64_t j = i;
-			while (j > beg && out[j - 1] > k) {
-				out[j] = out[j - 1];
-				j--;
+	uint64_t len = 0;
+	if (a < n) {
+		const uint64_t beg = owner_off[a], end = owner_off[a + 1];
+		len = end - beg;
+		if (len > 1 && len <= kSmallSeg) {  // insertion sort in place
+			for (uint64_t i = beg + 1; i < end; i++) {
+				const unsigned long long k = out[i];
+				uint64_t j = i;
+				while (j > beg && out[j - 1] > k) {
+					out[j] = out[j - 1];
+					j--;
+				}
+				out[j] = k;
 			}
-			out[j] = k;
 		}
-		return;
 	}
-	atomicMax(&stats->max_segment, (unsigned long long)len);
-	if (len > kBigSeg) {
-		atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
-		return;
+	const bool longer = len > kSmallSeg;
+	const uint32_t wmax = __reduce_max_sync(0xffffffffu, longer ? (uint32_t)min(len, (uint64_t)0xffffffffu) : 0u);
+	if ((threadIdx.x & 31) == 0 && wmax) atomicMax(&stats->max_segment, (unsigned long long)wmax);
+	if (len > kBigSeg) atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
+	// list the longer buckets, one counter atomic per warp and tier
+	const bool mid = longer && len <= kMidSeg, big = len > kMidSeg && len <= kBigSeg;
+	const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+#pragma unroll
+	for (int tier = 0; tier < 2; tier++) {
+		const bool want = tier == 0 ? mid : big;
+		const uint32_t m = __ballot_sync(0xffffffffu, want);
+		if (!m) continue;
+		unsigned long long base = 0;
+		if (lane == (uint32_t)(__ffs(m) - 1)) base = atomicAdd(tier == 0 ? &stats->big_segments : &stats->seg_big,
+		                                                       (unsigned long long)__popc(m));
+		base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+		if (want) {
+			const unsigned long long slot = base + __popc(m & lt);
+			if (slot < big_cap) big_list[tier == 0 ? slot : big_cap - 1 - slot] = (uint32_t)a;
+			else atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
+		}
 	}
-	const bool mid = len <= kMidSeg;
-	const unsigned long long slot = atomicAdd(mid ? &stats->big_segments : &stats->seg_big, 1ull);
-	if (slot < big_cap) big_list[mid ? slot : big_cap - 1 - slot] = (uint32_t)a;
-	else atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
 }
 
 // In-place bitonic sort of m (a power of two) 32-bit keys in shared memory by
@@ -669,14 +683,18 @@ void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cud
 	k_segsort<<<blocks_for(n), kNT, 0, s>>>(n, b.owner_off, out, b.big_list, b.big_cap, b.stats);
 }
 
+void launch_segsort_mid(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
+	k_segsort_mid<<<kNumSMs * 6, kMidNT, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
+}
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
 	static const bool attr = [] {
 		return cudaFuncSetAttribute(k_segsort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		                            kBigSeg * (int)sizeof(uint32_t)) == cudaSuccess;
 	}();
 	(void)attr;
-	k_segsort_mid<<<kNumSMs * 6, kMidNT, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
-	k_segsort_big<<<kNumSMs, 512, kBigSeg * sizeof(uint32_t), s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
+	// 64 KB of shared memory a block: three blocks fit on an SM
+	k_segsort_big<<<kNumSMs * 3, 512, kBigSeg * sizeof(uint32_t), s>>>(b.stats, b.big_cap, b.big_list, b.owner_off,
+	                                                                   out);
 }
 
 void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s) {

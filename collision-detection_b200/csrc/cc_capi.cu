@@ -27,11 +27,11 @@ struct Buf {
 // Kernel stages timed by the optional profiler.
 enum Stage : int {
 	ST_AABB, ST_BOUNDS, ST_COUNT, ST_SCAN_CELLS, ST_SCATTER, ST_PAIR_TEST, ST_SCAN_OWNER, ST_OWNER_SCATTER,
-	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_COUNT_
+	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_SEGSORT_MID, ST_SEGSORT_BIG, ST_COUNT_
 };
 const char *kStageNames[ST_COUNT_] = {"aabb", "bounds", "count", "scan_cells", "scatter", "pair_test",
                                       "scan_owner", "owner_scatter", "segsort", "mpr", "np_compact", "bins",
-                                      "copy_in", "copy_out"};
+                                      "copy_in", "copy_out", "segsort_mid", "segsort_big"};
 constexpr int kMaxMarks = 64;
 
 }  // namespace
@@ -387,7 +387,14 @@ void enqueue_emit(cc_ctx *c, uint64_t n, unsigned long long *out, uint64_t out_c
 	{
 		StageMark m(c, ST_SEGSORT, s);
 		launch_segsort(n, out, b, s);
-		launch_segsort_big(out, b, s);  // the warp and block tiers
+	}
+	{
+		StageMark m(c, ST_SEGSORT_MID, s);
+		launch_segsort_mid(out, b, s);
+	}
+	{
+		StageMark m(c, ST_SEGSORT_BIG, s);
+		launch_segsort_big(out, b, s);
 	}
 	c->launches += 4;
 }

@@ -144,6 +144,7 @@ void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
 // stats->np_n = P.
 void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+void launch_segsort_mid(unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 
 // ------------------------------------------------------------------ batches

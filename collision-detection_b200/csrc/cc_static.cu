@@ -183,6 +183,7 @@ extern "C" cc_status cc_broadphase_noalloc(uint64_t n, float *aabb, int gx, int 
 	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
 	launch_owner_scatter(pairs_cap, out, b, s);
 	launch_segsort(n, out, b, s);
+	launch_segsort_mid(out, b, s);
 	launch_segsort_big(out, b, s);
 	NA_CUDA(cudaGetLastError());
 	if ((st = read_stats(b.stats, s)) != CC_OK) return st;
