@@ -249,7 +249,9 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
                                                     const float4 *__restrict__ entries,
                                                     uint64_t entry_cap, uint32_t *__restrict__ owner_count,
                                                     unsigned long long *__restrict__ pairs, uint64_t pair_cap,
-                                                    unsigned long long *pair_counter, SceneMap sm) {
+                                                    unsigned long long *pair_counter, SceneMap sm, uint2 *dense,
+                                                    uint64_t dense_cap, unsigned long long *dense_count,
+                                                    uint32_t *err) {
 	__shared__ Plan sp;
 	__shared__ float4 win_all[kNT / 32][2 * kWin];
 	__shared__ unsigned long long out_all[kNT / 32][kOutBuf];
@@ -285,8 +287,19 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 			const uint32_t pc = __float_as_uint(ahi.w);
 			cx = pc & 1023; cy = (pc >> 10) & 1023; cz = (pc >> 20) & 1023;
 			const uint32_t c = cell_index(pl, cbase, cx, cy, cz);
+			const uint64_t beg = cell_start[c];
 			const uint64_t end = min((uint64_t)cell_start[c + 1], entry_cap);
 			my_n = (int)(end > e + 1 ? end - e - 1 : 0);
+			if (dense && end - beg > kDenseCell) {  // left to k_pair_test_dense
+				my_n = 0;
+				if (e == beg) {
+					const uint32_t chunks = (uint32_t)((end - beg + kNT - 1) / kNT);
+					const unsigned long long at = atomicAdd(dense_count, (unsigned long long)chunks);
+					for (uint32_t q = 0; q < chunks; q++)
+						if (at + q < dense_cap) dense[at + q] = make_uint2(c, q * kNT);
+						else atomicOr(err, (uint32_t)kErrCapacity);
+				}
+			}
 		}
 		float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
 		float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
@@ -383,6 +396,107 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 	if (ocnt) flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);
 }
 
+// Dense cells: one block per (cell, chunk of 256 rows). Thread t takes row
+// i = r0 + t and tests it against every later entry j > i of the cell, the
+// columns staged 256 at a time in shared memory and read by all lanes at once
+// (a broadcast), so one warp instruction carries 32 tests. Pairs owned by the
+// row (smaller index) are counted in a register, pairs owned by the column in
+// a shared counter per column; both reach owner_count once per tile.
+constexpr int kDenseOut = 512;
+template <bool kBatch>
+__global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, const uint32_t *__restrict__ cell_start,
+                                                          const float4 *__restrict__ entries, uint64_t entry_cap,
+                                                          uint32_t *__restrict__ owner_count,
+                                                          unsigned long long *__restrict__ pairs, uint64_t pair_cap,
+                                                          unsigned long long *pair_counter, SceneMap sm,
+                                                          const uint2 *__restrict__ dense, uint64_t dense_cap) {
+	__shared__ Plan sp;
+	__shared__ float4 tlo[kNT], thi[kNT];
+	__shared__ uint32_t colown[kNT];
+	__shared__ unsigned long long out_all[kNT / 32][kDenseOut];
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
+	__syncthreads();
+	if (!kBatch && !sp.valid) return;
+	const uint64_t items = min((uint64_t)stats->dense_items, dense_cap);
+	unsigned long long *obuf = out_all[threadIdx.x >> 5];
+	uint32_t ocnt = 0;
+	const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+	for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+		const uint2 w = dense[it];
+		const uint64_t s0 = cell_start[w.x];
+		const uint64_t s1 = min((uint64_t)cell_start[w.x + 1], entry_cap);
+		const uint32_t k = (uint32_t)(s1 - s0), r0 = w.y;
+		const uint32_t i = r0 + threadIdx.x;
+		const bool row = i < k;
+		float4 alo = make_float4(0.f, 0.f, 0.f, 0.f), ahi = alo;
+		if (row) {
+			alo = entries[2 * (s0 + i)];
+			ahi = entries[2 * (s0 + i) + 1];
+		}
+		const uint32_t ida = __float_as_uint(alo.w);
+		const uint32_t pc = __float_as_uint(ahi.w);
+		const int cx = pc & 1023, cy = (pc >> 10) & 1023, cz = (pc >> 20) & 1023;
+		uint32_t cb;
+		const Plan &pl = plan_of<kBatch>(sp, sm, row ? ida : __float_as_uint(entries[2 * s0].w), cb);
+		const float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
+		const float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
+		const int d0 = pl.dim[0], d1 = pl.dim[1], d2 = pl.dim[2];
+		const bool ax = row && cell_of(alo.x, lo0, iv0, d0) == cx;
+		const bool ay = row && cell_of(alo.y, lo1, iv1, d1) == cy;
+		const bool az = row && cell_of(alo.z, lo2, iv2, d2) == cz;
+		uint32_t owned = 0;
+		for (uint32_t c0 = r0; c0 < k; c0 += kNT) {
+			const uint32_t nt = min((uint32_t)kNT, k - c0);
+			__syncthreads();  // the previous tile is no longer read
+			if (threadIdx.x < nt) {
+				tlo[threadIdx.x] = entries[2 * (s0 + c0 + threadIdx.x)];
+				thi[threadIdx.x] = entries[2 * (s0 + c0 + threadIdx.x) + 1];
+			}
+			colown[threadIdx.x] = 0;
+			__syncthreads();
+			for (uint32_t jj = 0; jj < nt; jj++) {  // only j > i is tested
+				const uint32_t j = c0 + jj;
+				bool emit = false;
+				unsigned long long key = 0;
+				if (row && j > i) {
+					const float4 blo = tlo[jj], bhi = thi[jj];
+					if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
+					    blo.z <= ahi.z) {
+						const bool hx = ax || cell_of(blo.x, lo0, iv0, d0) == cx;
+						const bool hy = ay || cell_of(blo.y, lo1, iv1, d1) == cy;
+						const bool hz = az || cell_of(blo.z, lo2, iv2, d2) == cz;
+						if (hx && hy && hz) {
+							const uint32_t idb = __float_as_uint(blo.w);
+							const uint32_t lo = min(ida, idb), hi = max(ida, idb);
+							key = ((unsigned long long)lo << 32) | hi;
+							emit = true;
+							if (lo == ida) owned++;
+							else atomicAdd(&colown[jj], 1u);
+						}
+					}
+				}
+				const uint32_t bal = __ballot_sync(0xffffffffu, emit);
+				if (bal) {
+					const uint32_t nb = __popc(bal);
+					if (ocnt + nb > kDenseOut) {
+						flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);
+						ocnt = 0;
+					}
+					if (emit) obuf[ocnt + __popc(bal & lt)] = key;
+					ocnt += nb;
+					__syncwarp();
+				}
+			}
+			__syncthreads();  // column counts complete
+			if (threadIdx.x < nt && colown[threadIdx.x])
+				atomicAdd(&owner_count[__float_as_uint(tlo[threadIdx.x].w)], colown[threadIdx.x]);
+		}
+		if (owned) atomicAdd(&owner_count[ida], owned);
+	}
+	if (ocnt) flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);
+}
+
 // Bucket the unsorted pairs by owner (the smaller index). P comes from the
 // device; if it exceeds the scratch or the output nothing is written.
 __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t pair_cap, uint64_t out_cap,
@@ -394,11 +508,21 @@ __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t
 	const bool fits = P <= pair_cap && P <= out_cap;
 	if (blockIdx.x == 0 && threadIdx.x == 0) stats->np_n = fits ? P : 0ull;
 	if (!fits) return;
-	for (uint64_t t = (uint64_t)blockIdx.x * kNT + threadIdx.x; t < P; t += (uint64_t)gridDim.x * kNT) {
-		const unsigned long long key = tmp[t];
-		const uint32_t a = (uint32_t)(key >> 32);
-		const uint32_t k = atomicSub(&owner_count[a], 1u) - 1u;
-		out[owner_off[a] + k] = key;
+	// lanes of a warp whose pairs share an owner take their slots with one
+	// atomic (pair lists of dense cells arrive grouped by owner)
+	const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+	const uint64_t step = (uint64_t)gridDim.x * kNT;
+	for (uint64_t t0 = (uint64_t)blockIdx.x * kNT + (threadIdx.x & ~31u); t0 < P; t0 += step) {
+		const uint64_t t = t0 + lane;
+		const bool valid = t < P;
+		const unsigned long long key = valid ? tmp[t] : 0ull;
+		const uint32_t a = valid ? (uint32_t)(key >> 32) : 0xffffffffu;
+		const uint32_t peers = __match_any_sync(0xffffffffu, a);
+		const int leader = __ffs(peers) - 1;
+		uint32_t base = 0;
+		if (valid && (int)lane == leader) base = atomicSub(&owner_count[a], (uint32_t)__popc(peers));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if (valid) out[owner_off[a] + base - 1u - __popc(peers & lt)] = key;
 	}
 }
 
@@ -662,10 +786,27 @@ void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cud
 	unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(want, 1), (uint64_t)kNumSMs * 8);
 	if (b.sm.plans)
 		k_pair_test<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
-		                                       b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm);
+		                                       b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
+		                                       &b.stats->dense_items, &b.stats->err);
 	else
 		k_pair_test<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
-		                                        b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm);
+		                                        b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
+		                                        &b.stats->dense_items, &b.stats->err);
+	launch_pair_test_dense(b, s);
+}
+
+void launch_pair_test_dense(const BpBuffers &b, cudaStream_t s) {
+	if (!b.dense || !b.dense_cap) return;
+	// persistent blocks over the device-side item count (41 KB of shared memory each)
+	const unsigned grid = kNumSMs * 4;
+	if (b.sm.plans)
+		k_pair_test_dense<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+		                                             b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
+		                                             b.dense_cap);
+	else
+		k_pair_test_dense<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+		                                              b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
+		                                              b.dense_cap);
 }
 
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s) {

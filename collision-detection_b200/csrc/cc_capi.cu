@@ -42,7 +42,7 @@ struct cc_ctx {
 	GridParams gp{};
 	cudaError_t cuda_err = cudaSuccess;
 	// device scratch
-	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list;
+	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list, dense;
 	Buf ref_cnt, ref_off, ref_keys, ref_tmp, ref_flags, ref_runpos, rx_hist, rx_hoff;
 	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes;
 	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
@@ -251,6 +251,8 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.big_cap = c->big_list.bytes / sizeof(uint32_t);
 	b.pre_zeroed = c->pass_zeroed;
 	b.sm = c->sm;
+	b.dense = ptr<uint2>(c->dense);
+	b.dense_cap = c->dense.bytes / sizeof(uint2);
 	return b;
 }
 
@@ -300,6 +302,7 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 
 	CC_TRY(ensure_status(c));
 	CC_TRY(ensure(c, c->ticket, 64));
 	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * (n + 1024)));
+	CC_TRY(ensure(c, c->dense, sizeof(uint2) * (c->entries.bytes / (2 * sizeof(float4)) / kDenseCell + 1024)));
 	if (np_cap) CC_TRY(np_prepare(c, np_cap));
 	return CC_OK;
 }
@@ -427,6 +430,7 @@ cc_status reset_pass_counters(cc_ctx *c, uint64_t n, cudaStream_t s) {
 	CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 3 * sizeof(unsigned long long), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->np_n, 0, sizeof(unsigned long long), s));
+	CC_CUDA(c, cudaMemsetAsync(&d->dense_items, 0, sizeof(unsigned long long), s));
 	return CC_OK;
 }
 
@@ -441,7 +445,10 @@ cc_status settle(cc_ctx *c, uint64_t n, float *aabb, unsigned long long *out, ui
 		if (E <= b.entry_cap && P <= b.pair_cap) return CC_OK;
 		if (E >= 0xffffffffull)
 			return set_err(c, CC_ERR_CAPACITY, "search grid needs %llu entries (>= 2^32)", (unsigned long long)E);
-		if (E > b.entry_cap) CC_TRY(ensure(c, c->entries, 2 * sizeof(float4) * (E + E / 8)));
+		if (E > b.entry_cap) {
+			CC_TRY(ensure(c, c->entries, 2 * sizeof(float4) * (E + E / 8)));
+			CC_TRY(ensure(c, c->dense, sizeof(uint2) * ((E + E / 8) / kDenseCell + 1024)));
+		}
 		if (P > b.pair_cap) CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * (P + P / 8)));
 		CC_TRY(reset_pass_counters(c, n, s));
 		b = bp_buffers(c);
@@ -708,7 +715,8 @@ void cc_ctx_destroy(cc_ctx *c) {
 	if (!c) return;
 	cudaSetDevice(c->device);
 	Buf *bufs[] = {&c->stats,    &c->cell_count, &c->cell_start, &c->entries,  &c->owner_count, &c->owner_off,
-	               &c->pairs_tmp, &c->status,    &c->ticket,     &c->big_list, &c->ref_cnt,     &c->ref_off,
+	               &c->pairs_tmp, &c->status,    &c->ticket,     &c->big_list, &c->dense,       &c->ref_cnt,
+	               &c->ref_off,
 	               &c->ref_keys, &c->ref_tmp,    &c->ref_flags,  &c->ref_runpos, &c->rx_hist,   &c->rx_hoff,
 	               &c->np_norm,  &c->np_pa,      &c->np_pb,      &c->np_depth, &c->np_ids,      &c->np_pairs,
 	               &c->np_flag,  &c->np_pos,     &c->np_order, &c->np_classes, &c->in_T,       &c->in_A,     &c->in_B,        &c->in_C,

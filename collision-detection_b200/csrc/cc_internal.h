@@ -39,6 +39,7 @@ struct DevStats {
 	unsigned long long seg_big;       // owner buckets of 1025..16384 pairs (listed from the back)
 	unsigned long long cells;     // plan.G as a 64-bit scan count
 	unsigned long long np_n;      // pairs handed to the narrowphase (0 if an output was too small)
+	unsigned long long dense_items;  // (cell, row chunk) work items of the dense-cell pair test
 	uint32_t blocks_done;         // last-block detection of the bounds reduction
 	uint32_t pad_;
 	Plan plan;
@@ -128,6 +129,8 @@ struct BpBuffers {
 	uint32_t *ticket2 = nullptr;
 	bool pre_zeroed = false;      // status/ticket regions were zeroed by the pass's first kernel
 	SceneMap sm;                  // batch layout (empty: one scene)
+	uint2 *dense = nullptr;       // dense-cell work items (cell, first row)
+	uint64_t dense_cap = 0;
 };
 
 // Bounds pass over caller AABBs; its last block writes stats->plan.
@@ -139,6 +142,10 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
+// Cells holding more than kDenseCell entries are left out of the lane-per-entry
+// pair test and tested here instead, tile by tile (N-body style).
+constexpr uint32_t kDenseCell = 128;
+void launch_pair_test_dense(const BpBuffers &b, cudaStream_t s);
 // Device-driven emission: P is read from stats->pairs. If P exceeds the
 // scratch (pair_cap) or out_cap nothing is written and stats->np_n = 0, else
 // stats->np_n = P.

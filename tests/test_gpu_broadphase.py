@@ -134,6 +134,21 @@ def test_tuning_does_not_change_pairs(cb, target, ratio):
     assert np.array_equal(p, po), pair_set_diff(p, po)
 
 
+def test_dense_cells_match_oracle(cb):
+    # two tight clusters: cells of the search grid hold hundreds of entries, so
+    # their tests run in the tiled dense-cell kernel (the background in the
+    # lane-per-entry kernel); a coarse pinned grid makes nearly every cell dense
+    s = S.clustered_spheres(60_000, seed=2, clusters=2, sigma=0.01, background=0.05)
+    a = O.aabb(s)
+    _, po = O.broadphase(a, (64, 64, 64))
+    assert len(po) > 1_000_000
+    for dims in ((0, 0, 0), (20, 20, 20)):
+        ctx = cb.Context()
+        ctx.set_search_grid(dims)
+        _, p = gpu_broadphase(cb, a, (16, 16, 16), ctx)
+        assert np.array_equal(p, po), (dims, pair_set_diff(p, po))
+
+
 # ------------------------------------------------------------------ the reference's own tests
 @pytest.mark.parametrize("n", [1, 2, 10, 33, 100, 4097, 6000])
 def test_reference_test1_single_bin(cb, n):
