@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-scene batched measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
+    ap.add_argument("--no-clustered", action="store_true", help="skip the 16.7M clustered-sphere broadphase")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     return ap.parse_args()
 
@@ -112,6 +113,49 @@ def bench_batched(cb, ctx, dev, steps=10):
             "per_scene_launch": {"ms": tl, "value": N / (tl / 1000.0), "unit": "bodies/s",
                                  "how": "cc_collide once per scene, in order, outputs preallocated"},
             "speedup_vs_per_scene": tl / tb, "steps": steps}
+
+
+CLUSTER_WORKLOAD = ("clustered_spheres: 16,777,216 spheres, radii log-uniform [0.0005,0.005], 90% from 64 "
+                    "isotropic Gaussians (sigma 0.02, means U[0,1]^3), 10% U[0,1]^3; broadphase only")
+
+
+def bench_clustered(cb, dev, steps=3):
+    """The load-imbalanced broadphase: detectPossibleCollisions on 16.7M
+    clustered spheres (~3.9e9 pairs, a list the reference's uint32 counters
+    cannot hold)."""
+    import torch
+    from collide_b200 import scenes as S
+    sc = S.clustered_spheres(1 << 24, seed=0)
+    ds = cb.DeviceScene(sc, device=dev)
+    a0 = cb.AABBGenerator().GenerateAABB(*ds.arrays())
+    del ds
+    ctx = cb.Context()
+    bp = cb.Broadphase(ctx)
+    a = a0.clone()
+    p = bp.detectPossibleCollisions(a)  # sizes the output and the scratch
+    P = int(p.numel())
+    del p
+    ms = []
+    for _ in range(steps):
+        a.copy_(a0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        p = bp.detectPossibleCollisions(a)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        del p
+    dims, E = ctx.last_grid()
+    t = statistics.median(ms)
+    out = {"workload": CLUSTER_WORKLOAD, "bodies": sc.n, "pairs": P, "search_grid": list(dims), "entries": E,
+           "ms_per_step": t, "steps": steps, "value": sc.n / (t / 1000.0), "unit": "bodies/s",
+           "pairs_per_s": P / (t / 1000.0),
+           "device_gb_in_use": (lambda f: (f[1] - f[0]) / 1e9)(torch.cuda.mem_get_info()),
+           "reference": "infeasible: uint32 pair counters (Broadphase.cuh:45) cannot hold 3.9e9 pairs"}
+    del a, a0, bp, ctx
+    torch.cuda.empty_cache()
+    return out
 
 
 def bench_served(cb, dev, seconds):
@@ -474,6 +518,8 @@ def run_ours(args):
         line["batched"] = bench_batched(cb, ctx, dev)
     if rank == 0 and world == 1 and not args.no_serve:
         line["served"] = bench_served(cb, dev, args.serve_seconds)
+    if rank == 0 and world == 1 and not args.no_clustered:
+        line["clustered"] = bench_clustered(cb, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(scene, args.cpu_seconds)

@@ -149,6 +149,39 @@ def test_dense_cells_match_oracle(cb):
         assert np.array_equal(p, po), (dims, pair_set_diff(p, po))
 
 
+def test_clustered_4m_sorted_unique_and_subboxes(cb):
+    # 4,194,304 clustered spheres (about 2.5e8 pairs): the list is strictly
+    # increasing (sorted, no duplicates) and, restricted to the bodies meeting
+    # a box in a cluster core, equals the brute-force oracle there
+    s = S.clustered_spheres(1 << 22, seed=0)
+    ds = cb.DeviceScene(s)
+    a = cb.AABBGenerator().GenerateAABB(*ds.arrays())
+    p = cb.Broadphase(cb.Context()).detectPossibleCollisions(a)
+    P = p.numel()
+    assert P > 200_000_000
+    for s0 in range(0, P - 1, 1 << 27):
+        c = p[s0:min(P, s0 + (1 << 27) + 1)]
+        assert bool((c[1:] > c[:-1]).all())
+    an = a.cpu().numpy()
+    n = s.n
+    mn, mx = an[:n], an[n:]
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        c0 = mn[rng.integers(0, n)]  # a random body's corner: 90% of them lie in a cluster
+        half = 0.004
+        while True:
+            sel = np.nonzero(np.all(mn <= c0 + half, 1) & np.all(mx >= c0 - half, 1))[0]
+            if len(sel) <= 15000:
+                break
+            half /= 1.3
+        ref = O.pairs_bruteforce(np.concatenate([mn[sel], mx[sel]]))
+        ref = (sel[ref >> 32].astype(np.int64) << 32) | sel[ref & 0xFFFFFFFF].astype(np.int64)
+        mask = torch.zeros(n, dtype=torch.bool, device=p.device)
+        mask[torch.from_numpy(sel).to(p.device)] = True
+        got = torch.cat([c[mask[c >> 32] & mask[c & 0xFFFFFFFF]].cpu() for c in torch.split(p, 1 << 26)]).numpy()
+        assert np.array_equal(got, np.sort(ref)), (len(sel), len(got), len(ref))
+
+
 # ------------------------------------------------------------------ the reference's own tests
 @pytest.mark.parametrize("n", [1, 2, 10, 33, 100, 4097, 6000])
 def test_reference_test1_single_bin(cb, n):
