@@ -129,12 +129,19 @@ def bench_clustered(cb, dev, steps=3):
     ds = cb.DeviceScene(sc, device=dev)
     a0 = cb.AABBGenerator().GenerateAABB(*ds.arrays())
     del ds
+    from collide_b200 import tuner
     ctx = cb.Context()
     bp = cb.Broadphase(ctx)
     a = a0.clone()
-    p = bp.detectPossibleCollisions(a)  # sizes the output and the scratch
-    P = int(p.numel())
-    del p
+
+    def once():
+        a.copy_(a0)
+        q = bp.detectPossibleCollisions(a)
+        torch.cuda.synchronize()
+        return int(q.numel())
+    P = once()  # sizes the output and the scratch
+    best, table = tuner.tune(ctx, once, grid_candidates=((4.0, 2.0), (2.0, 2.0), (8.0, 2.0), (4.0, 1.0)),
+                             dense_candidates=(128, 512))
     ms = []
     for _ in range(steps):
         a.copy_(a0)
@@ -152,7 +159,9 @@ def bench_clustered(cb, dev, steps=3):
            "ms_per_step": t, "steps": steps, "value": sc.n / (t / 1000.0), "unit": "bodies/s",
            "pairs_per_s": P / (t / 1000.0),
            "device_gb_in_use": (lambda f: (f[1] - f[0]) / 1e9)(torch.cuda.mem_get_info()),
-           "reference": "infeasible: uint32 pair counters (Broadphase.cuh:45) cannot hold 3.9e9 pairs"}
+           "reference": "infeasible: uint32 pair counters (Broadphase.cuh:45) cannot hold 3.9e9 pairs",
+           "tuner": {"chosen": {"cell_target": best[0], "min_ratio": best[1], "dense_cell": best[2]},
+                     "candidates_ms": [[list(c), round(t, 2)] for c, t in table]}}
     del a, a0, bp, ctx
     torch.cuda.empty_cache()
     return out

@@ -121,6 +121,11 @@ class Context:
     def set_tuning(self, cell_target=4.0, min_ratio=2.0):
         self.check(lib.cc_set_tuning(self.h, float(cell_target), float(min_ratio)), "cc_set_tuning")
 
+    def set_dense_cell(self, entries=128):
+        """Cells holding more entries go to the tiled dense-cell pair test
+        (0: never)."""
+        self.check(lib.cc_set_dense_cell(self.h, int(entries)), "cc_set_dense_cell")
+
     def set_narrowphase_precision(self, mode="exact"):
         """"exact" (default): the reference's MPR arithmetic in FP64, equal to
         the FP64 oracle up to float rounding of the outputs; "fp64": FP64 in a

@@ -7,7 +7,9 @@ per axis and ``g_max`` cells in total. The pair list does not depend on the
 grid; only speed does.
 
 ``autotune`` measures a few (cell_target, min_ratio) settings on the actual
-scene and keeps the fastest per size bucket.
+scene and keeps the fastest per size bucket; ``tune`` does the same on a
+Context, together with the dense-cell threshold (which cells the tiled
+dense-cell pair test takes), and leaves the fastest setting on the context.
 """
 from __future__ import annotations
 
@@ -60,3 +62,34 @@ def autotune(run_with, candidates=((2.0, 2.0), (4.0, 2.0), (8.0, 2.0), (4.0, 1.0
     if key is not None:
         _cache[key] = best
     return best
+
+
+GRID_CANDIDATES = ((4.0, 2.0), (2.0, 2.0), (8.0, 2.0), (4.0, 1.0), (16.0, 1.0))
+DENSE_CANDIDATES = (128, 256, 512)
+
+
+def tune(ctx, run, grid_candidates=GRID_CANDIDATES, dense_candidates=DENSE_CANDIDATES, reps=1):
+    """Times run() (one call on the caller's scene through `ctx`) under every
+    (cell_target, min_ratio, dense_cell) candidate with CUDA events, sets the
+    fastest on `ctx` and returns (best, [(candidate, ms), ...]). Pairs and
+    contacts do not depend on the choice."""
+    import torch
+    table = []
+    for kt, mr in grid_candidates:
+        for dc in dense_candidates:
+            ctx.set_tuning(kt, mr)
+            ctx.set_dense_cell(dc)
+            run()  # sizes the scratch for this grid
+            best_ms = float("inf")
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                run()
+                e1.record()
+                torch.cuda.synchronize()
+                best_ms = min(best_ms, e0.elapsed_time(e1))
+            table.append(((kt, mr, dc), best_ms))
+    best = min(table, key=lambda x: x[1])[0]
+    ctx.set_tuning(best[0], best[1])
+    ctx.set_dense_cell(best[2])
+    return best, table

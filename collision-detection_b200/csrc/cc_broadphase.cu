@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
                                                     unsigned long long *__restrict__ pairs, uint64_t pair_cap,
                                                     unsigned long long *pair_counter, SceneMap sm, uint2 *dense,
                                                     uint64_t dense_cap, unsigned long long *dense_count,
-                                                    uint32_t *err) {
+                                                    uint32_t *err, uint32_t dense_cell) {
 	__shared__ Plan sp;
 	__shared__ float4 win_all[kNT / 32][2 * kWin];
 	__shared__ unsigned long long out_all[kNT / 32][kOutBuf];
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 			const uint64_t beg = cell_start[c];
 			const uint64_t end = min((uint64_t)cell_start[c + 1], entry_cap);
 			my_n = (int)(end > e + 1 ? end - e - 1 : 0);
-			if (dense && end - beg > kDenseCell) {  // left to k_pair_test_dense
+			if (dense && end - beg > dense_cell) {  // left to k_pair_test_dense
 				my_n = 0;
 				if (e == beg) {
 					const uint32_t chunks = (uint32_t)((end - beg + kNT - 1) / kNT);
@@ -787,11 +787,11 @@ void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cud
 	if (b.sm.plans)
 		k_pair_test<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                       b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
-		                                       &b.stats->dense_items, &b.stats->err);
+		                                       &b.stats->dense_items, &b.stats->err, b.dense_cell);
 	else
 		k_pair_test<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                        b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
-		                                        &b.stats->dense_items, &b.stats->err);
+		                                        &b.stats->dense_items, &b.stats->err, b.dense_cell);
 	launch_pair_test_dense(b, s);
 }
 

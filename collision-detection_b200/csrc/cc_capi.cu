@@ -253,6 +253,7 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.sm = c->sm;
 	b.dense = ptr<uint2>(c->dense);
 	b.dense_cap = c->dense.bytes / sizeof(uint2);
+	b.dense_cell = c->gp.dense_cell;
 	return b;
 }
 
@@ -700,6 +701,7 @@ cc_status cc_ctx_create(cc_ctx **out, int device) {
 	c->device = device;
 	c->gp.k_target = 4.0f;
 	c->gp.min_ratio = 2.0f;
+	c->gp.dense_cell = kDenseCell;
 	c->gp.user_dim[0] = c->gp.user_dim[1] = c->gp.user_dim[2] = 0;
 	if (const char *v = getenv("CC_GRAPH_REPLAY")) c->graph_off = v[0] == '0';
 	if (cudaSetDevice(device) != cudaSuccess || cudaMallocHost(&c->h_stats, sizeof(DevStats)) != cudaSuccess ||
@@ -775,6 +777,12 @@ cc_status cc_set_search_grid(cc_ctx *c, int gx, int gy, int gz) {
 	c->gp.user_dim[0] = pin ? gx : 0;
 	c->gp.user_dim[1] = pin ? gy : 0;
 	c->gp.user_dim[2] = pin ? gz : 0;
+	return CC_OK;
+}
+
+cc_status cc_set_dense_cell(cc_ctx *c, uint32_t entries) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	c->gp.dense_cell = entries ? std::max<uint32_t>(entries, kDenseCell) : 0xffffffffu;
 	return CC_OK;
 }
 

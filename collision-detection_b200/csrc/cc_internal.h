@@ -53,6 +53,7 @@ struct GridParams {
 	float min_ratio;  // minimum cell edge as a multiple of the mean box extent
 	int user_dim[3];  // > 0: search on exactly this grid (tuner bypassed)
 	uint32_t g_max;   // capacity of the per-cell arrays
+	uint32_t dense_cell;  // cells holding more entries go to the tiled dense-cell pair test
 };
 
 // Word ranges the first kernel of a pass zeroes (scan control words, class
@@ -131,6 +132,7 @@ struct BpBuffers {
 	SceneMap sm;                  // batch layout (empty: one scene)
 	uint2 *dense = nullptr;       // dense-cell work items (cell, first row)
 	uint64_t dense_cap = 0;
+	uint32_t dense_cell = 128;    // threshold (entries) of a dense cell
 };
 
 // Bounds pass over caller AABBs; its last block writes stats->plan.
@@ -142,8 +144,10 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
-// Cells holding more than kDenseCell entries are left out of the lane-per-entry
-// pair test and tested here instead, tile by tile (N-body style).
+// Cells holding more than b.dense_cell entries are left out of the
+// lane-per-entry pair test and tested here instead, tile by tile (N-body
+// style); kDenseCell is the default threshold and the smallest sizing unit of
+// the work list.
 constexpr uint32_t kDenseCell = 128;
 void launch_pair_test_dense(const BpBuffers &b, cudaStream_t s);
 // Device-driven emission: P is read from stats->pairs. If P exceeds the

@@ -85,6 +85,11 @@ CC_API const char *cc_version(void);
  * mean box extents wide. (gx,gy,gz) > 0 pins the grid. */
 CC_API cc_status cc_set_search_grid(cc_ctx *ctx, int gx, int gy, int gz);
 CC_API cc_status cc_set_tuning(cc_ctx *ctx, float cell_target, float min_ratio);
+/* Cells of the search grid holding more than `entries` entries (default 128,
+ * at least 128; 0 = never) are tested by the tiled dense-cell kernel instead
+ * of lane per entry. Pairs do not depend on it; the tuner picks it with the
+ * grid. No reference counterpart. */
+CC_API cc_status cc_set_dense_cell(cc_ctx *ctx, uint32_t entries);
 /* Narrowphase precision. The reference runs MPR in `real` (float). Here:
  *  CC_NP_EXACT (default): the reference's MPR arithmetic in FP64 in world
  *    coordinates, operation for operation — contacts equal those of the

@@ -143,10 +143,33 @@ def test_dense_cells_match_oracle(cb):
     _, po = O.broadphase(a, (64, 64, 64))
     assert len(po) > 1_000_000
     for dims in ((0, 0, 0), (20, 20, 20)):
-        ctx = cb.Context()
-        ctx.set_search_grid(dims)
-        _, p = gpu_broadphase(cb, a, (16, 16, 16), ctx)
-        assert np.array_equal(p, po), (dims, pair_set_diff(p, po))
+        for dense in (0, 128, 512):  # 0: every cell in the lane-per-entry kernel
+            ctx = cb.Context()
+            ctx.set_search_grid(dims)
+            ctx.set_dense_cell(dense)
+            _, p = gpu_broadphase(cb, a, (16, 16, 16), ctx)
+            assert np.array_equal(p, po), (dims, dense, pair_set_diff(p, po))
+
+
+def test_tuner_picks_a_setting_and_pairs_do_not_change(cb):
+    from collide_b200 import tuner
+    s = S.clustered_spheres(100_000, seed=4)
+    ds = cb.DeviceScene(s)
+    a0 = cb.AABBGenerator().GenerateAABB(*ds.arrays())
+    ctx = cb.Context()
+    bp = cb.Broadphase(ctx)
+    out = {}
+
+    def run():
+        a = a0.clone()
+        out["p"] = bp.detectPossibleCollisions(a)
+
+    run()
+    before = out["p"].clone()
+    best, table = tuner.tune(ctx, run, grid_candidates=((4.0, 2.0), (1.0, 1.0)), dense_candidates=(128, 0))
+    assert len(table) == 4 and best in [c for c, _ in table]
+    run()
+    assert torch.equal(out["p"], before)
 
 
 def test_clustered_4m_sorted_unique_and_subboxes(cb):
