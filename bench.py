@@ -168,9 +168,10 @@ def bench_clustered(cb, dev, steps=3):
 
 
 def bench_served(cb, dev, seconds):
-    """Poisson stream (2,000 queries/s, 70% updates / 30% new scenes) on
-    device-resident scenes: continuous batching against the per-query path,
-    plus the capacity of both with about 1,000 queries queued at once."""
+    """Poisson streams (2,000 and 4,000 queries/s, 70% updates / 30% new
+    scenes) on device-resident scenes: continuous batching against the
+    per-query path, plus the capacity of both with about 1,000 queries queued
+    at once."""
     from collide_b200 import serving as SV
     pool = [SV.PinnedScene(s) for s in SV.scene_pool(64, seed=0)]
     out = {"workload": "scene_pool: 64 mixed_slab scenes, bodies log-uniform [2,000, 500,000]; 256 resident at "
@@ -181,12 +182,16 @@ def bench_served(cb, dev, seconds):
         srv = SV.Server(pool, resident=256, budget_bytes=150e9, max_batch=256, grid=BINS, device=dev)
         srv.serve(SV.poisson_stream(2000.0, 0.1, resident=256, pool=64, seed=99), mode=mode)  # warm-up
         r = srv.serve(SV.poisson_stream(2000.0, seconds, resident=256, pool=64, seed=1), mode=mode)
+        hot = srv.serve(SV.poisson_stream(4000.0, seconds / 2, resident=256, pool=64, seed=3), mode=mode)
+        r["at_4000_qps"] = {k: hot[k] for k in ("queries", "queries_per_s", "p50_ms", "p99_ms", "mean_pass_queries")}
         cap = srv.serve(SV.poisson_stream(1e6, 1e-3, resident=256, pool=64, seed=2), mode=mode)
         r["capacity_queries_per_s"] = cap["queries_per_s"]
         r["capacity_queries"] = cap["queries"]
         out[mode] = r
         del srv
     out["p99_ratio_plain_over_batched"] = out["plain"]["p99_ms"] / out["batched"]["p99_ms"]
+    out["p99_ratio_plain_over_batched_at_4000_qps"] = (out["plain"]["at_4000_qps"]["p99_ms"] /
+                                                       out["batched"]["at_4000_qps"]["p99_ms"])
     out["capacity_ratio_batched_over_plain"] = (out["batched"]["capacity_queries_per_s"] /
                                                  out["plain"]["capacity_queries_per_s"])
     return out

@@ -196,52 +196,130 @@ class Server:
         return p.run()
 
     def serve(self, stream: Stream, mode="batched"):
+        if mode == "batched":
+            return self._serve_batched(stream)
         qs = stream.queries
         t0 = time.perf_counter()
         i = 0  # next query not yet taken
-        passes = []
         while i < len(qs):
             now = time.perf_counter() - t0
             if qs[i].arrival > now:
                 time.sleep(min(qs[i].arrival - now, 2e-4))
                 continue
-            if mode == "plain":
-                q = qs[i]
-                i += 1
-                sid = self._prepare(q)
-                if sid is not None:
-                    q.n_pairs, q.n_contacts = self.collide_one(sid)
-                torch.cuda.synchronize()
-                q.done = time.perf_counter() - t0
-                passes.append(1)
-                continue
-            # batched: everything that has arrived, up to max_batch
-            j = i
-            while j < len(qs) and j - i < self.max_batch and qs[j].arrival <= now:
-                j += 1
-            take = qs[i:j]
-            i = j
-            sids, used = [], set()
-            for q in take:  # scenes already in this pass are not evicted
-                s = self._prepare(q, pinned=used)
-                sids.append(s)
-                if s is not None:
-                    used.add(s)
-            live = [(q, s) for q, s in zip(take, sids) if s is not None]
-            if live:
-                # a scene updated twice in one pass is collided once, after both updates
-                uniq = list(dict.fromkeys(s for _, s in live))
-                res = dict(zip(uniq, self.collide_batch(uniq)))
-                for q, s in live:
-                    q.n_pairs, q.n_contacts = res[s]
+            q = qs[i]
+            i += 1
+            sid = self._prepare(q)
+            if sid is not None:
+                q.n_pairs, q.n_contacts = self.collide_one(sid)
             torch.cuda.synchronize()
-            t = time.perf_counter() - t0
-            for q in take:
-                q.done = t
-            passes.append(len(take))
+            q.done = time.perf_counter() - t0
+        return self._report(qs, t0, [1] * len(qs), mode)
+
+    def _report(self, qs, t0, passes, mode):
         wall = time.perf_counter() - t0
         lat = np.array([q.done - q.arrival for q in qs]) * 1e3
         return dict(mode=mode, queries=len(qs), wall_s=wall, queries_per_s=len(qs) / wall,
                     p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
                     mean_ms=float(lat.mean()), passes=len(passes), mean_pass_queries=float(np.mean(passes)),
                     rejected=self.rejected, resident=len(self.resident), resident_gb=self.bytes / 1e9)
+
+    def _serve_batched(self, stream: Stream):
+        """Continuous batching with the host side overlapped: a worker thread
+        runs the passes (time-step updates, then one cc_collide_scenes over
+        the pass's scenes) on its own CUDA stream, while this thread admits
+        the next arrivals and uploads their new scenes on a copy stream. A
+        pass waits for its uploads (an event); scenes referenced by a pass in
+        flight are never evicted."""
+        import queue
+        import threading
+        qs = stream.queries
+        jobs: queue.Queue = queue.Queue(maxsize=1)
+        copy_s, pass_s = torch.cuda.Stream(), torch.cuda.Stream()
+        busy: dict[int, int] = {}  # scene id -> passes in flight that use it
+        lock = threading.Lock()
+        passes = []
+        failure = []
+        t0 = time.perf_counter()
+
+        def worker():
+            try:
+                with torch.cuda.stream(pass_s):
+                    while True:
+                        job = jobs.get()
+                        if job is None:
+                            return
+                        ev, updates, uniq, scenes, live, take = job
+                        pass_s.wait_event(ev)
+                        for ds, seed in updates:
+                            perturb_(self.ctx, ds, seed)
+                        if uniq:
+                            self.batch.run(scenes)
+                            co = self.batch.contact_offsets.astype(np.int64)
+                            res = {sid: (int(self.batch.scene_pairs[k]), int(co[k + 1] - co[k]))
+                                   for k, sid in enumerate(uniq)}
+                            for q, sid in live:
+                                q.n_pairs, q.n_contacts = res[sid]
+                        pass_s.synchronize()
+                        t = time.perf_counter() - t0
+                        for q in take:
+                            q.done = t
+                        with lock:
+                            for sid in uniq:
+                                busy[sid] -= 1
+                                if busy[sid] == 0:
+                                    del busy[sid]
+            except Exception as e:  # surfaced by the main thread
+                failure.append(e)
+
+        th = threading.Thread(target=worker, daemon=True)
+        th.start()
+        i = 0
+        try:
+            while i < len(qs) and not failure:
+                now = time.perf_counter() - t0
+                if qs[i].arrival > now or jobs.full():
+                    time.sleep(2e-4 if qs[i].arrival <= now else min(qs[i].arrival - now, 2e-4))
+                    continue
+                j = i
+                while j < len(qs) and j - i < self.max_batch and qs[j].arrival <= now:
+                    j += 1
+                take = qs[i:j]
+                i = j
+                with lock:
+                    pinned = set(busy)
+                updates, live = [], []
+                with torch.cuda.stream(copy_s):
+                    for q in take:
+                        if q.kind == "new":
+                            sid = self.admit(self.pool[q.scene], pinned)
+                        else:
+                            sid = self.slots[q.scene % len(self.slots)]
+                            if sid not in self.resident:
+                                sid = None
+                            else:
+                                self.resident.move_to_end(sid)
+                                updates.append((self.resident[sid], q.seed))
+                        if sid is not None:
+                            pinned.add(sid)
+                            live.append((q, sid))
+                ev = copy_s.record_event()
+                # a scene updated twice in one pass is collided once, after both updates
+                uniq = list(dict.fromkeys(sid for _, sid in live))
+                scenes = [self.resident[sid] for sid in uniq]
+                with lock:
+                    for sid in uniq:
+                        busy[sid] = busy.get(sid, 0) + 1
+                jobs.put((ev, updates, uniq, scenes, live, take))
+                passes.append(len(take))
+        finally:
+            while th.is_alive():  # the worker may have stopped on an error
+                try:
+                    jobs.put(None, timeout=0.05)
+                    break
+                except queue.Full:
+                    continue
+            th.join()
+        if failure:
+            raise failure[0]
+        torch.cuda.synchronize()
+        return self._report(qs, t0, passes, "batched")
