@@ -121,6 +121,15 @@ class Context:
     def set_tuning(self, cell_target=4.0, min_ratio=2.0):
         self.check(lib.cc_set_tuning(self.h, float(cell_target), float(min_ratio)), "cc_set_tuning")
 
+    def set_incremental(self, on=True, margin=0.5):
+        """Keep the broadphase's cell lists between time steps of one scene,
+        boxes entered with `margin` mean extents of slack
+        (cc_set_incremental); results are identical either way."""
+        self.check(lib.cc_set_incremental(self.h, int(bool(on)), float(margin)), "cc_set_incremental")
+
+    def last_step_rebuilt(self):
+        return int(lib.cc_last_step_rebuilt(self.h))
+
     def set_dense_cell(self, entries=128):
         """Cells holding more entries go to the tiled dense-cell pair test
         (0: never)."""

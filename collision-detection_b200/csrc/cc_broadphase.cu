@@ -9,9 +9,10 @@
 //   k_scatter       cell-ordered (AABB, body) entries
 //   k_pair_test     closed AABB overlap (:237) of every entry with the later
 //                   entries of its cell; a pair is emitted only from its home
-//                   cell (the lowest cell the two cell ranges share), so each
-//                   overlapping pair appears exactly once and no unique pass is
-//                   needed (replaces :484-533)
+//                   cell (the cell holding the larger of the two min corners on
+//                   every axis, a point of both boxes and so of both cell
+//                   ranges), so each overlapping pair appears exactly once and no
+//                   unique pass is needed (replaces :484-533)
 //   scan            per-owner offsets (owner = smaller index)
 //   k_owner_scatter bucket pairs by owner; k_segsort sorts each bucket
 //                   -> the sorted, duplicate-free int64 list of :522-535
@@ -106,6 +107,15 @@ __device__ __forceinline__ CellRange cell_range(const Plan &p, float3 mn, float3
 	r.c1[2] = cell_of(mx.z, p.lo[2], p.inv[2], p.dim[2]);
 	return r;
 }
+// The cells a box enters: its own range, or (incremental steps) the range of
+// the box inflated by the plan's margin.
+__device__ __forceinline__ CellRange entry_range(const Plan &p, float3 mn, float3 mx) {
+	if (p.margin > 0.f) {
+		const float m = p.margin;
+		return cell_range(p, f3(mn.x - m, mn.y - m, mn.z - m), f3(mx.x + m, mx.y + m, mx.z + m));
+	}
+	return cell_range(p, mn, mx);
+}
 __device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
 	return (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
 }
@@ -145,7 +155,7 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
                                                 uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count,
                                                 SceneMap sm) {
 	__shared__ Plan sp;
-	__shared__ float stage[6 * kNT];
+	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	__syncthreads();
@@ -182,14 +192,110 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
 			for (int x = r.c0[0]; x <= r.c1[0]; x++) atomicAdd(&cell_count[cell_index(p, base, x, y, z)], 1u);
 }
 
+// ---- incremental steps (one scene)
+__device__ __forceinline__ unsigned long long pack_range(const CellRange &r) {
+	unsigned long long v = 0;
+	for (int d = 0; d < 3; d++) v |= ((unsigned long long)r.c0[d] << (20 * d)) | ((unsigned long long)r.c1[d] << (20 * d + 10));
+	return v;
+}
+
+// Shift in place (as k_count), zero the owner counts, and check that every
+// box still lies inside the cells it was entered in (its inflated range of
+// the step that built the lists); one that left them means rebuilding.
+__global__ void __launch_bounds__(kNT) k_count_inc(uint64_t n, float *__restrict__ aabb, DevStats *stats,
+                                                    uint32_t *__restrict__ owner_count,
+                                                    unsigned long long *__restrict__ ranges) {
+	__shared__ Plan sp;
+	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
+	__syncthreads();
+	if (!sp.valid) return;
+	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
+	load_tile_aabb(aabb, n, i0, stage);
+	__syncthreads();
+	for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
+	__syncthreads();
+	store_tile_aabb(aabb, n, i0, stage);
+	const uint64_t i = i0 + threadIdx.x;
+	bool changed = false;
+	if (i < n) {
+		const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
+		const float *hs = stage + 3 * kNT;
+		const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
+		owner_count[i] = 0u;
+		// the box must still lie in the cells it was entered in
+		const CellRange r = cell_range(sp, mn, mx);
+		const unsigned long long k = ranges[i];
+		for (int d = 0; d < 3; d++) {
+			const int c0 = (int)((k >> (20 * d)) & 1023), c1 = (int)((k >> (20 * d + 10)) & 1023);
+			if (r.c0[d] < c0 || r.c1[d] > c1) changed = true;
+		}
+	}
+	if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) atomicOr(&stats->rebuild, 1u);
+}
+
+// Counting pass of a rebuilding incremental step (the boxes are already
+// shifted): enters each box inflated by the plan's margin and records the
+// range; otherwise only tells the cell scan to do nothing.
+__global__ void __launch_bounds__(kNT) k_count_gated(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
+                                                      uint32_t *__restrict__ cell_count,
+                                                      unsigned long long *__restrict__ ranges) {
+	if (blockIdx.x == 0 && threadIdx.x == 0) stats->cells_scan = stats->rebuild ? stats->cells : 0ull;
+	if (!stats->rebuild || !stats->plan.valid) return;
+	__shared__ Plan sp;
+	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
+	if (threadIdx.x < sizeof(Plan) / 4)
+		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
+	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
+	load_tile_aabb(aabb, n, i0, stage);
+	__syncthreads();
+	const uint64_t i = i0 + threadIdx.x;
+	if (i >= n) return;
+	const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
+	const float *hs = stage + 3 * kNT;
+	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
+	const CellRange r = entry_range(sp, mn, mx);
+	ranges[i] = pack_range(r);
+	for (int z = r.c0[2]; z <= r.c1[2]; z++)
+		for (int y = r.c0[1]; y <= r.c1[1]; y++)
+			for (int x = r.c0[0]; x <= r.c1[0]; x++) atomicAdd(&cell_count[cell_index(sp, 0, x, y, z)], 1u);
+}
+
+// A step that keeps its cell lists: the entries get the bodies' new (shifted)
+// boxes; the entry count is the last step's.
+__global__ void __launch_bounds__(kNT) k_refresh_entries(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
+                                                          float4 *__restrict__ entries, uint64_t entry_cap,
+                                                          const IncState *inc) {
+	if (stats->rebuild || !stats->plan.valid) return;
+	const uint64_t E = min((uint64_t)inc->entries, entry_cap);
+	if (blockIdx.x == 0 && threadIdx.x == 0) stats->entries = E;
+	for (uint64_t e = (uint64_t)blockIdx.x * kNT + threadIdx.x; e < E; e += (uint64_t)gridDim.x * kNT) {
+		float4 lo = entries[2 * e], hi = entries[2 * e + 1];
+		const uint32_t id = __float_as_uint(lo.w);
+		if (id >= n) continue;
+		lo.x = aabb[3 * id]; lo.y = aabb[3 * id + 1]; lo.z = aabb[3 * id + 2];
+		hi.x = aabb[3 * (n + id)]; hi.y = aabb[3 * (n + id) + 1]; hi.z = aabb[3 * (n + id) + 2];
+		entries[2 * e] = lo;
+		entries[2 * e + 1] = hi;
+	}
+}
+
+__global__ void k_save_inc(const DevStats *stats, IncState *inc) {
+	inc->plan = stats->plan;
+	inc->entries = stats->entries;
+	inc->valid = stats->plan.valid && !(stats->err & (kErrCapacity | kErrSpinLimit)) ? 1u : 0u;
+}
+
 // Cell-ordered entries: one thread per body, a cursor atomic per covered cell.
 template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
                                                   const uint32_t *__restrict__ cell_start,
                                                   uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
-                                                  uint64_t cap, uint32_t *err, SceneMap sm) {
+                                                  uint64_t cap, uint32_t *err, SceneMap sm, const uint32_t *gate) {
+	if (gate && *gate == 0u) return;  // an incremental step that keeps its cell lists
 	__shared__ Plan sp;
-	__shared__ float stage[6 * kNT];
+	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
 	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
@@ -203,7 +309,7 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 	uint32_t base;
 	const Plan &p = plan_of<kBatch>(sp, sm, i, base);
 	if (kBatch && !p.valid) return;
-	const CellRange r = cell_range(p, mn, mx);
+	const CellRange r = entry_range(p, mn, mx);
 	bool over = false;
 	for (int z = r.c0[2]; z <= r.c1[2]; z++)
 		for (int y = r.c0[1]; y <= r.c1[1]; y++)
@@ -304,11 +410,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 		float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
 		float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
 		int d0 = pl.dim[0], d1 = pl.dim[1], d2 = pl.dim[2];
-		// home-cell test: the pair belongs to this cell iff, on every axis, one
-		// of the two min corners lies in this cell's slab
-		const uint32_t amask = (valid && cell_of(alo.x, lo0, iv0, d0) == cx ? 1u : 0u) |
-		                       (valid && cell_of(alo.y, lo1, iv1, d1) == cy ? 2u : 0u) |
-		                       (valid && cell_of(alo.z, lo2, iv2, d2) == cz ? 4u : 0u);
+
 		// the warp's sum(my_n) tests, dealt out 32 per round: test k belongs to
 		// the lane a with pre[a] <= k < pre[a] + my_n[a] (pre: exclusive scan)
 		int pre = my_n;
@@ -330,7 +432,6 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 				if (v <= k) a += step;
 			}
 			const int t = k - __shfl_sync(0xffffffffu, pre, a);
-			const uint32_t am = __shfl_sync(0xffffffffu, amask, a);
 			if constexpr (kBatch) {  // entries of one warp may come from different scenes
 				lo0 = __shfl_sync(0xffffffffu, pl.lo[0], a);
 				lo1 = __shfl_sync(0xffffffffu, pl.lo[1], a);
@@ -361,9 +462,11 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 				}
 				if (plo.x <= bhi.x && blo.x <= phi.x && plo.y <= bhi.y && blo.y <= phi.y && plo.z <= bhi.z &&
 				    blo.z <= phi.z) {
-					const bool hx = (am & 1u) || cell_of(blo.x, lo0, iv0, d0) == px;
-					const bool hy = (am & 2u) || cell_of(blo.y, lo1, iv1, d1) == py;
-					const bool hz = (am & 4u) || cell_of(blo.z, lo2, iv2, d2) == pz;
+					// home cell: the cell holding the larger min corner on every
+					// axis (a point of both boxes, so of both cell ranges)
+					const bool hx = cell_of(fmaxf(plo.x, blo.x), lo0, iv0, d0) == px;
+					const bool hy = cell_of(fmaxf(plo.y, blo.y), lo1, iv1, d1) == py;
+					const bool hz = cell_of(fmaxf(plo.z, blo.z), lo2, iv2, d2) == pz;
 					if (hx && hy && hz) {
 						const uint32_t ia = __float_as_uint(plo.w), idb = __float_as_uint(blo.w);
 						const uint32_t lo = min(ia, idb), hi = max(ia, idb);
@@ -442,9 +545,6 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
 		const float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
 		const float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
 		const int d0 = pl.dim[0], d1 = pl.dim[1], d2 = pl.dim[2];
-		const bool ax = row && cell_of(alo.x, lo0, iv0, d0) == cx;
-		const bool ay = row && cell_of(alo.y, lo1, iv1, d1) == cy;
-		const bool az = row && cell_of(alo.z, lo2, iv2, d2) == cz;
 		uint32_t owned = 0;
 		for (uint32_t c0 = r0; c0 < k; c0 += kNT) {
 			const uint32_t nt = min((uint32_t)kNT, k - c0);
@@ -463,9 +563,9 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
 					const float4 blo = tlo[jj], bhi = thi[jj];
 					if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
 					    blo.z <= ahi.z) {
-						const bool hx = ax || cell_of(blo.x, lo0, iv0, d0) == cx;
-						const bool hy = ay || cell_of(blo.y, lo1, iv1, d1) == cy;
-						const bool hz = az || cell_of(blo.z, lo2, iv2, d2) == cz;
+						const bool hx = cell_of(fmaxf(alo.x, blo.x), lo0, iv0, d0) == cx;
+						const bool hy = cell_of(fmaxf(alo.y, blo.y), lo1, iv1, d1) == cy;
+						const bool hz = cell_of(fmaxf(alo.z, blo.z), lo2, iv2, d2) == cz;
 						if (hx && hy && hz) {
 							const uint32_t idb = __float_as_uint(blo.w);
 							const uint32_t lo = min(ida, idb), hi = max(ida, idb);
@@ -774,10 +874,10 @@ void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStrea
 	if (!n) return;
 	if (b.sm.plans)
 		k_scatter<true><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
-		                                              b.entry_cap, &b.stats->err, b.sm);
+		                                              b.entry_cap, &b.stats->err, b.sm, nullptr);
 	else
 		k_scatter<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
-		                                               b.entry_cap, &b.stats->err, b.sm);
+		                                               b.entry_cap, &b.stats->err, b.sm, nullptr);
 }
 
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s) {
@@ -794,6 +894,26 @@ void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cud
 		                                        &b.stats->dense_items, &b.stats->err, b.dense_cell);
 	launch_pair_test_dense(b, s);
 }
+
+void launch_count_inc(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s) {
+	if (n) k_count_inc<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.owner_count, ranges);
+}
+void launch_count_gated(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s) {
+	if (n) k_count_gated<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, ranges);
+}
+void launch_scan_cells_gated(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
+	launch_scan_u32_to_u32(b.cell_count, g_max, b.cell_start, b.status, b.ticket, &b.stats->err, s,
+	                       &b.stats->cells_scan, &b.stats->entries, b.pre_zeroed, b.cell_count);
+}
+void launch_scatter_gated(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
+	if (n) k_scatter<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
+	                                                      b.entry_cap, &b.stats->err, b.sm, &b.stats->rebuild);
+}
+void launch_refresh_entries(uint64_t n, const float *aabb, const BpBuffers &b, const IncState *inc, cudaStream_t s) {
+	const unsigned grid = kNumSMs * 8;
+	k_refresh_entries<<<grid, kNT, 0, s>>>(n, aabb, b.stats, b.entries, b.entry_cap, inc);
+}
+void launch_save_inc(const BpBuffers &b, IncState *inc, cudaStream_t s) { k_save_inc<<<1, 1, 0, s>>>(b.stats, inc); }
 
 void launch_pair_test_dense(const BpBuffers &b, cudaStream_t s) {
 	if (!b.dense || !b.dense_cap) return;

@@ -85,6 +85,12 @@ struct cc_ctx {
 	// look-back status regions (words) of the cell, owner and contact-flag
 	// scans, laid out back to back in `status`
 	uint64_t st_words[3] = {0, 0, 0};
+	// incremental broadphase (cc_set_incremental): per-body cell ranges and
+	// the last step's grid; usable while n and the scratch stay the same
+	bool incremental = false, inc_valid = false;
+	float inc_margin = 0.5f;  // insertion margin in mean box extents
+	uint64_t inc_n = 0, inc_gen = 0;
+	Buf inc_state, inc_ranges;
 	// the current pass's first kernel zeroed the scan control words, the
 	// narrowphase class counters and the cell counts (ZeroList)
 	bool pass_zeroed = false;
@@ -353,9 +359,37 @@ uint64_t hint_E(const cc_ctx *c, uint64_t n) { return pow2ceil(std::max<uint64_t
 uint64_t hint_P(const cc_ctx *c) { return pow2ceil(std::max<uint64_t>(c->last_P, 1)); }
 
 // count .. owner scan: needs stats zeroed and the plan from the bounds pass.
-void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s) {
+void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool incremental = false) {
 	BpBuffers b = bp_buffers(c);
 	const uint32_t gmax = c->gp.g_max;
+	if (incremental) {
+		{
+			StageMark m(c, ST_COUNT, s);
+			launch_count_inc(n, aabb, b, ptr<unsigned long long>(c->inc_ranges), s);
+			launch_count_gated(n, aabb, b, ptr<unsigned long long>(c->inc_ranges), s);
+		}
+		{
+			StageMark m(c, ST_SCAN_CELLS, s);
+			launch_scan_cells_gated(b, gmax, s);
+		}
+		{
+			StageMark m(c, ST_SCATTER, s);
+			launch_scatter_gated(n, aabb, b, s);
+			launch_refresh_entries(n, aabb, b, ptr<IncState>(c->inc_state), s);
+		}
+		{
+			StageMark m(c, ST_PAIR_TEST, s);
+			launch_pair_test(n, b, hint_E(c, n), s);
+		}
+		launch_save_inc(b, ptr<IncState>(c->inc_state), s);
+		{
+			StageMark m(c, ST_SCAN_OWNER, s);
+			launch_scan_owner(n, b, s);
+		}
+		c->launches += 8;
+		return;
+	}
+	c->inc_valid = false;  // the kept cell lists are overwritten
 	{
 		StageMark m(c, ST_COUNT, s);
 		if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
@@ -451,9 +485,12 @@ cc_status settle(cc_ctx *c, uint64_t n, float *aabb, unsigned long long *out, ui
 			CC_TRY(ensure(c, c->dense, sizeof(uint2) * ((E + E / 8) / kDenseCell + 1024)));
 		}
 		if (P > b.pair_cap) CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * (P + P / 8)));
+		// an incremental step that kept its cell lists has them in place (its
+		// entry count is unchanged); any other step scatters them again
+		const bool keep_lists = c->incremental && !c->sm.plans && c->h_stats->rebuild == 0;
 		CC_TRY(reset_pass_counters(c, n, s));
 		b = bp_buffers(c);
-		launch_scatter(n, aabb, b, s);
+		if (!keep_lists) launch_scatter(n, aabb, b, s);
 		launch_pair_test(n, b, E, s);
 		launch_scan_owner(n, b, s);
 		c->launches += 3;
@@ -537,6 +574,13 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	c->retained = false;
 	const uint64_t n = sc.n;
 	CC_TRY(prepare(c, n, pairs_cap));
+	const bool inc = c->incremental && !c->sm.plans;
+	if (inc) {
+		CC_TRY(ensure(c, c->inc_ranges, sizeof(unsigned long long) * n));
+		CC_TRY(ensure(c, c->inc_state, sizeof(IncState)));
+	}
+	const bool inc_ready = inc && c->inc_valid && c->inc_n == n && c->inc_gen == c->buf_gen;
+	c->inc_valid = false;  // set again once this step has finished cleanly
 	DevStats *d = ptr<DevStats>(c->stats);
 	const int grid[3] = {gx, gy, gz};
 	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
@@ -560,11 +604,12 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 			StageMark m(c, ST_AABB, st);
 			CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), st));
 			launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb, d, &d->err,
-			            c->gp, grid, st, zero);
+			            c->gp, grid, st, zero, inc_ready ? ptr<IncState>(c->inc_state) : nullptr,
+			            inc ? c->inc_margin : 0.f);
 		}
 		c->launches += 1;
 		c->pass_zeroed = true;
-		enqueue_search(c, n, aabb, st);
+		enqueue_search(c, n, aabb, st, inc);
 		enqueue_emit(c, n, out, pairs_cap, st);
 		enqueue_np(c, a, pairs_cap, &d->np_n, st);
 		c->pass_zeroed = false;
@@ -574,7 +619,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	if (graphs && !c->prof && !c->graph_off) {
 		// everything the captured launches depend on
 		struct {
-			uint64_t n, nb, pairs_cap, hE, hP, gen, st[3];
+			uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
 			const void *p[18];
 			int dims[3], prec;
 			float env;
@@ -583,6 +628,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 		memset(&k, 0, sizeof(k));
 		k.n = n; k.nb = sc.nb; k.pairs_cap = pairs_cap; k.hE = hint_E(c, n); k.hP = hint_P(c); k.gen = c->buf_gen;
 		for (int r = 0; r < 3; r++) k.st[r] = c->st_words[r];
+		k.incm = (inc ? 2u : 0u) | (inc_ready ? 1u : 0u);
 		const void *ps[18] = {sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, aabb,
 		                      pairs, norm, cpta, cptb, depth, bids, nullptr, nullptr};
 		memcpy(k.p, ps, sizeof(ps));
@@ -683,9 +729,16 @@ cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, flo
 	if (sc.n == 0) return CC_OK;
 	CC_TRY(collide_enqueue(c, sc, gx, gy, gz, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids, s,
 	                       true));
+	const uint64_t gen = c->buf_gen;
 	CC_TRY(read_stats(c, s));
-	return collide_finish(c, sc, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids, n_pairs, n_contacts,
-	                      s);
+	const cc_status st = collide_finish(c, sc, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids,
+	                                    n_pairs, n_contacts, s);
+	if (st == CC_OK && c->incremental && !c->sm.plans && c->buf_gen == gen) {
+		c->inc_valid = true;  // the next step of this size may keep the cell lists
+		c->inc_n = sc.n;
+		c->inc_gen = gen;
+	}
+	return st;
 }
 
 }  // namespace
@@ -727,7 +780,7 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_off,    &c->b_scene_of, &c->b_gid,      &c->b_sst,    &c->b_plans,     &c->b_G,
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
-	               &c->g_act,    &c->g_src,      &c->g_off};
+	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
 	if (c->gexec) cudaGraphExecDestroy(c->gexec);
@@ -777,6 +830,16 @@ cc_status cc_set_search_grid(cc_ctx *c, int gx, int gy, int gz) {
 	c->gp.user_dim[0] = pin ? gx : 0;
 	c->gp.user_dim[1] = pin ? gy : 0;
 	c->gp.user_dim[2] = pin ? gz : 0;
+	return CC_OK;
+}
+
+int cc_last_step_rebuilt(const cc_ctx *c) { return c && c->h_stats ? (int)(c->h_stats->rebuild != 0) : -1; }
+
+cc_status cc_set_incremental(cc_ctx *c, int on, float margin) {
+	if (!c || !(margin > 0.f)) return CC_ERR_INVALID_ARGUMENT;
+	c->incremental = on != 0;
+	c->inc_margin = margin;
+	c->inc_valid = false;
 	return CC_OK;
 }
 
@@ -936,6 +999,7 @@ cc_status cc_broadphase_fetch(cc_ctx *c, int64_t *pairs, uint64_t pairs_cap, voi
 cc_status cc_broadphase_bins(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy, int gz, uint32_t *bin_number,
                              uint32_t *body_number, uint64_t entries_cap, uint64_t *n_entries, uint32_t *active_bins,
                              uint32_t *bin_end, uint64_t active_cap, uint64_t *n_active, void *stream) {
+	if (c) c->inc_valid = false;
 	if (!c || !n_entries || !n_active) return CC_ERR_INVALID_ARGUMENT;
 	ProfGuard pg_(c, stream);
 	c->launches = 0;

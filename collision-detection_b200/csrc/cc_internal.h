@@ -20,6 +20,16 @@ struct Plan {
 	float invbin[3];  // reference inverse bin size: grid / fabs(max + fabs(min)) (:380-381)
 	int grid[3];      // reference bins per axis
 	int valid;        // bounds were finite and every box had min <= max
+	float margin;     // incremental steps: boxes enter cells inflated by this much (0 otherwise)
+	int pad_;
+};
+
+// What an incremental broadphase keeps between two steps of one scene.
+struct IncState {
+	Plan plan;                   // the last step's search grid (in its shifted frame) and shift
+	unsigned long long entries;  // its entry count
+	uint32_t valid;
+	uint32_t pad_;
 };
 
 // Per-call device state; zeroed (one memset) at the start of every call.
@@ -40,6 +50,9 @@ struct DevStats {
 	unsigned long long cells;     // plan.G as a 64-bit scan count
 	unsigned long long np_n;      // pairs handed to the narrowphase (0 if an output was too small)
 	unsigned long long dense_items;  // (cell, row chunk) work items of the dense-cell pair test
+	unsigned long long cells_scan;   // incremental steps: cells to scan (0 when the cell lists are reused)
+	uint32_t rebuild;                // incremental steps: the cell lists must be rebuilt
+	uint32_t pad2_;
 	uint32_t blocks_done;         // last-block detection of the bounds reduction
 	uint32_t pad_;
 	Plan plan;
@@ -98,7 +111,7 @@ void radix_sort_u64(unsigned long long *keys, unsigned long long *tmp, uint64_t 
 void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
                  uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s,
-                 const ZeroList &zero = ZeroList());
+                 const ZeroList &zero = ZeroList(), const IncState *inc = nullptr, float inc_margin = 0.f);
 
 // ------------------------------------------------------------------ broadphase
 // A batch of independent scenes laid out as one concatenated scene: every
@@ -144,6 +157,17 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
+// Incremental steps (one scene; the plan's search grid carried over from the
+// last step when the scene still fits it): shift + per-body cell ranges
+// compared with the last step's (any change sets stats->rebuild); the count,
+// cell scan and scatter then run only when rebuilding, else the kept entries
+// get the new box coordinates; the last call stores the state.
+void launch_count_inc(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s);
+void launch_count_gated(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s);
+void launch_scan_cells_gated(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
+void launch_scatter_gated(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
+void launch_refresh_entries(uint64_t n, const float *aabb, const BpBuffers &b, const IncState *inc, cudaStream_t s);
+void launch_save_inc(const BpBuffers &b, IncState *inc, cudaStream_t s);
 // Cells holding more than b.dense_cell entries are left out of the
 // lane-per-entry pair test and tested here instead, tile by tile (N-body
 // style); kDenseCell is the default threshold and the smallest sizing unit of

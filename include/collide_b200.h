@@ -85,6 +85,21 @@ CC_API const char *cc_version(void);
  * mean box extents wide. (gx,gy,gz) > 0 pins the grid. */
 CC_API cc_status cc_set_search_grid(cc_ctx *ctx, int gx, int gy, int gz);
 CC_API cc_status cc_set_tuning(cc_ctx *ctx, float cell_target, float min_ratio);
+/* Incremental broadphase for time-step updates (default off). When lists are
+ * built, every box enters the cells of itself inflated by `margin` mean box
+ * extents (> 0). cc_collide keeps the search grid, those cell lists and each
+ * body's entered range; while the next step has the same shape count, the
+ * scene still fits that grid and every new box still lies inside the cells
+ * it was entered in, the count, cell scan and scatter are skipped and the
+ * kept lists get the new boxes; otherwise the lists are rebuilt. Pairs are
+ * emitted from the cell holding the larger min corner of the two boxes, which
+ * both boxes entered, so results are identical with it on or off. Any other
+ * broadphase use of the context drops the kept state. No reference
+ * counterpart. */
+CC_API cc_status cc_set_incremental(cc_ctx *ctx, int on, float margin);
+/* 1 if the last broadphase built its cell lists, 0 if an incremental step
+ * kept them. */
+CC_API int cc_last_step_rebuilt(const cc_ctx *ctx);
 /* Cells of the search grid holding more than `entries` entries (default 128,
  * at least 128; 0 = never) are tested by the tiled dense-cell kernel instead
  * of lane per entry. Pairs do not depend on it; the tuner picks it with the
