@@ -60,12 +60,42 @@ __device__ __forceinline__ vec<T> crossp(vec<T> a, vec<T> b) {
 }
 template <class T>
 __device__ __forceinline__ T len(vec<T> a) { return sqrt(dotp(a, a)); }
+// One FP64 quotient a / l from y = RN(1/l), equal to the IEEE quotient:
+// q = a*y corrected once is a faithful quotient, and one more correction
+// q + (a - l*q)*y, with the residual exact in an FMA, rounds to RN(a / l)
+// (Markstein's theorem: P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990). The
+// corrections are written as -fma(-r, y, -q) so that a = -0 keeps its sign.
+// Valid without underflow or overflow: l and a nonzero |a| in [2^-500, 2^500].
+__device__ __forceinline__ double quot_rcp(double a, double l, double y) {
+	const double q0 = a * y;
+	const double q1 = -fma(-fma(-l, q0, a), y, -q0);
+	return -fma(-fma(-l, q1, a), y, -q1);
+}
+__device__ __forceinline__ bool quot_range(double x) {
+	const double m = fabs(x);
+	return m == 0.0 || (m >= 0x1p-500 && m <= 0x1p500);
+}
+// a / l componentwise with IEEE results. In double, one correctly rounded
+// reciprocal (__drcp_rn) serves the three components: an FP64 division is a
+// dependent sequence of ~120 cycles and three of them run one after the
+// other, while the three corrections overlap (~2x faster normalization).
+template <class T>
+__device__ __forceinline__ vec<T> div3(vec<T> a, T l) {
+	if constexpr (sizeof(T) == 8) {
+		if (l >= 0x1p-500 && l <= 0x1p500 && quot_range(a.x) && quot_range(a.y) && quot_range(a.z)) {
+			const double y = __drcp_rn(l);
+			return {quot_rcp(a.x, l, y), quot_rcp(a.y, l, y), quot_rcp(a.z, l, y)};
+		}
+	}
+	return {a.x / l, a.y / l, a.z / l};
+}
 // normalize: the reference's a / |a| (exact) or a * rsqrt(a.a) (fast)
 template <class T, bool kExact>
 __device__ __forceinline__ vec<T> unit(vec<T> a) {
 	if constexpr (kExact) {
 		const T l = len(a);
-		return {a.x / l, a.y / l, a.z / l};
+		return div3(a, l);
 	} else {
 		const T il = rsqrt(dotp(a, a));
 		return {a.x * il, a.y * il, a.z * il};
@@ -119,7 +149,7 @@ __device__ __forceinline__ vec<S> support_local(int type, vec<S> B, vec<S> n) {
 			const vec<S> nn = unit<S, true>(n);
 			const vec<S> bbn = mulv(mulv(B, B), nn);
 			const S l = len(mulv(B, nn));
-			return {bbn.x / l, bbn.y / l, bbn.z / l};
+			return div3(bbn, l);
 		} else {  // B*B*n / |B*n|
 			const vec<S> bn = mulv(B, n);
 			const S il = rsqrt(dotp(bn, bn));

@@ -106,11 +106,26 @@ __global__ void __launch_bounds__(256) k_np_class_scatter(uint64_t P, const unsi
 		off[c] = acc;
 	}
 	__syncthreads();
+	// per 256-pair tile: ranks within the block from shared-memory counters,
+	// then one global cursor reservation per class and block (a few classes
+	// hold most pairs, so per-pair global atomics would serialise on them)
+	__shared__ uint32_t h[kNpClasses], base[kNpClasses];
 	uint32_t *cursor = classes + kNpClasses;
 	const uint64_t Pn = P_dev ? min(P, (uint64_t)*P_dev) : P;
-	for (uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x; i < Pn; i += (uint64_t)gridDim.x * 256) {
-		const uint32_t c = pair_class(i, n, T, pairs);
-		order[off[c] + atomicAdd(&cursor[c], 1u)] = (uint32_t)i;
+	for (uint64_t i0 = (uint64_t)blockIdx.x * 256; i0 < Pn; i0 += (uint64_t)gridDim.x * 256) {
+		if (threadIdx.x < kNpClasses) h[threadIdx.x] = 0;
+		__syncthreads();
+		const uint64_t i = i0 + threadIdx.x;
+		uint32_t c = 0, r = 0;
+		if (i < Pn) {
+			c = pair_class(i, n, T, pairs);
+			r = atomicAdd(&h[c], 1u);
+		}
+		__syncthreads();
+		if (threadIdx.x < kNpClasses && h[threadIdx.x]) base[threadIdx.x] = atomicAdd(&cursor[threadIdx.x], h[threadIdx.x]);
+		__syncthreads();
+		if (i < Pn) order[off[c] + base[c] + r] = (uint32_t)i;
+		__syncthreads();
 	}
 }
 
