@@ -137,14 +137,14 @@ __device__ __forceinline__ vec<S> mcol(vec<S> r0, vec<S> r1, vec<S> r2, vec<S> v
 
 // Local support maps (SupportFunctions.cuh:11-99), on a unit direction in the
 // exact variant; the fast variant uses that every map but the sphere's is
-// invariant to the length of n.
-template <class S, bool kExact>
-__device__ __forceinline__ vec<S> support_local(int type, vec<S> B, vec<S> n) {
-	switch (type) {
-	case SPHERE:
+// invariant to the length of n. support_local_t: the four round and boxy
+// types by compile-time type.
+template <class S, bool kExact, int TYPE>
+__device__ __forceinline__ vec<S> support_local_t(vec<S> B, vec<S> n) {
+	if constexpr (TYPE == SPHERE) {
 		if constexpr (kExact) return scl(B.x, n);
 		else return scl(B.x, unit<S, false>(n));
-	case ELLIPSOID: {
+	} else if constexpr (TYPE == ELLIPSOID) {
 		if constexpr (kExact) {
 			const vec<S> nn = unit<S, true>(n);
 			const vec<S> bbn = mulv(mulv(B, B), nn);
@@ -155,10 +155,11 @@ __device__ __forceinline__ vec<S> support_local(int type, vec<S> B, vec<S> n) {
 			const S il = rsqrt(dotp(bn, bn));
 			return {B.x * bn.x * il, B.y * bn.y * il, B.z * bn.z * il};
 		}
-	}
-	case BOX:
+	} else if constexpr (TYPE == BOX) {
 		return {sgn(n.x) * B.x, sgn(n.y) * B.y, sgn(n.z) * B.z};
-	case CYLINDER: {  // axis = local y: w = n - (u.n) u = (n.x, 0, n.z)
+	} else {
+		static_assert(TYPE == CYLINDER, "sphere, ellipsoid, box or cylinder");
+		// axis = local y: w = n - (u.n) u = (n.x, 0, n.z)
 		const vec<S> w = mk<S>(n.x, S(0), n.z);
 		const S sy = sgn(n.y) * B.y;
 		if (len(w) != S(0)) {
@@ -167,6 +168,14 @@ __device__ __forceinline__ vec<S> support_local(int type, vec<S> B, vec<S> n) {
 		}
 		return mk<S>(S(0), sy, S(0));
 	}
+}
+template <class S, bool kExact>
+__device__ __forceinline__ vec<S> support_local(int type, vec<S> B, vec<S> n) {
+	switch (type) {
+	case SPHERE: return support_local_t<S, kExact, SPHERE>(B, n);
+	case ELLIPSOID: return support_local_t<S, kExact, ELLIPSOID>(B, n);
+	case BOX: return support_local_t<S, kExact, BOX>(B, n);
+	case CYLINDER: return support_local_t<S, kExact, CYLINDER>(B, n);
 	case RECT: {
 		vec<S> r = B;
 		if (n.x < S(0)) r.x = -r.x;
@@ -432,12 +441,14 @@ __device__ __forceinline__ bool post_step(Lane<S, kExact> &L, vec<S> pa, vec<S> 
 		L.v32 = pb;
 		L.v3 = vd(pb, pa);
 		if (dotp(L.v3, L.n) <= 0.0) return false;
-		if (dotp(crossp(L.v1, L.v3), L.v0) < 0.0) {
+		// both side tests evaluated up front (independent; same arithmetic)
+		const double s13 = dotp(crossp(L.v1, L.v3), L.v0), s32 = dotp(crossp(L.v3, L.v2), L.v0);
+		if (s13 < 0.0) {
 			L.v2 = L.v3; L.v21 = L.v31; L.v22 = L.v32;
 			L.n = crossp(sub(L.v1, L.v0), sub(L.v3, L.v0));
 			return true;
 		}
-		if (dotp(crossp(L.v3, L.v2), L.v0) < 0.0) {
+		if (s32 < 0.0) {
 			L.v1 = L.v3; L.v11 = L.v31; L.v12 = L.v32;
 			L.n = crossp(sub(L.v3, L.v0), sub(L.v2, L.v0));
 			return true;
@@ -449,6 +460,10 @@ __device__ __forceinline__ bool post_step(Lane<S, kExact> &L, vec<S> pa, vec<S> 
 		const D3 v4 = vd(pb, pa);
 		const double delta = dotp(sub(v4, L.v3), L.n);
 		const double depth = dotp(v4, L.n);
+		// the three side tests of the portal update (:295-310), evaluated up
+		// front beside the termination test (independent; same arithmetic)
+		const double s41 = dotp(crossp(v4, L.v1), L.v0), s42 = dotp(crossp(v4, L.v2), L.v0),
+		             s43 = dotp(crossp(v4, L.v3), L.v0);
 		if (delta <= 1e-20 || depth <= 0.0 || L.phase2 > kMaxIter) {
 			if (!L.hit) return false;
 			const D3 v1 = L.v1, v2 = L.v2, v3v = L.v3, v0 = L.v0, n = L.n;
@@ -473,11 +488,11 @@ __device__ __forceinline__ bool post_step(Lane<S, kExact> &L, vec<S> pa, vec<S> 
 			to_post(L, unit<double, kExact>(n), pt);
 			return true;
 		}
-		if (dotp(crossp(v4, L.v1), L.v0) < 0.0) {
-			if (dotp(crossp(v4, L.v2), L.v0) < 0.0) { L.v1 = v4; L.v11 = pa; L.v12 = pb; }
+		if (s41 < 0.0) {
+			if (s42 < 0.0) { L.v1 = v4; L.v11 = pa; L.v12 = pb; }
 			else { L.v3 = v4; L.v31 = pa; L.v32 = pb; }
 		} else {
-			if (dotp(crossp(v4, L.v3), L.v0) < 0.0) { L.v2 = v4; L.v21 = pa; L.v22 = pb; }
+			if (s43 < 0.0) { L.v2 = v4; L.v21 = pa; L.v22 = pb; }
 			else { L.v1 = v4; L.v11 = pa; L.v12 = pb; }
 		}
 		return true;
