@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-clustered", action="store_true", help="skip the 16.7M clustered-sphere broadphase")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--clustered-bodies", type=int, default=1 << 24,
+                    help="body count of the clustered-sphere measurement (profiling uses smaller cases)")
+    ap.add_argument("--only-clustered", action="store_true",
+                    help="run only the clustered-sphere broadphase and print its object (one GPU)")
     return ap.parse_args()
 
 
@@ -119,13 +123,13 @@ CLUSTER_WORKLOAD = ("clustered_spheres: 16,777,216 spheres, radii log-uniform [0
                     "isotropic Gaussians (sigma 0.02, means U[0,1]^3), 10% U[0,1]^3; broadphase only")
 
 
-def bench_clustered(cb, dev, steps=3):
+def bench_clustered(cb, dev, steps=3, bodies=1 << 24):
     """The load-imbalanced broadphase: detectPossibleCollisions on 16.7M
     clustered spheres (~3.9e9 pairs, a list the reference's uint32 counters
     cannot hold)."""
     import torch
     from collide_b200 import scenes as S
-    sc = S.clustered_spheres(1 << 24, seed=0)
+    sc = S.clustered_spheres(bodies, seed=0)
     ds = cb.DeviceScene(sc, device=dev)
     a0 = cb.AABBGenerator().GenerateAABB(*ds.arrays())
     del ds
@@ -155,7 +159,8 @@ def bench_clustered(cb, dev, steps=3):
         del p
     dims, E = ctx.last_grid()
     t = statistics.median(ms)
-    out = {"workload": CLUSTER_WORKLOAD, "bodies": sc.n, "pairs": P, "search_grid": list(dims), "entries": E,
+    workload = CLUSTER_WORKLOAD if bodies == 1 << 24 else CLUSTER_WORKLOAD.replace("16,777,216", f"{bodies:,}")
+    out = {"workload": workload, "bodies": sc.n, "pairs": P, "search_grid": list(dims), "entries": E,
            "ms_per_step": t, "steps": steps, "value": sc.n / (t / 1000.0), "unit": "bodies/s",
            "pairs_per_s": P / (t / 1000.0),
            "device_gb_in_use": (lambda f: (f[1] - f[0]) / 1e9)(torch.cuda.mem_get_info()),
@@ -383,6 +388,10 @@ def run_ours(args):
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     import collide_b200 as cb
+    if args.only_clustered:
+        if rank == 0:
+            print(json.dumps({"clustered": bench_clustered(cb, dev, bodies=args.clustered_bodies)}), flush=True)
+        return 0
     scene = scene_for(rank, args.n)
     ctx = cb.Context(local)
     ds = cb.DeviceScene(scene, device=dev)
@@ -533,7 +542,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_serve:
         line["served"] = bench_served(cb, dev, args.serve_seconds)
     if rank == 0 and world == 1 and not args.no_clustered:
-        line["clustered"] = bench_clustered(cb, dev)
+        line["clustered"] = bench_clustered(cb, dev, bodies=args.clustered_bodies)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(scene, args.cpu_seconds)
