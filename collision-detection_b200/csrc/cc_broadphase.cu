@@ -555,11 +555,12 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
 			}
 			colown[threadIdx.x] = 0;
 			__syncthreads();
-			for (uint32_t jj = 0; jj < nt; jj++) {  // only j > i is tested
-				const uint32_t j = c0 + jj;
+			// only j > i is tested: on the diagonal tile (c0 == r0) that needs a
+			// check per column, every later tile lies wholly past this block's rows
+			const auto column = [&](uint32_t jj, bool test) {
 				bool emit = false;
 				unsigned long long key = 0;
-				if (row && j > i) {
+				if (test) {
 					const float4 blo = tlo[jj], bhi = thi[jj];
 					if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
 					    blo.z <= ahi.z) {
@@ -587,6 +588,12 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
 					ocnt += nb;
 					__syncwarp();
 				}
+			};
+			if (c0 == r0) {
+				for (uint32_t jj = 0; jj < nt; jj++) column(jj, row && c0 + jj > i);
+			} else {
+#pragma unroll 4
+				for (uint32_t jj = 0; jj < nt; jj++) column(jj, row);
 			}
 			__syncthreads();  // column counts complete
 			if (threadIdx.x < nt && colown[threadIdx.x])
