@@ -119,6 +119,25 @@ __device__ __forceinline__ CellRange entry_range(const Plan &p, float3 mn, float
 __device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
 	return (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
 }
+// Home-cell test by per-entry codes. cell_of is monotone, so the cell of the
+// larger min corner of two boxes is, per axis, the larger of the two min
+// corners' cells; it equals the cell (cx, cy, cz) both entries were entered in
+// exactly when one min corner's cell equals it and the other's does not
+// exceed it. home_code: bits 0-2 = min-corner cell == the cell's coordinate
+// on x/y/z, bits 3-5 = min-corner cell <= it; computed once per entry (the
+// dense-cell kernel, where most tested boxes overlap).
+__device__ __forceinline__ uint32_t home_code(const Plan &p, float4 lo, uint32_t packed_cell) {
+	const int cx = packed_cell & 1023, cy = (packed_cell >> 10) & 1023, cz = (packed_cell >> 20) & 1023;
+	const int x = cell_of(lo.x, p.lo[0], p.inv[0], p.dim[0]);
+	const int y = cell_of(lo.y, p.lo[1], p.inv[1], p.dim[1]);
+	const int z = cell_of(lo.z, p.lo[2], p.inv[2], p.dim[2]);
+	return (uint32_t)(x == cx) | ((uint32_t)(y == cy) << 1) | ((uint32_t)(z == cz) << 2) | ((uint32_t)(x <= cx) << 3) |
+	       ((uint32_t)(y <= cy) << 4) | ((uint32_t)(z <= cz) << 5);
+}
+// cell_of(max(a.min, b.min)) == cell on every axis
+__device__ __forceinline__ bool home_pair(uint32_t a, uint32_t b) {
+	return (((a & (b >> 3)) | (b & (a >> 3))) & 7u) == 7u;
+}
 
 __global__ void __launch_bounds__(kNT) k_bounds(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
                                                  PlanArgs pa, ZeroList zero) {
@@ -463,7 +482,8 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 				if (plo.x <= bhi.x && blo.x <= phi.x && plo.y <= bhi.y && blo.y <= phi.y && plo.z <= bhi.z &&
 				    blo.z <= phi.z) {
 					// home cell: the cell holding the larger min corner on every
-					// axis (a point of both boxes, so of both cell ranges)
+					// axis (a point of both boxes, so of both cell ranges); few
+					// boxes overlap in sparse cells, so it is evaluated per pair
 					const bool hx = cell_of(fmaxf(plo.x, blo.x), lo0, iv0, d0) == px;
 					const bool hy = cell_of(fmaxf(plo.y, blo.y), lo1, iv1, d1) == py;
 					const bool hz = cell_of(fmaxf(plo.z, blo.z), lo2, iv2, d2) == pz;
@@ -515,7 +535,7 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
                                                           const uint2 *__restrict__ dense, uint64_t dense_cap) {
 	__shared__ Plan sp;
 	__shared__ float4 tlo[kNT], thi[kNT];
-	__shared__ uint32_t colown[kNT];
+	__shared__ uint32_t colown[kNT], tcode[kNT];
 	__shared__ unsigned long long out_all[kNT / 32][kDenseOut];
 	if (threadIdx.x < sizeof(Plan) / 4)
 		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
@@ -539,19 +559,18 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
 		}
 		const uint32_t ida = __float_as_uint(alo.w);
 		const uint32_t pc = __float_as_uint(ahi.w);
-		const int cx = pc & 1023, cy = (pc >> 10) & 1023, cz = (pc >> 20) & 1023;
 		uint32_t cb;
 		const Plan &pl = plan_of<kBatch>(sp, sm, row ? ida : __float_as_uint(entries[2 * s0].w), cb);
-		const float lo0 = pl.lo[0], lo1 = pl.lo[1], lo2 = pl.lo[2];
-		const float iv0 = pl.inv[0], iv1 = pl.inv[1], iv2 = pl.inv[2];
-		const int d0 = pl.dim[0], d1 = pl.dim[1], d2 = pl.dim[2];
+		const uint32_t rcode = home_code(pl, alo, pc);
 		uint32_t owned = 0;
 		for (uint32_t c0 = r0; c0 < k; c0 += kNT) {
 			const uint32_t nt = min((uint32_t)kNT, k - c0);
 			__syncthreads();  // the previous tile is no longer read
 			if (threadIdx.x < nt) {
-				tlo[threadIdx.x] = entries[2 * (s0 + c0 + threadIdx.x)];
-				thi[threadIdx.x] = entries[2 * (s0 + c0 + threadIdx.x) + 1];
+				const float4 l = entries[2 * (s0 + c0 + threadIdx.x)], h = entries[2 * (s0 + c0 + threadIdx.x) + 1];
+				tlo[threadIdx.x] = l;
+				thi[threadIdx.x] = h;
+				tcode[threadIdx.x] = home_code(pl, l, __float_as_uint(h.w));  // the rows' cell
 			}
 			colown[threadIdx.x] = 0;
 			__syncthreads();
@@ -564,10 +583,7 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
 					const float4 blo = tlo[jj], bhi = thi[jj];
 					if (alo.x <= bhi.x && blo.x <= ahi.x && alo.y <= bhi.y && blo.y <= ahi.y && alo.z <= bhi.z &&
 					    blo.z <= ahi.z) {
-						const bool hx = cell_of(fmaxf(alo.x, blo.x), lo0, iv0, d0) == cx;
-						const bool hy = cell_of(fmaxf(alo.y, blo.y), lo1, iv1, d1) == cy;
-						const bool hz = cell_of(fmaxf(alo.z, blo.z), lo2, iv2, d2) == cz;
-						if (hx && hy && hz) {
+						if (home_pair(rcode, tcode[jj])) {
 							const uint32_t idb = __float_as_uint(blo.w);
 							const uint32_t lo = min(ida, idb), hi = max(ida, idb);
 							key = ((unsigned long long)lo << 32) | hi;
