@@ -741,30 +741,87 @@ __device__ __forceinline__ void bitonic_u32(uint32_t *s, int m, int t, int nt, S
 	}
 }
 
-// Buckets of 33..1024 keys: one warp per bucket, the partner halves sorted in
-// shared memory (4 KB per warp).
+// Register bitonic sort of 32*K keys held by one warp, striped: key e = 32*r
+// + lane sits in v[r] of that lane. Steps whose partner distance j is below 32
+// exchange across lanes (shuffle), the others pair registers of the same lane
+// (register distance j/32, resolved at compile time through a switch so that
+// v stays in registers).
+template <int K, int JR>
+__device__ __forceinline__ void bitonic_reg_step(uint32_t (&v)[K], int lane, int k) {
+	if constexpr (JR < K) {
+#pragma unroll
+		for (int r = 0; r < K; r++)
+			if ((r & JR) == 0) {
+				const bool up = ((32 * r + lane) & k) == 0;
+				const uint32_t x = v[r], y = v[r | JR];
+				v[r] = up ? min(x, y) : max(x, y);
+				v[r | JR] = up ? max(x, y) : min(x, y);
+			}
+	}
+}
+template <int K>
+__device__ __forceinline__ void bitonic_reg(uint32_t (&v)[K], int lane) {
+	for (int k = 2; k <= 32 * K; k <<= 1) {
+		for (int j = k >> 1; j > 0; j >>= 1) {
+			if (j < 32) {
+				const bool lower = (lane & j) == 0;
+#pragma unroll
+				for (int r = 0; r < K; r++) {
+					const uint32_t o = __shfl_xor_sync(0xffffffffu, v[r], j);
+					const bool up = ((32 * r + lane) & k) == 0;
+					v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+				}
+			} else {
+				switch (j >> 5) {
+				case 1: bitonic_reg_step<K, 1>(v, lane, k); break;
+				case 2: bitonic_reg_step<K, 2>(v, lane, k); break;
+				case 4: bitonic_reg_step<K, 4>(v, lane, k); break;
+				case 8: bitonic_reg_step<K, 8>(v, lane, k); break;
+				case 16: bitonic_reg_step<K, 16>(v, lane, k); break;
+				}
+			}
+		}
+	}
+}
+// One bucket of len <= 32*K keys: partner halves into registers (padding
+// sorts last), sorted, written back with the owner in the high half.
+template <int K>
+__device__ __forceinline__ void sort_bucket_reg(unsigned long long *__restrict__ out, uint64_t beg, uint64_t len,
+                                                uint32_t a, int lane) {
+	uint32_t v[K];
+#pragma unroll
+	for (int r = 0; r < K; r++) {
+		const uint64_t e = 32u * r + lane;
+		v[r] = e < len ? (uint32_t)out[beg + e] : 0xffffffffu;
+	}
+	bitonic_reg<K>(v, lane);
+	const unsigned long long hi = (unsigned long long)a << 32;
+#pragma unroll
+	for (int r = 0; r < K; r++) {
+		const uint64_t e = 32u * r + lane;
+		if (e < len) out[beg + e] = hi | v[r];
+	}
+}
+
+// Buckets of 33..1024 keys: one warp per bucket, sorted in registers
+// (2..32 keys per lane by bucket size).
 constexpr int kMidNT = 256;
 __global__ void __launch_bounds__(kMidNT) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
                                                          const uint32_t *__restrict__ big_list,
                                                          const unsigned long long *__restrict__ owner_off,
                                                          unsigned long long *__restrict__ out) {
-	__shared__ uint32_t s_all[kMidNT / 32][kMidSeg];
 	if (stats->np_n != stats->pairs) return;
 	const uint64_t nmid = min((uint64_t)stats->big_segments, big_cap);
-	uint32_t *s = s_all[threadIdx.x >> 5];
 	const int lane = threadIdx.x & 31;
 	const uint64_t warps = (uint64_t)gridDim.x * (kMidNT / 32);
 	for (uint64_t g = (uint64_t)blockIdx.x * (kMidNT / 32) + (threadIdx.x >> 5); g < nmid; g += warps) {
 		const uint32_t a = big_list[g];
-		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
-		int m = 64;
-		while ((uint64_t)m < len) m <<= 1;
-		for (int i = lane; i < m; i += 32) s[i] = (uint64_t)i < len ? (uint32_t)out[beg + i] : 0xffffffffu;
-		__syncwarp();
-		bitonic_u32(s, m, lane, 32, [] { __syncwarp(); });
-		const unsigned long long hi = (unsigned long long)a << 32;
-		for (int i = lane; (uint64_t)i < len; i += 32) out[beg + i] = hi | s[i];
-		__syncwarp();
+		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;  // 33..1024, listed by k_segsort
+		if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane);
+		else if (len <= 128) sort_bucket_reg<4>(out, beg, len, a, lane);
+		else if (len <= 256) sort_bucket_reg<8>(out, beg, len, a, lane);
+		else if (len <= 512) sort_bucket_reg<16>(out, beg, len, a, lane);
+		else sort_bucket_reg<32>(out, beg, len, a, lane);
 	}
 }
 
