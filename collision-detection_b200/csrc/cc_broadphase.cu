@@ -632,37 +632,20 @@ __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t
 	if (blockIdx.x == 0 && threadIdx.x == 0) stats->np_n = fits ? P : 0ull;
 	if (!fits) return;
 	// lanes of a warp whose pairs share an owner take their slots with one
-	// atomic (pair lists of dense cells arrive grouped by owner). A warp
-	// handles kOwnU x 32 consecutive keys per round, so that the slot atomics
-	// and offset loads of kOwnU keys per lane are in flight together (the
-	// kernel waits on memory); the order of keys inside an owner's bucket is
-	// immaterial, the bucket sort follows.
-	constexpr int kOwnU = 4;
+	// atomic (pair lists of dense cells arrive grouped by owner)
 	const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
-	const uint64_t step = (uint64_t)gridDim.x * kNT * kOwnU;
-	for (uint64_t t0 = ((uint64_t)blockIdx.x * kNT + (threadIdx.x & ~31u)) * kOwnU; t0 < P; t0 += step) {
-		unsigned long long key[kOwnU], off[kOwnU];
-		uint32_t a[kOwnU], peers[kOwnU], base[kOwnU];
-#pragma unroll
-		for (int u = 0; u < kOwnU; u++) {
-			const uint64_t t = t0 + 32u * u + lane;
-			key[u] = t < P ? tmp[t] : 0ull;
-			a[u] = t < P ? (uint32_t)(key[u] >> 32) : 0xffffffffu;
-		}
-#pragma unroll
-		for (int u = 0; u < kOwnU; u++) {
-			const bool valid = t0 + 32u * u + lane < P;
-			peers[u] = __match_any_sync(0xffffffffu, a[u]);
-			base[u] = 0;
-			if (valid && (int)lane == __ffs(peers[u]) - 1)
-				base[u] = atomicSub(&owner_count[a[u]], (uint32_t)__popc(peers[u]));
-			off[u] = valid ? owner_off[a[u]] : 0ull;
-		}
-#pragma unroll
-		for (int u = 0; u < kOwnU; u++) {
-			const uint32_t b = __shfl_sync(0xffffffffu, base[u], __ffs(peers[u]) - 1);
-			if (t0 + 32u * u + lane < P) out[off[u] + b - 1u - __popc(peers[u] & lt)] = key[u];
-		}
+	const uint64_t step = (uint64_t)gridDim.x * kNT;
+	for (uint64_t t0 = (uint64_t)blockIdx.x * kNT + (threadIdx.x & ~31u); t0 < P; t0 += step) {
+		const uint64_t t = t0 + lane;
+		const bool valid = t < P;
+		const unsigned long long key = valid ? tmp[t] : 0ull;
+		const uint32_t a = valid ? (uint32_t)(key >> 32) : 0xffffffffu;
+		const uint32_t peers = __match_any_sync(0xffffffffu, a);
+		const int leader = __ffs(peers) - 1;
+		uint32_t base = 0;
+		if (valid && (int)lane == leader) base = atomicSub(&owner_count[a], (uint32_t)__popc(peers));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if (valid) out[owner_off[a] + base - 1u - __popc(peers & lt)] = key;
 	}
 }
 
