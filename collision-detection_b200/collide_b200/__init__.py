@@ -127,6 +127,12 @@ class Context:
         (cc_set_incremental); results are identical either way."""
         self.check(lib.cc_set_incremental(self.h, int(bool(on)), float(margin)), "cc_set_incremental")
 
+    def set_static_shapes(self, on=True):
+        """Host steps copy the shape arrays (T, A, B, C, R, ID) only when they
+        are other arrays than last time; body poses are copied every step.
+        Call again after changing shape arrays in place."""
+        self.check(lib.cc_set_static_shapes(self.h, int(bool(on))), "cc_set_static_shapes")
+
     def last_step_rebuilt(self):
         return int(lib.cc_last_step_rebuilt(self.h))
 
@@ -414,8 +420,11 @@ class HostSession:
         self.depth = e(cap, torch.float32)
         self.bids = e((cap, 2), torch.int32)
 
-    def input_bytes(self):
-        return int(sum(t.numel() * t.element_size() for t in self.inputs))
+    def input_bytes(self, poses_only=False):
+        """Host-to-device bytes of one step: every input array, or with static
+        shapes (Context.set_static_shapes) the body poses and flags alone."""
+        ts = self.inputs[6:] if poses_only else self.inputs
+        return int(sum(t.numel() * t.element_size() for t in ts))
 
     def output_bytes(self):
         k = self.n_contacts

@@ -22,6 +22,7 @@ namespace {
 struct Buf {
 	void *p = nullptr;
 	size_t bytes = 0;
+	uint64_t allocs = 0;  // times allocated (a new allocation may reuse the old address)
 };
 
 // Kernel stages timed by the optional profiler.
@@ -66,6 +67,19 @@ struct cc_ctx {
 	uint64_t buf_gen = 0;
 	// ensure() in dry-run mode records would_grow instead of reallocating
 	bool dry_run = false, would_grow = false;
+	// host steps with static shapes (cc_set_static_shapes): which host arrays
+	// of which size each device copy of the six shape arrays holds; a copy is
+	// reused while on, the same and of the current generation (every setter
+	// call starts a new one)
+	struct ShapeCopy {
+		const void *src[6] = {};
+		void *dst[6] = {};
+		uint64_t allocs[6] = {};  // the device buffers' allocation counts at the copy
+		uint64_t n = 0, gen = 0;
+	};
+	bool static_shapes = false;
+	uint64_t shapes_gen = 1;
+	ShapeCopy in_shapes, hs_shapes[2];
 	// pipelined host steps (cc_collide_host_submit / _wait): two slots of
 	// device inputs and outputs; copies in on one stream, the pipeline on
 	// another, copies out on a third
@@ -155,6 +169,7 @@ cc_status ensure(cc_ctx *c, Buf &b, size_t bytes) {
 	}
 	CC_CUDA(c, cudaMalloc(&b.p, nb));
 	b.bytes = nb;
+	b.allocs++;
 	c->buf_gen++;
 	return CC_OK;
 }
@@ -862,6 +877,13 @@ cc_status cc_set_narrowphase_precision(cc_ctx *c, int mode) {
 	return CC_OK;
 }
 
+cc_status cc_set_static_shapes(cc_ctx *c, int on) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	c->static_shapes = on != 0;
+	c->shapes_gen++;  // every call drops the kept copies
+	return CC_OK;
+}
+
 cc_status cc_get_last_grid(const cc_ctx *c, int *dims3, uint64_t *entries) {
 	if (!c) return CC_ERR_INVALID_ARGUMENT;
 	if (dims3)
@@ -1353,6 +1375,27 @@ cc_status host_copy_out(cc_ctx *c, cc_ctx::HostSlot &h, cc_result *res, uint64_t
 	return CC_OK;
 }
 
+// The six shape arrays of a host step (T, A, B, C, R, ID) into dst, unless
+// static shapes are on and dst already holds these host arrays' contents.
+cc_status upload_shapes(cc_ctx *c, cc_ctx::ShapeCopy &sh, Buf *const dst[6], const cc_scene *sc, cudaStream_t t) {
+	const void *src[6] = {sc->T, sc->A, sc->B, sc->C, sc->R, sc->ID};
+	static const uint64_t bytes[6] = {4, 12, 12, 12, 16, 4};
+	bool same = c->static_shapes && sh.gen == c->shapes_gen && sh.n == sc->n;
+	for (int k = 0; k < 6; k++)
+		same = same && sh.src[k] == src[k] && sh.dst[k] == dst[k]->p && sh.allocs[k] == dst[k]->allocs;
+	if (same) return CC_OK;
+	sh.gen = 0;  // not valid until every copy is enqueued
+	for (int k = 0; k < 6; k++) {
+		CC_CUDA(c, cudaMemcpyAsync(dst[k]->p, src[k], bytes[k] * sc->n, cudaMemcpyHostToDevice, t));
+		sh.src[k] = src[k];
+		sh.dst[k] = dst[k]->p;
+		sh.allocs[k] = dst[k]->allocs;
+	}
+	sh.n = sc->n;
+	sh.gen = c->shapes_gen;
+	return CC_OK;
+}
+
 // Sizes one slot for a scene of n shapes / nb bodies and cap pairs and points
 // its device view at it.
 cc_status host_slot_prepare(cc_ctx *c, cc_ctx::HostSlot &h, uint64_t n, uint64_t nb, uint64_t cap) {
@@ -1423,12 +1466,8 @@ cc_status cc_collide_host_submit(cc_ctx *c, const cc_scene *sc, int gx, int gy, 
 	{
 		StageMark m(c, ST_COPY_IN, c->hs_copy);
 		cudaStream_t t = c->hs_copy;
-		CC_CUDA(c, cudaMemcpyAsync(h.T.p, sc->T, 4 * n, cudaMemcpyHostToDevice, t));
-		CC_CUDA(c, cudaMemcpyAsync(h.A.p, sc->A, 12 * n, cudaMemcpyHostToDevice, t));
-		CC_CUDA(c, cudaMemcpyAsync(h.B.p, sc->B, 12 * n, cudaMemcpyHostToDevice, t));
-		CC_CUDA(c, cudaMemcpyAsync(h.C.p, sc->C, 12 * n, cudaMemcpyHostToDevice, t));
-		CC_CUDA(c, cudaMemcpyAsync(h.R.p, sc->R, 16 * n, cudaMemcpyHostToDevice, t));
-		CC_CUDA(c, cudaMemcpyAsync(h.ID.p, sc->ID, 4 * n, cudaMemcpyHostToDevice, t));
+		Buf *const dst[6] = {&h.T, &h.A, &h.B, &h.C, &h.R, &h.ID};
+		CC_TRY(upload_shapes(c, c->hs_shapes[c->hs_next], dst, sc, t));
 		CC_CUDA(c, cudaMemcpyAsync(h.pos.p, sc->body_pos, 12 * nb, cudaMemcpyHostToDevice, t));
 		CC_CUDA(c, cudaMemcpyAsync(h.rot.p, sc->body_rot, 16 * nb, cudaMemcpyHostToDevice, t));
 		CC_CUDA(c, cudaMemcpyAsync(h.act.p, sc->active, nb, cudaMemcpyHostToDevice, t));
@@ -1535,12 +1574,10 @@ cc_status cc_collide_host(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz,
 	CC_TRY(ensure(c, c->out_depth, 4 * std::max<uint64_t>(cap, 1)));
 	CC_TRY(ensure(c, c->out_bids, 8 * std::max<uint64_t>(cap, 1)));
 	std::unique_ptr<StageMark> cin(new StageMark(c, ST_COPY_IN, s));
-	CC_CUDA(c, cudaMemcpyAsync(c->in_T.p, sc->T, 4 * n, cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(c->in_A.p, sc->A, 12 * n, cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(c->in_B.p, sc->B, 12 * n, cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(c->in_C.p, sc->C, 12 * n, cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(c->in_R.p, sc->R, 16 * n, cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(c->in_ID.p, sc->ID, 4 * n, cudaMemcpyHostToDevice, s));
+	{
+		Buf *const dst[6] = {&c->in_T, &c->in_A, &c->in_B, &c->in_C, &c->in_R, &c->in_ID};
+		CC_TRY(upload_shapes(c, c->in_shapes, dst, sc, s));
+	}
 	CC_CUDA(c, cudaMemcpyAsync(c->in_pos.p, sc->body_pos, 12 * nb, cudaMemcpyHostToDevice, s));
 	CC_CUDA(c, cudaMemcpyAsync(c->in_rot.p, sc->body_rot, 16 * nb, cudaMemcpyHostToDevice, s));
 	CC_CUDA(c, cudaMemcpyAsync(c->in_act.p, sc->active, nb, cudaMemcpyHostToDevice, s));

@@ -274,6 +274,18 @@ CC_API cc_status cc_collide_host(cc_ctx *ctx, const cc_scene *scene, int gx, int
 CC_API cc_status cc_collide_host_submit(cc_ctx *ctx, const cc_scene *scene, int gx, int gy, int gz, float envelope,
                                         cc_result *res, void *stream);
 CC_API cc_status cc_collide_host_wait(cc_ctx *ctx, cc_result *res, void *stream);
+/* Static shapes for host steps (cc_collide_host, cc_collide_host_submit).
+ * In a simulation the shape arrays T, A, B, C, R, ID (60 of the 89 bytes per
+ * shape and body) stay the same from step to step while the body poses move.
+ * With on != 0 a host step copies those six arrays only when their host
+ * pointers or the shape count differ from the last copy into the same device
+ * buffers; body_pos, body_rot and active are copied every step. The caller
+ * must not change the shape arrays' contents in place while this is on, or
+ * must call cc_set_static_shapes(ctx, 1) again after doing so: every call of
+ * this function drops the kept copies. Off by default; results are identical
+ * either way. No reference counterpart (the reference takes device vectors
+ * that its caller keeps up to date). */
+CC_API cc_status cc_set_static_shapes(cc_ctx *ctx, int on);
 
 /* Number of kernels the last call on this context launched. */
 CC_API uint64_t cc_last_launch_count(const cc_ctx *ctx);
