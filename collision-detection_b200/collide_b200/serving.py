@@ -7,7 +7,8 @@ cc_perturb_bodies launch on the device) or a new scene (copied from pinned
 host memory, then admitted). Admission is by byte accounting against an HBM
 budget: a new scene is admitted when its bytes fit, after evicting idle
 scenes least recently used first; otherwise the query is rejected (and
-counted).
+counted). Resident scenes are placed in one device arena reserved when the
+server starts, so serving a stream allocates no device memory.
 
 Server.serve() runs an arrival stream against the wall clock. In batched
 mode every loop iteration takes ALL queries that have arrived (up to
@@ -20,7 +21,9 @@ its own bounds, shift and grid).
 """
 from __future__ import annotations
 
+import bisect
 import ctypes
+import gc
 import math
 import time
 from collections import OrderedDict
@@ -65,12 +68,69 @@ class PinnedScene:
     def nbytes(self):
         return self.scene.nbytes()
 
-    def upload(self, device) -> DeviceScene:
+    def device_bytes(self) -> int:
+        """Bytes of the device copy, each array starting on a 256-byte boundary."""
+        return sum(_align(v.numel() * v.element_size()) for v in self.t.values())
+
+    def upload(self, device, copy_stream=None, space=None) -> DeviceScene:
+        """The device copy, filled on copy_stream if given. space: a uint8
+        device tensor of device_bytes() to hold the arrays (views into it);
+        without it each array is a new allocation."""
         ds = DeviceScene.__new__(DeviceScene)
         ds.n, ds.nb = self.n, self.nb
+        off = 0
         for k, v in self.t.items():
-            setattr(ds, k, v.to(device, non_blocking=True))
+            nbytes = v.numel() * v.element_size()
+            if space is None:
+                d = torch.empty(v.shape, dtype=v.dtype, device=device)
+            else:
+                d = space[off:off + nbytes].view(v.dtype).view(v.shape)
+                off += _align(nbytes)
+            if copy_stream is None:
+                d.copy_(v, non_blocking=True)
+            else:
+                with torch.cuda.stream(copy_stream):
+                    d.copy_(v, non_blocking=True)
+            setattr(ds, k, d)
         return ds
+
+
+def _align(nbytes, a=256):
+    return (int(nbytes) + a - 1) // a * a
+
+
+class Arena:
+    """One device buffer holding the resident scenes' arrays, placed first-fit
+    with free neighbours merged. Admitting a scene is then a copy into space
+    the server already owns: no device allocation (cudaMalloc stalls every
+    thread that uses the device) while queries are served."""
+
+    def __init__(self, nbytes, device):
+        self.size = _align(nbytes)
+        self.buf = torch.empty(self.size, dtype=torch.uint8, device=device)
+        self.free = [(0, self.size)]  # (offset, bytes), by offset
+
+    def take(self, nbytes):
+        nbytes = _align(nbytes)
+        for k, (off, sz) in enumerate(self.free):
+            if sz >= nbytes:
+                if sz == nbytes:
+                    del self.free[k]
+                else:
+                    self.free[k] = (off + nbytes, sz - nbytes)
+                return off
+        return None
+
+    def give(self, off, nbytes):
+        nbytes = _align(nbytes)
+        k = bisect.bisect_left(self.free, (off, 0))
+        self.free.insert(k, (off, nbytes))
+        if k + 1 < len(self.free) and off + nbytes == self.free[k + 1][0]:  # merge the next range
+            self.free[k] = (off, nbytes + self.free[k + 1][1])
+            del self.free[k + 1]
+        if k > 0 and self.free[k - 1][0] + self.free[k - 1][1] == self.free[k][0]:  # and the previous
+            self.free[k - 1] = (self.free[k - 1][0], self.free[k - 1][1] + self.free[k][1])
+            del self.free[k]
 
 
 @dataclass
@@ -117,15 +177,15 @@ def scene_pool(count=64, nmin=2000, nmax=500_000, seed=0):
 class Server:
     def __init__(self, pool, resident=256, budget_bytes=150e9, max_batch=256, grid=(16, 16, 16), precision="exact",
                  device="cuda", reserve_bytes=None):
-        # reserve the working set up front (torch keeps a freed block cached
-        # and carves later scenes from it): admitting a scene then costs a
-        # copy, not a device allocation
+        # the resident scenes live in one arena reserved up front, so admitting
+        # a scene costs a copy, not a device allocation (reserve_bytes=0: one
+        # allocation per array instead)
         reserve = int(min(budget_bytes, 32e9) if reserve_bytes is None else reserve_bytes)
-        if reserve > 0:
-            del_me = torch.empty(reserve, dtype=torch.uint8, device=device)
-            del del_me
+        self.arena = Arena(reserve, device) if reserve > 0 else None
         self.pool = [p if isinstance(p, PinnedScene) else PinnedScene(p) for p in pool]
         self.device = device
+        # the batched loop's streams, kept for the server's lifetime
+        self.copy_s, self.pass_s = torch.cuda.Stream(device), torch.cuda.Stream(device)
         self.budget, self.max_batch, self.grid = float(budget_bytes), int(max_batch), tuple(grid)
         self.ctx = Context()
         self.ctx.set_narrowphase_precision(precision)
@@ -148,28 +208,43 @@ class Server:
         torch.cuda.synchronize()
 
     # -- residency ------------------------------------------------------
-    def admit(self, ps: PinnedScene, pinned=()):
+    def admit(self, ps: PinnedScene, pinned=(), copy_stream=None):
         """Makes a pool scene resident; evicts idle scenes (least recently
         used first, never one in `pinned`) until it fits. Returns its id, or
-        None if it cannot fit."""
+        None if it cannot fit. The upload runs on copy_stream if given."""
         need = int(ps.nbytes() + 24 * ps.n)
-        if self.bytes + need > self.budget:
-            for sid in [s for s in self.resident if s not in pinned]:
-                if self.bytes + need <= self.budget:
+        place = ps.device_bytes()
+
+        # evict least recently used idle scenes until the scene fits the
+        # budget and a free range of the arena
+        victims = (s for s in list(self.resident) if s not in pinned)
+        at = None
+        while True:
+            if self.bytes + need <= self.budget:
+                at = self.arena.take(place) if self.arena is not None else -1
+                if at is not None:
                     break
-                ds = self.resident.pop(sid)
-                self.bytes -= ds.resident_bytes
-                self.plain.pop(sid, None)
-        if self.bytes + need > self.budget:
-            self.rejected += 1
-            return None
-        ds = ps.upload(self.device)
+            sid = next(victims, None)
+            if sid is None:
+                self.rejected += 1
+                return None
+            self._evict(sid)
+        space = None if self.arena is None else self.arena.buf[at:at + place]
+        ds = ps.upload(self.device, copy_stream, space)
+        ds.arena_at, ds.arena_bytes = at, place
         ds.resident_bytes = need
         sid = self.next_id
         self.next_id += 1
         self.resident[sid] = ds
         self.bytes += need
         return sid
+
+    def _evict(self, sid):
+        ds = self.resident.pop(sid)
+        self.bytes -= ds.resident_bytes
+        self.plain.pop(sid, None)
+        if self.arena is not None:
+            self.arena.give(ds.arena_at, ds.arena_bytes)
 
     def _prepare(self, q: Query, pinned=()):
         """Applies a query's input; returns its resident scene id (None: the
@@ -196,6 +271,17 @@ class Server:
         return p.run()
 
     def serve(self, stream: Stream, mode="batched"):
+        """Runs a query stream; Python's cyclic garbage collector is paused
+        meanwhile (a full collection stalls the loop for tens of ms)."""
+        was = gc.isenabled()
+        gc.disable()
+        try:
+            return self._serve(stream, mode)
+        finally:
+            if was:
+                gc.enable()
+
+    def _serve(self, stream: Stream, mode):
         if mode == "batched":
             return self._serve_batched(stream)
         qs = stream.queries
@@ -234,7 +320,7 @@ class Server:
         import threading
         qs = stream.queries
         jobs: queue.Queue = queue.Queue(maxsize=1)
-        copy_s, pass_s = torch.cuda.Stream(), torch.cuda.Stream()
+        copy_s, pass_s = self.copy_s, self.pass_s
         busy: dict[int, int] = {}  # scene id -> passes in flight that use it
         lock = threading.Lock()
         passes = []
@@ -288,20 +374,19 @@ class Server:
                 with lock:
                     pinned = set(busy)
                 updates, live = [], []
-                with torch.cuda.stream(copy_s):
-                    for q in take:
-                        if q.kind == "new":
-                            sid = self.admit(self.pool[q.scene], pinned)
+                for q in take:
+                    if q.kind == "new":
+                        sid = self.admit(self.pool[q.scene], pinned, copy_s)
+                    else:
+                        sid = self.slots[q.scene % len(self.slots)]
+                        if sid not in self.resident:
+                            sid = None
                         else:
-                            sid = self.slots[q.scene % len(self.slots)]
-                            if sid not in self.resident:
-                                sid = None
-                            else:
-                                self.resident.move_to_end(sid)
-                                updates.append((self.resident[sid], q.seed))
-                        if sid is not None:
-                            pinned.add(sid)
-                            live.append((q, sid))
+                            self.resident.move_to_end(sid)
+                            updates.append((self.resident[sid], q.seed))
+                    if sid is not None:
+                        pinned.add(sid)
+                        live.append((q, sid))
                 ev = copy_s.record_event()
                 # a scene updated twice in one pass is collided once, after both updates
                 uniq = list(dict.fromkeys(sid for _, sid in live))
