@@ -181,7 +181,8 @@ def bench_served(cb, dev, seconds):
     pool = [SV.PinnedScene(s) for s in SV.scene_pool(64, seed=0)]
     out = {"workload": "scene_pool: 64 mixed_slab scenes, bodies log-uniform [2,000, 500,000]; 256 resident at "
                        "start; updates move bodies by N(0,1e-4^2) and turn them by <= 1e-3 rad; new scenes come "
-                       "from pinned host memory; HBM budget 150 GB, scenes placed in a 32 GB arena reserved at start-up",
+                       "from pinned host memory; HBM budget 150 GB, scenes placed in a 32 GB arena reserved at "
+                       "start-up",
            "rate_qps": 2000.0, "duration_s": seconds}
     for mode in ("batched", "plain"):
         srv = SV.Server(pool, resident=256, budget_bytes=150e9, max_batch=256, grid=BINS, device=dev)
