@@ -729,42 +729,46 @@ __device__ __forceinline__ void bitonic_u32(uint32_t *s, int m, int t, int nt, S
 // exchange across lanes (shuffle), the others pair registers of the same lane
 // (register distance j/32, resolved at compile time through a switch so that
 // v stays in registers).
+// el = the key index held in v[0] by this lane (the warp's first key +
+// lane); the network sorts key e ascending where (e & k) == 0 in merge size k.
 template <int K, int JR>
-__device__ __forceinline__ void bitonic_reg_step(uint32_t (&v)[K], int lane, int k) {
+__device__ __forceinline__ void bitonic_reg_step(uint32_t (&v)[K], int el, int k) {
 	if constexpr (JR < K) {
 #pragma unroll
 		for (int r = 0; r < K; r++)
 			if ((r & JR) == 0) {
-				const bool up = ((32 * r + lane) & k) == 0;
+				const bool up = ((el + 32 * r) & k) == 0;
 				const uint32_t x = v[r], y = v[r | JR];
 				v[r] = up ? min(x, y) : max(x, y);
 				v[r | JR] = up ? max(x, y) : min(x, y);
 			}
 	}
 }
+// One step of partner distance j < 32 * K (inside the warp's keys).
 template <int K>
-__device__ __forceinline__ void bitonic_reg(uint32_t (&v)[K], int lane) {
-	for (int k = 2; k <= 32 * K; k <<= 1) {
-		for (int j = k >> 1; j > 0; j >>= 1) {
-			if (j < 32) {
-				const bool lower = (lane & j) == 0;
+__device__ __forceinline__ void bitonic_warp_step(uint32_t (&v)[K], int el, int j, int k) {
+	if (j < 32) {
+		const bool lower = (el & j) == 0;
 #pragma unroll
-				for (int r = 0; r < K; r++) {
-					const uint32_t o = __shfl_xor_sync(0xffffffffu, v[r], j);
-					const bool up = ((32 * r + lane) & k) == 0;
-					v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
-				}
-			} else {
-				switch (j >> 5) {
-				case 1: bitonic_reg_step<K, 1>(v, lane, k); break;
-				case 2: bitonic_reg_step<K, 2>(v, lane, k); break;
-				case 4: bitonic_reg_step<K, 4>(v, lane, k); break;
-				case 8: bitonic_reg_step<K, 8>(v, lane, k); break;
-				case 16: bitonic_reg_step<K, 16>(v, lane, k); break;
-				}
-			}
+		for (int r = 0; r < K; r++) {
+			const uint32_t o = __shfl_xor_sync(0xffffffffu, v[r], j);
+			const bool up = ((el + 32 * r) & k) == 0;
+			v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+		}
+	} else {
+		switch (j >> 5) {
+		case 1: bitonic_reg_step<K, 1>(v, el, k); break;
+		case 2: bitonic_reg_step<K, 2>(v, el, k); break;
+		case 4: bitonic_reg_step<K, 4>(v, el, k); break;
+		case 8: bitonic_reg_step<K, 8>(v, el, k); break;
+		case 16: bitonic_reg_step<K, 16>(v, el, k); break;
 		}
 	}
+}
+template <int K>
+__device__ __forceinline__ void bitonic_reg(uint32_t (&v)[K], int lane) {
+	for (int k = 2; k <= 32 * K; k <<= 1)
+		for (int j = k >> 1; j > 0; j >>= 1) bitonic_warp_step<K>(v, lane, j, k);
 }
 // One bucket of len <= 32*K keys: partner halves into registers (padding
 // sorts last), sorted, written back with the owner in the high half.
@@ -786,10 +790,52 @@ __device__ __forceinline__ void sort_bucket_reg(unsigned long long *__restrict__
 	}
 }
 
+// A bucket of 1025..2048 keys on a pair of warps (half = 0, 1), 1024 keys
+// each, 32 per lane; the one step of partner distance 1024 exchanges through
+// the pair's 8 KB of shared memory x, the pair synchronizing on its own
+// named barrier `bar` (both warps run the same steps).
+constexpr int kPairSeg = 2048;
+__device__ __forceinline__ void pair_sync(int bar) { asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory"); }
+__device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict__ out, uint64_t beg, uint64_t len,
+                                                 uint32_t a, int half, int lane, uint32_t *x, int bar) {
+	const int el = half * 1024 + lane;
+	uint32_t v[32];
+#pragma unroll
+	for (int r = 0; r < 32; r++) {
+		const uint64_t e = (uint64_t)el + 32u * r;
+		v[r] = e < len ? (uint32_t)out[beg + e] : 0xffffffffu;
+	}
+	for (int k = 2; k <= kPairSeg; k <<= 1)
+		for (int j = k >> 1; j > 0; j >>= 1) {
+			if (j == 1024) {
+#pragma unroll
+				for (int r = 0; r < 32; r++) x[el + 32 * r] = v[r];
+				pair_sync(bar);
+				const bool lower = half == 0;
+#pragma unroll
+				for (int r = 0; r < 32; r++) {
+					const uint32_t o = x[(el + 32 * r) ^ 1024];
+					const bool up = ((el + 32 * r) & k) == 0;
+					v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+				}
+				pair_sync(bar);  // x is free again
+			} else {
+				bitonic_warp_step<32>(v, el, j, k);
+			}
+		}
+	const unsigned long long hi = (unsigned long long)a << 32;
+#pragma unroll
+	for (int r = 0; r < 32; r++) {
+		const uint64_t e = (uint64_t)el + 32u * r;
+		if (e < len) out[beg + e] = hi | v[r];
+	}
+}
+
 // Buckets of 33..1024 keys: one warp per bucket, sorted in registers
-// (2..32 keys per lane by bucket size).
+// (2..32 keys per lane by bucket size); then buckets of 1025..2048 keys
+// (listed for k_segsort_big, which leaves them) on pairs of warps.
 constexpr int kMidNT = 256;
-__global__ void __launch_bounds__(kMidNT) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
+__global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
                                                          const uint32_t *__restrict__ big_list,
                                                          const unsigned long long *__restrict__ owner_off,
                                                          unsigned long long *__restrict__ out) {
@@ -806,9 +852,19 @@ __global__ void __launch_bounds__(kMidNT) k_segsort_mid(const DevStats *stats, u
 		else if (len <= 512) sort_bucket_reg<16>(out, beg, len, a, lane);
 		else sort_bucket_reg<32>(out, beg, len, a, lane);
 	}
+	__shared__ uint32_t xch[kMidNT / 64][kPairSeg];
+	const uint64_t nbig = min((uint64_t)stats->seg_big, big_cap);
+	const int pair = threadIdx.x >> 6, half = (threadIdx.x >> 5) & 1;
+	const uint64_t npairs = (uint64_t)gridDim.x * (kMidNT / 64);
+	for (uint64_t g = (uint64_t)blockIdx.x * (kMidNT / 64) + pair; g < nbig; g += npairs) {
+		const uint32_t a = big_list[big_cap - 1 - g];
+		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
+		if (len > kPairSeg) continue;  // the block tier's (uniform over the pair)
+		sort_bucket_pair(out, beg, len, a, half, lane, xch[pair], 1 + pair);
+	}
 }
 
-// Buckets of 1025..16384 keys: one block per bucket (grid-stride over the
+// Buckets of 2049..16384 keys: one block per bucket (grid-stride over the
 // device-side count), bitonic sort of the partner halves in 64 KB of
 // dynamic shared memory.
 __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint64_t big_cap,
@@ -821,6 +877,7 @@ __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint
 	for (uint64_t g = blockIdx.x; g < nbig; g += gridDim.x) {
 		const uint32_t a = big_list[big_cap - 1 - g];
 		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
+		if (len <= kPairSeg) continue;  // sorted by warp pairs in k_segsort_mid (uniform over the block)
 		int m = 1;
 		while ((uint64_t)m < len) m <<= 1;
 		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? (uint32_t)out[beg + i] : 0xffffffffu;
