@@ -160,7 +160,7 @@ REF_API int64_t ccref_bins(uint64_t n, float *aabb, int gx, int gy, int gz, uint
 }
 #endif
 
-/* Narrowphase::DoNarrowphase (Narrowphase.cu:511-595) in this build's `real`.
+/* Narrowphase::DoNarrowphase (Narrowphase.cu:511-595) in the `real` type this file is compiled with.
  * Inputs are float arrays converted to `real`. `pairs` (P keys) is permuted in
  * place like the reference does (Narrowphase.cu:584-588). Contact outputs
  * (norm, cpta, cptb as 3 doubles each, depth, bids as 2 int32) are written
