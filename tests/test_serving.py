@@ -27,6 +27,34 @@ def test_scene_bytes_counts_inputs_and_boxes():
     assert SV.scene_bytes(sc) == sc.nbytes() + 24 * 1000
 
 
+def test_arena_first_fit_merges_and_never_overlaps():
+    # the resident-scene arena's free list on a host buffer: random takes and
+    # gives keep the ranges aligned, disjoint, merged with free neighbours,
+    # and the free and taken bytes always add up to the arena
+    a = SV.Arena(1 << 20, "cpu")
+    rng = np.random.default_rng(0)
+    live = {}
+    for it in range(5000):
+        if live and rng.random() < 0.5:
+            k = list(live)[int(rng.integers(0, len(live)))]
+            a.give(*live.pop(k))
+        else:
+            size = int(rng.integers(1, 60_000))
+            off = a.take(size)
+            if off is not None:
+                assert off % 256 == 0
+                for o, z in live.values():
+                    assert off + SV._align(size) <= o or o + SV._align(z) <= off
+                live[it] = (off, size)
+        fr = a.free
+        assert all(fr[i][0] + fr[i][1] < fr[i + 1][0] for i in range(len(fr) - 1))
+        assert sum(z for _, z in fr) + sum(SV._align(z) for _, z in live.values()) == a.size
+    for off, size in live.values():
+        a.give(off, size)
+    assert a.free == [(0, a.size)]
+    assert a.take(a.size + 1) is None
+
+
 @pytest.mark.gpu
 def test_results_same_alone_and_in_the_mix(cb):
     pool = [S.mixed_slab(n, seed=n, extent=(1.0, 1.0, 0.1)) for n in (3000, 12000, 800, 25000)]
