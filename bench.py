@@ -172,6 +172,32 @@ def bench_clustered(cb, dev, steps=3, bodies=1 << 24):
     return out
 
 
+SMALL_WORKLOAD = ("spheres_uniform: 16,384 spheres, centres U[0,1]^3, radii U[0.002,0.006], identity orientation "
+                  "(the reference's CPU-runnable case)")
+
+
+def bench_small(cb, dev, steps=200):
+    """The 16,384-sphere scene: one cc_collide per step on device-resident
+    inputs (graph replay after the second call); launch-latency bound."""
+    import torch
+    from collide_b200 import scenes as S
+    sc = S.spheres_uniform(16384, seed=0)
+    pipe = cb.DevicePipeline(cb.DeviceScene(sc, device=dev), grid=BINS, ctx=cb.Context())
+    for _ in range(10):
+        pipe.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        pipe.run()
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / steps
+    return {"workload": SMALL_WORKLOAD, "bodies": sc.n, "pairs": pipe.n_pairs, "contacts": pipe.n_contacts,
+            "ms_per_step": t, "value": sc.n / (t / 1000.0), "unit": "bodies/s", "steps": steps,
+            "l2": "not flushed (the scene is 1.4 MB)"}
+
+
 def bench_served(cb, dev, seconds):
     """Poisson streams (2,000 and 4,000 queries/s, 70% updates / 30% new
     scenes) on device-resident scenes: continuous batching against the
@@ -569,6 +595,7 @@ def run_ours(args):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_batch:
+        line["small"] = bench_small(cb, dev)
         line["batched"] = bench_batched(cb, ctx, dev)
     if rank == 0 and world == 1 and not args.no_serve:
         line["served"] = bench_served(cb, dev, args.serve_seconds)
