@@ -377,16 +377,6 @@ def run_reference(args):
         times.append(float(t.sum()))
     ms = 1000.0 * sum(times) / len(times)
     value = scene.n / (ms / 1000.0)
-    # the broadphase as one unit: the single-pass byte model 88N + 56E + 16C + 8P
-    # (C = candidates; the home-cell test emits none twice, so C = P here) over
-    # the summed stage times from the shift/count pass to the sorted list
-    bp_stages = ("count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
-    bp_ms = sum(kern[k][0] / kern[k][1] for k in bp_stages if k in kern)
-    bp_bytes = 88 * scene.n + 56 * E + 16 * P + 8 * P
-    bp_roof = {"bound": "hbm", "stages": list(bp_stages), "ms": bp_ms,
-               "model_bytes": bp_bytes, "achieved": bp_bytes / (bp_ms / 1000.0) / 1e9, "peak": hbm, "unit": "GB/s",
-               "frac": bp_bytes / (bp_ms / 1000.0) / 1e9 / hbm,
-               "floor_bytes": 24 * scene.n + 8 * P, "pairs_per_s": P / (bp_ms / 1000.0)}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
