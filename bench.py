@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=N_BODIES, help=argparse.SUPPRESS)
+    ap.add_argument("--n", "--bodies", dest="n", type=int, default=N_BODIES, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-scene batched measurement")

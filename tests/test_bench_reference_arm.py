@@ -21,3 +21,49 @@ def test_reference_arm_prints_its_line():
     assert line["impl"] == "reference" and line["metric"] == "bodies/s" and line["value"] > 0
     assert line["e2e"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "reference"
     assert line["config"]["pairs"] > 0
+
+
+def _free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_two_ranks_under_torchrun_over_gloo():
+    # the launch the driver uses for N > 1, on the host: rank 0 prints one line,
+    # rank 1 leaves without work, both exit 0
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libccref_f32.so")):
+        pytest.skip("the reference's CPU build is absent (make -C oracle ref)")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(_free_port()), os.path.join(ROOT, "bench.py"), "--impl", "reference",
+           "--gpus", "2", "--steps", "1", "--warmup", "1", "--bodies", "20000"]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1 and json.loads(lines[0])["n_gpus"] == 2
+
+
+_MAX_OVER_RANKS = r'''
+import os, sys
+sys.path.insert(0, sys.argv[1])
+import bench
+world, rank, _ = bench.dist_setup(2)
+bench.dist_barrier(world)
+v = bench.dist_max(10.0 + rank, world)
+assert world == 2 and v == 11.0, (world, v)  # every rank sees the maximum
+if rank == 0:
+    print("max", v, flush=True)
+'''
+
+
+def test_max_over_ranks_over_gloo(tmp_path):
+    script = tmp_path / "max_over_ranks.py"
+    script.write_text(_MAX_OVER_RANKS)
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(_free_port()), str(script), ROOT]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert [ln for ln in out.stdout.splitlines() if ln.startswith("max")] == ["max 11.0"]
