@@ -30,7 +30,49 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.join(ROOT, "collision-detection_b200"))
+PKG_DIR = os.path.join(ROOT, "collision-detection_b200")
+sys.path.insert(0, PKG_DIR)
+
+
+def numpy_module(name):
+    """collide_b200/<name>.py (scenes, tuner: NumPy only) loaded by file path,
+    without running the package's __init__, which maps libcollide_b200.so.
+    The reference arm and the CPU-baseline leg use these so that the process
+    timing the reference's CPU build never loads this repository's GPU
+    library."""
+    import importlib.util
+    key = f"_bench_{name}"
+    if key not in sys.modules:
+        spec = importlib.util.spec_from_file_location(key, os.path.join(PKG_DIR, "collide_b200", f"{name}.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[key] = mod  # dataclasses look their module up while the class is built
+        spec.loader.exec_module(mod)
+    return sys.modules[key]
+
+
+def mapped_repo_libraries():
+    """Shared libraries of this repository mapped into the current process."""
+    libs = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                p = ln.split()[-1] if ln.count("/") else ""
+                if p.endswith(".so") and p.startswith(ROOT):
+                    libs.add(os.path.relpath(p, ROOT))
+    except OSError:
+        pass
+    return sorted(libs)
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 N_BODIES = 1 << 20
 WORKLOAD = ("mixed_slab: 1,048,576 convex shapes (40% sphere, 30% box, 15% ellipsoid, 15% cylinder), "
@@ -56,6 +98,12 @@ STAGE_BYTES = {
 }
 
 
+# Stages of the broadphase proper (detectPossibleCollisions after the AABBs),
+# in pipeline order; stages absent from a run are skipped.
+BP_STAGES = ("count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
+STAGE_TIERS = {"segsort": ("segsort_mid", "segsort_big")}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -73,6 +121,8 @@ def parse():
                     help="body count of the clustered-sphere measurement (profiling uses smaller cases)")
     ap.add_argument("--only-clustered", action="store_true",
                     help="run only the clustered-sphere broadphase and print its object (one GPU)")
+    ap.add_argument("--only-passes", type=int, default=0,
+                    help="profiling: run this many pipeline passes of the headline workload and exit (no timing)")
     return ap.parse_args()
 
 
@@ -234,8 +284,14 @@ def bench_served(cb, dev, seconds):
 
 
 def scene_for(rank, n):
-    from collide_b200 import scenes as S
-    return S.mixed_slab(n, seed=rank)
+    return numpy_module("scenes").mixed_slab(n, seed=rank)
+
+
+# The workload identity both arms print as `config` (rank r uses seed r).
+def workload_config(n, world):
+    return {"workload": WORKLOAD if n == N_BODIES else WORKLOAD.replace("1,048,576", f"{n:,}"), "bodies": n,
+            "seeds": "rank r draws the scene with seed r", "bins_per_axis": list(BINS),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
 # ---------------------------------------------------------------------------- clocks
@@ -339,27 +395,62 @@ def dist_barrier(world):
 
 
 # ---------------------------------------------------------------------------- reference (CPU) timing
-def reference_session(scene, threads):
+STAGE_NAMES = ("generate_aabb", "detect_possible_collisions", "do_narrowphase")
+
+
+def reference_session(scene, threads, grid=None):
+    """The reference's own CPU build (oracle/_ref) on `scene`. Its bins per
+    axis default to the search grid the GPU path picks for the scene (the
+    pair list does not depend on the grid, the reference's speed does)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from collide_b200 import tuner
-    grid = tuner.heuristic_dims(O.aabb(scene))
-    return O.RefSession(scene, grid, threads=threads, all_parallel=True), grid
+    if grid is None:
+        grid = numpy_module("tuner").heuristic_dims(O.aabb(scene))
+    return O.RefSession(scene, grid, threads=threads, all_parallel=True), tuple(int(g) for g in grid)
+
+
+def time_reference(sess, warmup, steps=None, seconds=None, max_steps=50):
+    """Per-stage seconds of `steps` runs (or of as many runs as fit in
+    `seconds`, at least 3) after `warmup` untimed ones."""
+    for _ in range(warmup):
+        sess.run()
+    rows, t0 = [], time.perf_counter()
+    while True:
+        t, P, C = sess.run()
+        rows.append(t.copy())
+        if steps is not None and len(rows) >= steps:
+            break
+        if steps is None and len(rows) >= 3 and (time.perf_counter() - t0 >= seconds or len(rows) >= max_steps):
+            break
+    return np.array(rows), P, C
+
+
+def stage_summary_cpu(rows):
+    med = np.median(rows, axis=0)
+    return {name: round(1000.0 * float(v), 4) for name, v in zip(STAGE_NAMES, med)}
 
 
 def cpu_baseline(scene, seconds):
-    """The reference's own CPU path on this host, every thread, bounded time."""
+    """The reference's own CPU path on this host, every thread, bounded time:
+    the 1M workload at the GPU's grid, and the 16,384-sphere scene at the
+    reference's default 16^3 bins (Broadphase.cu:37)."""
     sess, grid = reference_session(scene, os.cpu_count() or 1)
-    sess.run()  # warm-up
-    times, t0 = [], time.perf_counter()
-    while len(times) < 3 or (time.perf_counter() - t0 < seconds and len(times) < 50):
-        t, P, C = sess.run()
-        times.append(float(t.sum()))
-    med = statistics.median(times)
+    rows, P, C = time_reference(sess, 1, seconds=seconds)
+    med = float(np.median(rows.sum(1)))
     out = {"value": scene.n / med, "unit": UNIT, "cores": sess.threads, "kind": "reference",
-           "sample": f"full {scene.n}-shape workload, {len(times)} runs (median), grid {list(grid)}, "
-                     f"all setParallelConfiguration flags on; pairs {P}, contacts {C}"}
+           "cpu_model": cpu_model(), "nproc": os.cpu_count(),
+           "stages_ms_median": stage_summary_cpu(rows),
+           "sample": f"full {scene.n}-shape workload, {len(rows)} runs (median of the per-run stage sums), "
+                     f"bins {list(grid)}, all setParallelConfiguration flags on; pairs {P}, contacts {C}"}
     sess.close()
+    small = numpy_module("scenes").spheres_uniform(16384, seed=0)
+    ss, g16 = reference_session(small, os.cpu_count() or 1, grid=BINS)
+    rows, P, C = time_reference(ss, 3, seconds=min(2.0, seconds))
+    med = float(np.median(rows.sum(1)))
+    out["small_at_default_bins"] = {"workload": SMALL_WORKLOAD, "bins": list(g16), "value": small.n / med,
+                                    "unit": UNIT, "ms_per_step": 1000.0 * med, "runs": len(rows),
+                                    "stages_ms_median": stage_summary_cpu(rows), "pairs": P, "contacts": C}
+    ss.close()
     return out
 
 
@@ -369,23 +460,23 @@ def run_reference(args):
         return 0
     scene = scene_for(0, args.n)
     sess, grid = reference_session(scene, os.cpu_count() or 1)
-    for _ in range(args.warmup):
-        sess.run()
-    times = []
-    for _ in range(args.steps):
-        t, P, C = sess.run()
-        times.append(float(t.sum()))
-    ms = 1000.0 * sum(times) / len(times)
+    rows, P, C = time_reference(sess, args.warmup, steps=args.steps)
+    ms = 1000.0 * float(rows.sum(1).mean())
     value = scene.n / (ms / 1000.0)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "seed": 0, "grid": list(grid), "pairs": P, "contacts": C},
+        "config": workload_config(scene.n, world),
+        "result": {"pairs": P, "contacts": C, "reference_bins": list(grid)},
+        "stages_ms_mean": {k: round(1000.0 * float(v), 4) for k, v in zip(STAGE_NAMES, rows.mean(0))},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": sess.threads, "kind": "reference",
+                         "cpu_model": cpu_model(), "nproc": os.cpu_count(),
                          "sample": f"each step = one GenerateAABB + detectPossibleCollisions + DoNarrowphase "
-                                   f"on the full {scene.n}-shape scene"},
+                                   f"of the reference's own CPU/OpenMP build on the full {scene.n}-shape scene, "
+                                   f"bins {list(grid)}, every setParallelConfiguration flag on"},
+        "native_libraries": mapped_repo_libraries(),
     }
     sess.close()
     print(json.dumps(line), flush=True)
@@ -393,14 +484,62 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------- our arm
-def traffic_from_profiles(kernel):
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    try:
-        with open(p) as f:
-            d = json.load(f)
-        return d.get(kernel)
-    except (OSError, ValueError):
+def compact_cpus(cpus):
+    if not cpus:
         return None
+    cpus, out, i = sorted(cpus), [], 0
+    while i < len(cpus):
+        j = i
+        while j + 1 < len(cpus) and cpus[j + 1] == cpus[j] + 1:
+            j += 1
+        out.append(f"{cpus[i]}-{cpus[j]}" if j > i else f"{cpus[i]}")
+        i = j + 1
+    return ",".join(out)
+
+
+def h2d_rate(pinned, dev, stream):
+    """GB/s of copying the pinned tensors `pinned` to the device (best of 5)."""
+    import torch
+    dst = [torch.empty(t.shape, dtype=t.dtype, device=dev) for t in pinned]
+    nbytes = sum(t.numel() * t.element_size() for t in pinned)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for d, t in zip(dst, pinned):
+            d.copy_(t, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del dst
+    return nbytes / (best / 1000.0) / 1e9
+
+
+def profile_figures():
+    """Per-step figures of one ncu capture of this workload (DRAM bytes per
+    stage, the MPR's FP64 FLOPs and pipe use), committed under profiles/."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_figures.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def sum_traffic(prof, stages):
+    d = prof.get("dram_bytes_per_step") or {}
+    if not stages or any(k not in d for k in stages):
+        return None
+    return sum(d[k] for k in stages)
+
+
+def merge_tiers(stage):
+    """Stages that run as several launches (the bucket sort's tiers) as one."""
+    for parent, tiers in STAGE_TIERS.items():
+        for tier in tiers:
+            if tier in stage and parent in stage:
+                stage[parent] = (stage[parent][0] + stage[tier][0], stage[parent][1])
+                del stage[tier]
+    return stage
 
 
 def run_ours(args):
@@ -417,6 +556,13 @@ def run_ours(args):
     ctx = cb.Context(local)
     ds = cb.DeviceScene(scene, device=dev)
     pipe = cb.DevicePipeline(ds, grid=BINS, ctx=ctx)
+    if args.only_passes:
+        for _ in range(args.only_passes):
+            pipe.run()
+        torch.cuda.synchronize()
+        print(json.dumps({"passes": args.only_passes, "pairs": pipe.n_pairs, "contacts": pipe.n_contacts,
+                          "launches_per_pass": ctx.launches()}), flush=True)
+        return 0
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream()
 
@@ -526,13 +672,18 @@ def run_ours(args):
                         "how": "cc_collide_host, one step at a time"}}
     assert (hq.n_pairs, hq.n_contacts) == (hs.n_pairs, hs.n_contacts)
     static_ms = dist_max(f0.elapsed_time(f1) / args.steps, world)
+    e2e["host_memory"] = {"gpu_numa_node": cb.gpu_numa_node(local),
+                          "pinned_on_cpus": compact_cpus(cb.gpu_local_cpus(local)),
+                          "h2d_GBps": h2d_rate(hp.inputs, dev, stream),
+                          "how": "pinned input buffers allocated while the thread ran on the GPU's NUMA node "
+                                 "(sysfs local_cpulist); h2d_GBps = one step's input copies, best of 5"}
     e2e["static_shapes"] = {"ms_per_step": static_ms, "value": world * scene.n / (static_ms / 1000.0),
                             "h2d_bytes_per_step": hq.input_bytes(poses_only=True),
                             "d2h_bytes_per_step": hq.output_bytes(),
                             "how": "as e2e with cc_set_static_shapes on: the shape arrays were copied in the "
                                    "warm-up, every timed step copies body poses and flags in and results out"}
 
-    # ---- roofline of the dominant kernel stage
+    # ---- rooflines
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -540,46 +691,62 @@ def run_ours(args):
     except (OSError, ValueError):
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    # the bucket sort runs as three tiers (thread, warp, block): one stage here
-    stage = dict(stage)
-    for tier in ("segsort_mid", "segsort_big"):
-        if tier in stage and "segsort" in stage:
-            stage["segsort"] = (stage["segsort"][0] + stage[tier][0], stage["segsort"][1])
-            del stage[tier]
+    peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback (6650 GB/s)"
+    prof = profile_figures()
+    stage = merge_tiers(dict(stage))
     kern = {k: v for k, v in stage.items() if k in STAGE_BYTES}
-    dom = max(kern, key=lambda k: kern[k][0])
-    dom_ms = kern[dom][0] / kern[dom][1]
-    dom_bytes = STAGE_BYTES[dom](scene.n, E, G, P, C)
-    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
     stage_summary = {k: {"ms_per_launch": v[0] / v[1], "share": v[0] / sum(x[0] for x in kern.values()),
                          "algorithmic_GBps": STAGE_BYTES[k](scene.n, E, G, P, C) / (v[0] / v[1] / 1000) / 1e9}
                      for k, v in kern.items()}
+    timing = ("CUDA events around each stage on the launch stream, over a second pass of the same "
+              f"{args.steps} steps ({prof_ms / args.steps:.4f} ms/step with the events)")
 
-    # the broadphase as one unit: the single-pass byte model 88N + 56E + 16C + 8P
-    # (C = candidates; the home-cell test emits none twice, so C = P here) over
-    # the summed stage times from the shift/count pass to the sorted list
-    bp_stages = ("count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
-    bp_ms = sum(kern[k][0] / kern[k][1] for k in bp_stages if k in kern)
+    # Headline: the broadphase (detectPossibleCollisions: shift and cell count
+    # through the sorted pair list) as one unit against HBM bandwidth, with
+    # the single-pass byte model 88N + 56E + 16C + 8P (C = candidates; the
+    # home-cell test emits no pair twice, so C = P) over the summed stage times.
+    bp_present = [k for k in BP_STAGES if k in kern]
+    bp_ms = sum(kern[k][0] / kern[k][1] for k in bp_present)
     bp_bytes = 88 * scene.n + 56 * E + 16 * P + 8 * P
-    bp_roof = {"bound": "hbm", "stages": list(bp_stages), "ms": bp_ms,
-               "model_bytes": bp_bytes, "achieved": bp_bytes / (bp_ms / 1000.0) / 1e9, "peak": hbm, "unit": "GB/s",
-               "frac": bp_bytes / (bp_ms / 1000.0) / 1e9 / hbm,
-               "floor_bytes": 24 * scene.n + 8 * P, "pairs_per_s": P / (bp_ms / 1000.0)}
+    bp_traffic = sum_traffic(prof, bp_present)
+    bp_achieved = bp_bytes / (bp_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": "broadphase: " + " + ".join(bp_present), "achieved": bp_achieved,
+                "peak": hbm, "unit": "GB/s", "frac": bp_achieved / hbm, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": bp_bytes, "model": "88*N + 56*E + 16*C + 8*P bytes per step",
+                "traffic": bp_traffic, "traffic_source": prof.get("source") if bp_traffic else None,
+                "ms_per_launch": bp_ms, "floor_bytes": 24 * scene.n + 8 * P,
+                "floor_frac": (24 * scene.n + 8 * P) / (bp_ms / 1000.0) / 1e9 / hbm,
+                "pairs_per_s": P / (bp_ms / 1000.0), "timing": timing}
+
+    # The exact MPR stage is bound by FP64 dependent-chain latency, not by
+    # memory: its FP64 FLOPs per launch (ncu thread-instruction counts of the
+    # same workload: 2 x DFMA + DADD + DMUL) over its event time, against the
+    # FP64 FMA peak measured here by cc_fma_peak.
+    fp64_peak = cb.fma_peak(fp64=True)
+    fp32_peak = cb.fma_peak(fp64=False)
+    mpr = None
+    if "mpr" in kern:
+        mpr_ms = kern["mpr"][0] / kern["mpr"][1]
+        fl = (prof.get("fp64_flops_per_step") or {}).get("mpr")
+        mpr = {"bound": "fp64 dependent-chain latency", "unit": "TFLOP/s", "ms_per_launch": mpr_ms,
+               "peak": fp64_peak / 1e12, "peak_source": "measured by cc_fma_peak (FP64 FMA, this GPU, this run)",
+               "fp32_peak": fp32_peak / 1e12, "flops_per_launch": fl,
+               "achieved": fl / (mpr_ms / 1000.0) / 1e12 if fl else None,
+               "frac": fl / (mpr_ms / 1000.0) / fp64_peak if fl else None,
+               "fp64_pipe_active_pct": prof.get("mpr_fp64_pipe_active_pct"),
+               "warps_active_pct": prof.get("mpr_warps_active_pct"),
+               "traffic": sum_traffic(prof, ["mpr"]),
+               "algorithmic_bytes_per_launch": STAGE_BYTES["mpr"](scene.n, E, G, P, C), "timing": timing}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "seed": "rank", "bins_per_axis": list(BINS), "search_grid": list(dims),
-                   "entries": E, "pairs": P, "contacts": C, "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": workload_config(scene.n, world),
+        "result": {"search_grid": list(dims), "entries": E, "pairs": P, "contacts": C,
+                   "l2": "flushed between steps (256 MiB write)"},
         "e2e": e2e,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_source": peak_src,
-                     "algorithmic_bytes_per_launch": dom_bytes, "traffic": traffic_from_profiles(dom),
-                     "timing": "CUDA events around each stage on the launch stream, over a second pass of the "
-                               f"same {args.steps} steps ({prof_ms / args.steps:.4f} ms/step with the events)"},
-        "roofline_broadphase": bp_roof,
+        "roofline": roofline,
+        "roofline_mpr": mpr,
         "stages": stage_summary,
         "gpu_launches": launches,
         "clocks": clk,

@@ -43,17 +43,54 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def gpu_local_cpus(device=None):
-    """CPUs on the GPU's own NUMA node (NVML), or None if unknown. Host
-    buffers that feed the GPU belong on that node: a copy from the other
-    socket's memory crosses the inter-socket link first."""
+def _gpu_pci_dir(device):
+    pr = torch.cuda.get_device_properties(device)
+    bdf = f"{pr.pci_domain_id:04x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+    return os.path.join("/sys/bus/pci/devices", bdf)
+
+
+def _parse_cpulist(text):
+    cpus = set()
+    for part in text.strip().split(","):
+        if not part:
+            continue
+        lo, _, hi = part.partition("-")
+        cpus.update(range(int(lo), int(hi or lo) + 1))
+    return cpus
+
+
+def gpu_numa_node(device=None):
+    """NUMA node of the GPU's PCI device (sysfs), or None if unknown."""
     try:
-        import pynvml
         if device is None:
             device = torch.cuda.current_device()
+        with open(os.path.join(_gpu_pci_dir(device), "numa_node")) as f:
+            node = int(f.read().strip())
+        return node if node >= 0 else None
+    except Exception:
+        return None
+
+
+def gpu_local_cpus(device=None):
+    """CPUs on the GPU's own NUMA node, or None if unknown: the PCI device's
+    local_cpulist in sysfs (the same GPU as CUDA's device index, whatever
+    CUDA_VISIBLE_DEVICES says), else NVML. Host buffers that feed the GPU
+    belong on that node: a copy from the other socket's memory crosses the
+    inter-socket link first."""
+    if device is None:
+        device = torch.cuda.current_device()
+    try:
+        with open(os.path.join(_gpu_pci_dir(device), "local_cpulist")) as f:
+            cpus = _parse_cpulist(f.read()) & os.sched_getaffinity(0)
+        if cpus:
+            return cpus
+    except Exception:
+        pass
+    try:
+        import pynvml
         pynvml.nvmlInit()
         pr = torch.cuda.get_device_properties(device)
-        try:  # the same GPU as CUDA's device index, whatever CUDA_VISIBLE_DEVICES says
+        try:
             bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
             h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
         except Exception:
@@ -64,6 +101,16 @@ def gpu_local_cpus(device=None):
         return cpus or None
     except Exception:
         return None
+
+
+def fma_peak(fp64=True):
+    """FMA throughput of the current GPU in FLOP/s (cc_fma_peak): the
+    denominator of the exact MPR stage's roofline."""
+    v = ctypes.c_double()
+    st = lib.cc_fma_peak(int(bool(fp64)), ctypes.byref(v), _stream())
+    if st != _lib.CC_OK:
+        raise CollideError(st, "cc_fma_peak")
+    return float(v.value)
 
 
 class numa_local:

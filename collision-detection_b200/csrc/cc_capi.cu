@@ -1503,9 +1503,10 @@ cc_status cc_collide_host_wait(cc_ctx *c, cc_result *res, void *stream) {
 	NoProfile np_(c);
 	if (c->hs_inflight == 0) return set_err(c, CC_ERR_NO_RESULT, "no step in flight");
 	cc_ctx::HostSlot &h = c->hs[c->hs_oldest];
+	// a mismatched wait leaves the oldest step in flight for the right one
+	if (res != h.res) return set_err(c, CC_ERR_INVALID_ARGUMENT, "wait with a different result than the oldest submit");
 	c->hs_oldest ^= 1;
 	c->hs_inflight--;
-	if (res != h.res) return set_err(c, CC_ERR_INVALID_ARGUMENT, "wait with a different result than the oldest submit");
 	CC_CUDA(c, cudaSetDevice(c->device));
 	CC_CUDA(c, cudaEventSynchronize(h.done));
 	res->n_pairs = res->n_contacts = 0;

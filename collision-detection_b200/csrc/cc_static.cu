@@ -1,18 +1,16 @@
 // cc_broadphase_noalloc: the broadphase for callers that cannot allocate
 // device memory.
 //
-// Some callers of a collision step are not allowed to call cudaMalloc or
-// cudaFree, or to have a library do it for them: code that runs while a CUDA
-// stream capture is active (an allocation there is an error), hard real-time
-// simulation loops (cudaMalloc and cudaFree can synchronize the whole device
-// and take unbounded time), and host frameworks that hand out every byte of
-// device memory from their own pool and forbid side allocations. For them this
-// entry point takes its scratch from one file-scope device array of fixed size
-// (kScratchBytes, 16 MiB) that every GPU loading the library holds until the
-// process exits, and it calls no allocating routine: no cudaMalloc/cudaFree,
-// no pinned host memory, no library that allocates. The caller passes the
-// AABBs (shifted in place, as detectPossibleCollisions does) and the pair
-// output buffer.
+// Some callers of a collision step cannot call cudaMalloc or cudaFree, or let
+// a library do it for them: hard real-time simulation loops (cudaMalloc and
+// cudaFree can synchronize the whole device and take unbounded time), and host
+// frameworks that hand out every byte of device memory from their own pool and
+// forbid side allocations. For them this entry point takes its scratch from
+// one file-scope device array of fixed size (kScratchBytes, 16 MiB) that every
+// GPU loading the library holds until the process exits, and it calls no
+// allocating routine: no cudaMalloc/cudaFree, no pinned host memory, no
+// library that allocates. The caller passes the AABBs (shifted in place, as
+// detectPossibleCollisions does) and the pair output buffer.
 //
 // Limits: n <= CC_NOALLOC_MAX_BODIES; the search-grid entries and the pair
 // count must fit the scratch (CC_NOALLOC_MAX_ENTRIES, CC_NOALLOC_MAX_PAIRS);
@@ -20,11 +18,12 @@
 // include/collide_b200.h).
 //
 // Set-up: the first call on each device (with that device current) looks up
-// the device address of the scratch array with cudaGetSymbolAddress; make that
-// first call before any stream capture. Every call shares the one array (and
-// one host-side staging block): calls that overlap on the GPU, or come from
-// two host threads at once, race. Each call zeroes what must start at zero,
-// so stale contents from the previous call never leak into the result.
+// the device address of the scratch array with cudaGetSymbolAddress. Each call
+// waits for its stream twice, to read the entry and pair counts. Every call
+// shares the one array (and one host-side staging block), which keeps the last
+// call's contents: calls that overlap on the GPU, or come from two host
+// threads at once, race. Each call zeroes what must start at zero, so stale
+// contents from the previous call never leak into the result.
 #include <mutex>
 
 #include "../../include/collide_b200.h"

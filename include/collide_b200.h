@@ -301,12 +301,18 @@ CC_API const char *cc_stage_name(int stage);
 CC_API cc_status cc_stage_times(const cc_ctx *ctx, double *ms, uint64_t *launches, int cap);
 CC_API cc_status cc_reset_stage_times(cc_ctx *ctx);
 
+/* Roofline denominator (no reference counterpart): the FP32 (fp64 = 0) or
+ * FP64 (fp64 = 1) multiply-add throughput of the current device in FLOP/s,
+ * timed with CUDA events on `stream` over a kernel that fills every SM with
+ * independent FMA chains (best of three runs after one warm-up). */
+CC_API cc_status cc_fma_peak(int fp64, double *flop_per_s, void *stream);
+
 /* ---- broadphase without allocation ---------------------------------------
- * No counterpart in the reference: an extra entry point for callers that may
- * not allocate device memory — code running under CUDA stream capture (where
- * cudaMalloc is an error), real-time step loops (cudaMalloc/cudaFree can
- * synchronize the device and take unbounded time) and frameworks that own all
- * device memory through their own pool. Same contract as cc_broadphase (shifts
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory while they run. A real-time step loop cannot
+ * afford cudaMalloc/cudaFree, which may synchronize the whole device and take
+ * unbounded time; a framework that hands out all device memory from its own
+ * pool cannot let a library allocate behind its back. Same contract as cc_broadphase (shifts
  * `aabb` in place, writes the sorted unique pair list, *n_pairs = count), but
  * it needs no context and allocates nothing: its scratch is one fixed
  * CC_NOALLOC_SCRATCH_BYTES device array that every GPU loading the library
@@ -314,9 +320,11 @@ CC_API cc_status cc_reset_stage_times(cc_ctx *ctx);
  * CC_NOALLOC_MAX_ENTRIES, pairs <= CC_NOALLOC_MAX_PAIRS; beyond them it returns
  * CC_ERR_CAPACITY (with *n_pairs set once the count is known). pairs_cap below
  * the count also returns CC_ERR_CAPACITY; nothing is retained. The first call
- * on each device sets up the scratch address and should come before any stream
- * capture. All calls share the one scratch array: calls that overlap on the
- * GPU, or from two host threads at once, race. */
+ * on each device looks up the scratch array's device address (once per
+ * device, with that device current). The call waits for its stream twice (to
+ * read the entry and pair counts). All calls share the one scratch array, which
+ * keeps the last call's contents: calls that overlap on the GPU, or that come
+ * from two host threads at once, race. */
 #define CC_NOALLOC_MAX_BODIES 65536u
 #define CC_NOALLOC_MAX_ENTRIES (4u * CC_NOALLOC_MAX_BODIES)
 #define CC_NOALLOC_MAX_PAIRS (4u * CC_NOALLOC_MAX_BODIES)

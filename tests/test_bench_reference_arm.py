@@ -20,7 +20,21 @@ def test_reference_arm_prints_its_line():
     line = json.loads([ln for ln in out.stdout.splitlines() if ln.startswith("{")][-1])
     assert line["impl"] == "reference" and line["metric"] == "bodies/s" and line["value"] > 0
     assert line["e2e"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "reference"
-    assert line["config"]["pairs"] > 0
+    assert line["result"]["pairs"] > 0
+    assert set(line["stages_ms_mean"]) == {"generate_aabb", "detect_possible_collisions", "do_narrowphase"}
+    # the process that timed the reference's CPU build mapped none of this
+    # repository's GPU code (read from its own /proc/self/maps)
+    libs = line["native_libraries"]
+    assert "oracle/_ref/libccref_f32.so" in libs
+    assert not any("libcollide_b200" in p for p in libs), libs
+
+
+def test_both_arms_print_the_same_config():
+    # the driver compares the two arms' `config` objects
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.workload_config(1 << 20, 1)["workload"] == bench.WORKLOAD
+    assert bench.workload_config(1 << 20, 1) == bench.workload_config(1 << 20, 1)
 
 
 def _free_port():
