@@ -149,6 +149,7 @@ def bench_batched(cb, ctx, dev, steps=10):
     torch.cuda.synchronize()
     tb = e0.elapsed_time(e1) / steps
     P, C = bp.n_pairs, bp.n_contacts
+    check = check_batch_sample(bp, db, scenes)  # outside the timed region
     del bp, db
     pipes = [cb.DevicePipeline(cb.DeviceScene(s, device=dev), grid=BINS, ctx=ctx) for s in scenes]
     for p in pipes:
@@ -166,7 +167,69 @@ def bench_batched(cb, ctx, dev, steps=10):
             "ms_per_batch": tb, "value": N / (tb / 1000.0), "unit": "bodies/s",
             "per_scene_launch": {"ms": tl, "value": N / (tl / 1000.0), "unit": "bodies/s",
                                  "how": "cc_collide once per scene, in order, outputs preallocated"},
-            "speedup_vs_per_scene": tl / tb, "steps": steps}
+            "speedup_vs_per_scene": tl / tb, "steps": steps, "checked": check}
+
+
+def contact_error_stats(gk, norm, cpta, cptb, depth, ref, scale):
+    """max / p99 of the contact errors against the FP64 oracle on the pairs
+    both report: unit-normal difference, depth difference in units of the
+    largest shape size, point difference relative to the point's magnitude."""
+    rk = ref["pairs"][: ref["n"]]
+    common, gi, ri = np.intersect1d(gk, rk, return_indices=True)
+    if not len(common):
+        return None, 0, len(np.setdiff1d(gk, rk)) + len(np.setdiff1d(rk, gk))
+    nrm = np.linalg.norm(norm[gi].astype(np.float64) - ref["norm"][ri], axis=1)
+    dep = np.abs(depth[gi].astype(np.float64) - ref["depth"][ri]) / scale
+    pa = np.linalg.norm(cpta[gi].astype(np.float64) - ref["cpta"][ri], axis=1)
+    pb = np.linalg.norm(cptb[gi].astype(np.float64) - ref["cptb"][ri], axis=1)
+    mag = np.maximum(np.maximum(np.linalg.norm(ref["cpta"][ri], axis=1), np.linalg.norm(ref["cptb"][ri], axis=1)),
+                     scale)
+    return {"normal": nrm, "depth": dep, "point": np.maximum(pa, pb) / mag}, len(common), \
+        len(np.setdiff1d(gk, rk)) + len(np.setdiff1d(rk, gk))
+
+
+def check_batch_sample(bp, db, scenes, k=16, seed=12345):
+    """Checks a seeded sample of k scenes of a finished batch pass against the
+    oracle (CPU, after the timing): each scene's pair list bit for bit
+    against the oracle's broadphase of that scene alone, and the contacts
+    against the FP64 MPR oracle (max / p99 errors over the sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    so = db.shape_offsets.astype(np.int64)
+    P, C = bp.n_pairs, bp.n_contacts
+    keys = bp.pairs[:P].cpu().numpy()
+    ck = keys[:C]
+    norm, cpta, cptb = (bp.norm[:C].cpu().numpy(), bp.cpta[:C].cpu().numpy(), bp.cptb[:C].cpu().numpy())
+    depth = bp.depth[:C].cpu().numpy()
+    coff = bp.contact_offsets.astype(np.int64)
+    pick = sorted(np.random.default_rng(seed).choice(len(scenes), size=min(k, len(scenes)), replace=False).tolist())
+    errs, exact, bodies, pairs_checked, contacts_checked, set_diff = [], True, 0, 0, 0, 0
+    for s in pick:
+        sc, a0, a1 = scenes[s], so[s], so[s + 1]
+        own = keys >> 32
+        mine = keys[(own >= a0) & (own < a1)]
+        loc = np.sort(((mine >> 32) - a0) << 32 | ((mine & 0xFFFFFFFF) - a0))
+        _, p_ref = O.broadphase(O.aabb(sc), BINS)
+        exact &= bool(np.array_equal(loc, p_ref))
+        bodies += sc.n
+        pairs_checked += len(p_ref)
+        c0, c1 = coff[s], coff[s + 1]
+        gk = ((ck[c0:c1] >> 32) - a0) << 32 | ((ck[c0:c1] & 0xFFFFFFFF) - a0)
+        ref = O.narrowphase(sc, p_ref, 0.0, "f64")
+        e, ncom, diff = contact_error_stats(gk, norm[c0:c1], cpta[c0:c1], cptb[c0:c1], depth[c0:c1], ref,
+                                            float(np.max(sc.B)))
+        contacts_checked += ncom
+        set_diff += diff
+        if e:
+            errs.append(e)
+    out = {"scenes": pick, "bodies": int(bodies), "pairs_bit_exact_vs_oracle": exact, "pairs": int(pairs_checked),
+           "contacts_compared": int(contacts_checked), "contact_set_differences": int(set_diff),
+           "against": "oracle broadphase of each scene alone; FP64 MPR oracle (narrowphase exact mode)"}
+    for key in ("normal", "depth", "point"):
+        v = np.concatenate([e[key] for e in errs]) if errs else np.zeros(1)
+        out[f"{key}_err_max"] = float(v.max())
+        out[f"{key}_err_p99"] = float(np.percentile(v, 99))
+    return out
 
 
 CLUSTER_WORKLOAD = ("clustered_spheres: 16,777,216 spheres, radii log-uniform [0.0005,0.005], 90% from 64 "

@@ -72,6 +72,7 @@ SIGNATURES = {
     "cc_reset_stage_times": (I32, [P]),
     "cc_broadphase_noalloc": (I32, [U64, P, I32, I32, I32, P, U64, PU64, P]),
     "cc_fma_peak": (I32, [I32, ctypes.POINTER(ctypes.c_double), P]),
+    "cc_perturb_scenes": (I32, [P, U64, P, P, P, P, F32, F32, P]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

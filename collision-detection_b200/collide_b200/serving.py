@@ -47,6 +47,30 @@ def perturb_(ctx: Context, ds: DeviceScene, seed: int, sigma=1e-4, max_angle=1e-
                                     float(sigma), float(max_angle), _stream()), "cc_perturb_bodies")
 
 
+def perturb_many(ctx: Context, updates, sigma=1e-4, max_angle=1e-3):
+    """Time-step updates [(DeviceScene, seed), ...] in as few launches as
+    possible (cc_perturb_scenes): one per round of distinct scenes, a scene
+    updated twice going into the next round, so every scene gets its updates
+    in list order, exactly as perturb_ one at a time gives them."""
+    rounds = []
+    for ds, seed in updates:
+        for r in rounds:
+            if id(ds) not in r:
+                r[id(ds)] = (ds, seed)
+                break
+        else:
+            rounds.append({id(ds): (ds, seed)})
+    for r in rounds:
+        items = list(r.values())
+        k = len(items)
+        nb = (ctypes.c_uint64 * k)(*[ds.nb for ds, _ in items])
+        pos = (ctypes.c_void_p * k)(*[ds.pos.data_ptr() for ds, _ in items])
+        rot = (ctypes.c_void_p * k)(*[ds.rot.data_ptr() for ds, _ in items])
+        seeds = (ctypes.c_uint64 * k)(*[int(sd) & (2**64 - 1) for _, sd in items])
+        ctx.check(lib.cc_perturb_scenes(ctx.h, k, nb, pos, rot, seeds, float(sigma), float(max_angle), _stream()),
+                  "cc_perturb_scenes")
+
+
 class PinnedScene:
     """A host scene in pinned memory, uploaded without a staging copy."""
 
@@ -336,8 +360,7 @@ class Server:
                             return
                         ev, updates, uniq, scenes, live, take = job
                         pass_s.wait_event(ev)
-                        for ds, seed in updates:
-                            perturb_(self.ctx, ds, seed)
+                        perturb_many(self.ctx, updates)
                         if uniq:
                             self.batch.run(scenes)
                             co = self.batch.contact_offsets.astype(np.int64)

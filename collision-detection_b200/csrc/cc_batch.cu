@@ -218,9 +218,11 @@ __device__ __forceinline__ float2 normal2(uint64_t key) {
 
 // pos += N(0, sigma^2); rot = normalize(dq * rot), dq = (cos(a/2), u sin(a/2))
 // with u uniform on the sphere and a ~ U[0, max_angle]. Quaternions (w,x,y,z).
-__global__ void __launch_bounds__(kNT) k_perturb(uint64_t nb, float *__restrict__ pos, float *__restrict__ rot,
-                                                  uint64_t seed, float sigma, float max_angle) {
-	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < nb; i += (uint64_t)gridDim.x * kNT) {
+// Body i of a scene updated with `seed` (the random numbers are a function of
+// (seed, i) alone).
+__device__ __forceinline__ void perturb_one(float *__restrict__ pos, float *__restrict__ rot, uint64_t i,
+                                            uint64_t seed, float sigma, float max_angle) {
+	{
 		const uint64_t key = mix64(seed) + 8 * i;
 		const float2 n01 = normal2(key), n23 = normal2(key + 1), n45 = normal2(key + 2);
 		pos[3 * i] += sigma * n01.x;
@@ -247,7 +249,37 @@ __global__ void __launch_bounds__(kNT) k_perturb(uint64_t nb, float *__restrict_
 		reinterpret_cast<float4 *>(rot)[i] = make_float4(r.x / rl, r.y / rl, r.z / rl, r.w / rl);
 	}
 }
+
+__global__ void __launch_bounds__(kNT) k_perturb(uint64_t nb, float *__restrict__ pos, float *__restrict__ rot,
+                                                  uint64_t seed, float sigma, float max_angle) {
+	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < nb; i += (uint64_t)gridDim.x * kNT)
+		perturb_one(pos, rot, i, seed, sigma, max_angle);
+}
+
+// Several scenes in one launch: the bodies of all scenes as one index range,
+// scene k owning [d[k].first, d[k].first + d[k].nb) (found by binary search).
+__global__ void __launch_bounds__(kNT) k_perturb_scenes(uint32_t count, uint64_t total,
+                                                         const PerturbScene *__restrict__ d, float sigma,
+                                                         float max_angle) {
+	for (uint64_t g = (uint64_t)blockIdx.x * kNT + threadIdx.x; g < total; g += (uint64_t)gridDim.x * kNT) {
+		uint32_t lo = 0, hi = count;  // last scene with first <= g
+		while (hi - lo > 1) {
+			const uint32_t mid = (lo + hi) >> 1;
+			if (d[mid].first <= g) lo = mid;
+			else hi = mid;
+		}
+		const PerturbScene sc = d[lo];
+		perturb_one(sc.pos, sc.rot, g - sc.first, sc.seed, sigma, max_angle);
+	}
+}
 }  // namespace
+
+void launch_perturb_scenes(uint32_t count, uint64_t total, const PerturbScene *d, float sigma, float max_angle,
+                           cudaStream_t s) {
+	if (!count || !total) return;
+	const unsigned g = (unsigned)std::min<uint64_t>((total + kNT - 1) / kNT, (uint64_t)kNumSMs * 16);
+	k_perturb_scenes<<<g, kNT, 0, s>>>(count, total, d, sigma, max_angle);
+}
 
 void launch_perturb(uint64_t nb, float *pos, float *rot, uint64_t seed, float sigma, float max_angle, cudaStream_t s) {
 	if (!nb) return;

@@ -172,7 +172,7 @@ __device__ __forceinline__ uint32_t cell_index(const Plan &p, uint32_t base, int
 template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, const DevStats *stats,
                                                 uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count,
-                                                SceneMap sm) {
+                                                SceneMap sm, int oshift) {
 	__shared__ Plan sp;
 	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
 	if (threadIdx.x < sizeof(Plan) / 4)
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
 	const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
 	const float *hs = stage + 3 * kNT;
 	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
-	owner_count[i] = 0u;
+	if ((i & ((1ull << oshift) - 1)) == 0) owner_count[i >> oshift] = 0u;  // the first body of its owner bucket
 	uint32_t base;
 	const Plan &p = plan_of<kBatch>(sp, sm, i, base);
 	if (kBatch && !p.valid) return;
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
                                                     unsigned long long *__restrict__ pairs, uint64_t pair_cap,
                                                     unsigned long long *pair_counter, SceneMap sm, uint2 *dense,
                                                     uint64_t dense_cap, unsigned long long *dense_count,
-                                                    uint32_t *err, uint32_t dense_cell) {
+                                                    uint32_t *err, uint32_t dense_cell, int oshift) {
 	__shared__ Plan sp;
 	__shared__ float4 win_all[kNT / 32][2 * kWin];
 	__shared__ unsigned long long out_all[kNT / 32][kOutBuf];
@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 				}
 				if (emit) {
 					obuf[ocnt + __popc(b & lt)] = key;
-					if (other_owner != 0xffffffffu) atomicAdd(&owner_count[other_owner], 1u);
+					if (other_owner != 0xffffffffu) atomicAdd(&owner_count[other_owner >> oshift], 1u);
 				}
 				ocnt += nb;
 				__syncwarp();
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 		}
 		__syncwarp();
 		const uint32_t owned = owned_s[threadIdx.x];
-		if (owned) atomicAdd(&owner_count[ida], owned);
+		if (owned) atomicAdd(&owner_count[ida >> oshift], owned);
 	}
 	if (ocnt) flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);
 }
@@ -532,7 +532,8 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
                                                           uint32_t *__restrict__ owner_count,
                                                           unsigned long long *__restrict__ pairs, uint64_t pair_cap,
                                                           unsigned long long *pair_counter, SceneMap sm,
-                                                          const uint2 *__restrict__ dense, uint64_t dense_cap) {
+                                                          const uint2 *__restrict__ dense, uint64_t dense_cap,
+                                                          int oshift) {
 	__shared__ Plan sp;
 	__shared__ float4 tlo[kNT], thi[kNT];
 	__shared__ uint32_t colown[kNT], tcode[kNT];
@@ -613,20 +614,21 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
 			}
 			__syncthreads();  // column counts complete
 			if (threadIdx.x < nt && colown[threadIdx.x])
-				atomicAdd(&owner_count[__float_as_uint(tlo[threadIdx.x].w)], colown[threadIdx.x]);
+				atomicAdd(&owner_count[__float_as_uint(tlo[threadIdx.x].w) >> oshift], colown[threadIdx.x]);
 		}
-		if (owned) atomicAdd(&owner_count[ida], owned);
+		if (owned) atomicAdd(&owner_count[ida >> oshift], owned);
 	}
 	if (ocnt) flush_pairs(obuf, ocnt, lane, pair_counter, pairs, pair_cap);
 }
 
-// Bucket the unsorted pairs by owner (the smaller index). P comes from the
-// device; if it exceeds the scratch or the output nothing is written.
+// Bucket the unsorted pairs by owner bucket (the smaller index >> oshift). P
+// comes from the device; if it exceeds the scratch or the output nothing is
+// written.
 __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t pair_cap, uint64_t out_cap,
                                                         const unsigned long long *__restrict__ tmp,
                                                         const unsigned long long *__restrict__ owner_off,
                                                         uint32_t *__restrict__ owner_count,
-                                                        unsigned long long *__restrict__ out) {
+                                                        unsigned long long *__restrict__ out, int oshift) {
 	const unsigned long long P = stats->pairs;
 	const bool fits = P <= pair_cap && P <= out_cap;
 	if (blockIdx.x == 0 && threadIdx.x == 0) stats->np_n = fits ? P : 0ull;
@@ -639,7 +641,7 @@ __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t
 		const uint64_t t = t0 + lane;
 		const bool valid = t < P;
 		const unsigned long long key = valid ? tmp[t] : 0ull;
-		const uint32_t a = valid ? (uint32_t)(key >> 32) : 0xffffffffu;
+		const uint32_t a = valid ? (uint32_t)(key >> 32) >> oshift : 0xffffffffu;
 		const uint32_t peers = __match_any_sync(0xffffffffu, a);
 		const int leader = __ffs(peers) - 1;
 		uint32_t base = 0;
@@ -649,14 +651,32 @@ __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t
 	}
 }
 
+// Sort keys inside an owner bucket: 32-bit packings of the 64-bit pair keys
+// that order like them (the bucket fixes the high bits of the owner).
+struct KeyPack {
+	int shift, kb;  // BpBuffers::owner_shift, key_bits
+};
+__device__ __forceinline__ uint32_t pack_key(unsigned long long key, KeyPack kp) {
+	const uint32_t b = (uint32_t)key;
+	if (!kp.shift) return b;
+	const uint32_t alo = (uint32_t)(key >> 32) & ((1u << kp.shift) - 1u);
+	return (alo << kp.kb) | b;
+}
+__device__ __forceinline__ unsigned long long unpack_key(uint32_t v, uint32_t bucket, KeyPack kp) {
+	if (!kp.shift) return ((unsigned long long)bucket << 32) | v;
+	const uint32_t a = (bucket << kp.shift) | (v >> kp.kb);
+	return ((unsigned long long)a << 32) | (v & ((1u << kp.kb) - 1u));
+}
+
 constexpr int kSmallSeg = 32;
 constexpr int kMidSeg = 1024;
 constexpr int kBigSeg = 16384;
 
-// Sorts each owner bucket (all keys share the owner in the high half):
-// <= 32 keys by one thread in place; longer buckets are listed for
-// k_segsort_mid (<= 1024 keys, from the front of big_list) or k_segsort_big
-// (<= 16384, from the back).
+// Sorts each owner bucket (all keys share the bucket's owners, n here is the
+// bucket count): <= 32 keys by one thread in place on the 64-bit keys; longer
+// buckets are listed for k_segsort_mid (<= 1024 keys, from the front of
+// big_list) or k_segsort_big (<= 16384, from the back), which sort the packed
+// 32-bit keys (pack_key).
 __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long long *__restrict__ owner_off,
                                                   unsigned long long *__restrict__ out, uint32_t *big_list,
                                                   uint64_t big_cap, DevStats *stats) {
@@ -774,19 +794,18 @@ __device__ __forceinline__ void bitonic_reg(uint32_t (&v)[K], int lane) {
 // sorts last), sorted, written back with the owner in the high half.
 template <int K>
 __device__ __forceinline__ void sort_bucket_reg(unsigned long long *__restrict__ out, uint64_t beg, uint64_t len,
-                                                uint32_t a, int lane) {
+                                                uint32_t a, int lane, KeyPack kp) {
 	uint32_t v[K];
 #pragma unroll
 	for (int r = 0; r < K; r++) {
 		const uint64_t e = 32u * r + lane;
-		v[r] = e < len ? (uint32_t)out[beg + e] : 0xffffffffu;
+		v[r] = e < len ? pack_key(out[beg + e], kp) : 0xffffffffu;
 	}
 	bitonic_reg<K>(v, lane);
-	const unsigned long long hi = (unsigned long long)a << 32;
 #pragma unroll
 	for (int r = 0; r < K; r++) {
 		const uint64_t e = 32u * r + lane;
-		if (e < len) out[beg + e] = hi | v[r];
+		if (e < len) out[beg + e] = unpack_key(v[r], a, kp);
 	}
 }
 
@@ -797,13 +816,13 @@ __device__ __forceinline__ void sort_bucket_reg(unsigned long long *__restrict__
 constexpr int kPairSeg = 2048;
 __device__ __forceinline__ void pair_sync(int bar) { asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory"); }
 __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict__ out, uint64_t beg, uint64_t len,
-                                                 uint32_t a, int half, int lane, uint32_t *x, int bar) {
+                                                 uint32_t a, int half, int lane, uint32_t *x, int bar, KeyPack kp) {
 	const int el = half * 1024 + lane;
 	uint32_t v[32];
 #pragma unroll
 	for (int r = 0; r < 32; r++) {
 		const uint64_t e = (uint64_t)el + 32u * r;
-		v[r] = e < len ? (uint32_t)out[beg + e] : 0xffffffffu;
+		v[r] = e < len ? pack_key(out[beg + e], kp) : 0xffffffffu;
 	}
 	for (int k = 2; k <= kPairSeg; k <<= 1)
 		for (int j = k >> 1; j > 0; j >>= 1) {
@@ -823,11 +842,10 @@ __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict_
 				bitonic_warp_step<32>(v, el, j, k);
 			}
 		}
-	const unsigned long long hi = (unsigned long long)a << 32;
 #pragma unroll
 	for (int r = 0; r < 32; r++) {
 		const uint64_t e = (uint64_t)el + 32u * r;
-		if (e < len) out[beg + e] = hi | v[r];
+		if (e < len) out[beg + e] = unpack_key(v[r], a, kp);
 	}
 }
 
@@ -838,7 +856,7 @@ constexpr int kMidNT = 256;
 __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
                                                          const uint32_t *__restrict__ big_list,
                                                          const unsigned long long *__restrict__ owner_off,
-                                                         unsigned long long *__restrict__ out) {
+                                                         unsigned long long *__restrict__ out, KeyPack kp) {
 	if (stats->np_n != stats->pairs) return;
 	const uint64_t nmid = min((uint64_t)stats->big_segments, big_cap);
 	const int lane = threadIdx.x & 31;
@@ -846,11 +864,11 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
 	for (uint64_t g = (uint64_t)blockIdx.x * (kMidNT / 32) + (threadIdx.x >> 5); g < nmid; g += warps) {
 		const uint32_t a = big_list[g];
 		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;  // 33..1024, listed by k_segsort
-		if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane);
-		else if (len <= 128) sort_bucket_reg<4>(out, beg, len, a, lane);
-		else if (len <= 256) sort_bucket_reg<8>(out, beg, len, a, lane);
-		else if (len <= 512) sort_bucket_reg<16>(out, beg, len, a, lane);
-		else sort_bucket_reg<32>(out, beg, len, a, lane);
+		if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane, kp);
+		else if (len <= 128) sort_bucket_reg<4>(out, beg, len, a, lane, kp);
+		else if (len <= 256) sort_bucket_reg<8>(out, beg, len, a, lane, kp);
+		else if (len <= 512) sort_bucket_reg<16>(out, beg, len, a, lane, kp);
+		else sort_bucket_reg<32>(out, beg, len, a, lane, kp);
 	}
 	__shared__ uint32_t xch[kMidNT / 64][kPairSeg];
 	const uint64_t nbig = min((uint64_t)stats->seg_big, big_cap);
@@ -860,7 +878,7 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
 		const uint32_t a = big_list[big_cap - 1 - g];
 		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
 		if (len > kPairSeg) continue;  // the block tier's (uniform over the pair)
-		sort_bucket_pair(out, beg, len, a, half, lane, xch[pair], 1 + pair);
+		sort_bucket_pair(out, beg, len, a, half, lane, xch[pair], 1 + pair, kp);
 	}
 }
 
@@ -870,7 +888,7 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
 __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint64_t big_cap,
                                                       const uint32_t *__restrict__ big_list,
                                                       const unsigned long long *__restrict__ owner_off,
-                                                      unsigned long long *__restrict__ out) {
+                                                      unsigned long long *__restrict__ out, KeyPack kp) {
 	extern __shared__ uint32_t s[];
 	if (stats->np_n != stats->pairs) return;
 	const uint64_t nbig = min((uint64_t)stats->seg_big, big_cap);
@@ -880,11 +898,10 @@ __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint
 		if (len <= kPairSeg) continue;  // sorted by warp pairs in k_segsort_mid (uniform over the block)
 		int m = 1;
 		while ((uint64_t)m < len) m <<= 1;
-		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? (uint32_t)out[beg + i] : 0xffffffffu;
+		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? pack_key(out[beg + i], kp) : 0xffffffffu;
 		__syncthreads();
 		bitonic_u32(s, m, threadIdx.x, blockDim.x, [] { __syncthreads(); });
-		const unsigned long long hi = (unsigned long long)a << 32;
-		for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = hi | s[i];
+		for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = unpack_key(s[i], a, kp);
 		__syncthreads();
 	}
 }
@@ -996,9 +1013,10 @@ void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridPar
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
 	if (!n) return;
 	if (b.sm.plans)
-		k_count<true><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm);
+		k_count<true><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm, 0);
 	else
-		k_count<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm);
+		k_count<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm,
+		                                             b.owner_shift);
 }
 
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
@@ -1024,11 +1042,11 @@ void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cud
 	if (b.sm.plans)
 		k_pair_test<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                       b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
-		                                       &b.stats->dense_items, &b.stats->err, b.dense_cell);
+		                                       &b.stats->dense_items, &b.stats->err, b.dense_cell, b.owner_shift);
 	else
 		k_pair_test<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                        b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
-		                                        &b.stats->dense_items, &b.stats->err, b.dense_cell);
+		                                        &b.stats->dense_items, &b.stats->err, b.dense_cell, b.owner_shift);
 	launch_pair_test_dense(b, s);
 }
 
@@ -1059,30 +1077,33 @@ void launch_pair_test_dense(const BpBuffers &b, cudaStream_t s) {
 	if (b.sm.plans)
 		k_pair_test_dense<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                             b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
-		                                             b.dense_cap);
+		                                             b.dense_cap, b.owner_shift);
 	else
 		k_pair_test_dense<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                              b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
-		                                              b.dense_cap);
+		                                              b.dense_cap, b.owner_shift);
 }
 
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s) {
-	launch_scan_u32_to_u64(b.owner_count, n, b.owner_off, b.status2 ? b.status2 : b.status,
+	launch_scan_u32_to_u64(b.owner_count, owner_buckets(n, b.owner_shift), b.owner_off, b.status2 ? b.status2 : b.status,
 	                       b.ticket2 ? b.ticket2 : b.ticket, &b.stats->err, s, nullptr, nullptr, b.pre_zeroed);
 }
 
 void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
 	const uint64_t bound = std::min<uint64_t>(b.pair_cap, out_cap);
 	const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(blocks_for(bound), 1), (uint64_t)kNumSMs * 8);
-	k_owner_scatter<<<grid, kNT, 0, s>>>(b.stats, b.pair_cap, out_cap, b.pairs_tmp, b.owner_off, b.owner_count, out);
+	k_owner_scatter<<<grid, kNT, 0, s>>>(b.stats, b.pair_cap, out_cap, b.pairs_tmp, b.owner_off, b.owner_count, out,
+	                                     b.owner_shift);
 }
 
 void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
-	k_segsort<<<blocks_for(n), kNT, 0, s>>>(n, b.owner_off, out, b.big_list, b.big_cap, b.stats);
+	const uint64_t nbk = owner_buckets(n, b.owner_shift);
+	k_segsort<<<blocks_for(nbk), kNT, 0, s>>>(nbk, b.owner_off, out, b.big_list, b.big_cap, b.stats);
 }
 
 void launch_segsort_mid(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
-	k_segsort_mid<<<kNumSMs * 6, kMidNT, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out);
+	k_segsort_mid<<<kNumSMs * 6, kMidNT, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out,
+	                                             KeyPack{b.owner_shift, b.key_bits});
 }
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
 	static const bool attr = [] {
@@ -1092,7 +1113,7 @@ void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_
 	(void)attr;
 	// 64 KB of shared memory a block: three blocks fit on an SM
 	k_segsort_big<<<kNumSMs * 3, 512, kBigSeg * sizeof(uint32_t), s>>>(b.stats, b.big_cap, b.big_list, b.owner_off,
-	                                                                   out);
+	                                                                   out, KeyPack{b.owner_shift, b.key_bits});
 }
 
 void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s) {

@@ -3,6 +3,7 @@
 // here; every device pass is a launcher from cc_aabb.cu, cc_broadphase.cu,
 // cc_narrowphase.cu or cc_sort.cu.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -51,6 +52,8 @@ struct cc_ctx {
 	// batch scratch: offsets, scene of each shape, global body ids, per-scene
 	// stats and plans, scene cell counts and bases, G-scan control, results
 	Buf b_off, b_scene_of, b_gid, b_sst, b_plans, b_G, b_base, b_status, b_ticket, b_res;
+	// descriptor table of cc_perturb_scenes
+	Buf pt_desc;
 	// gather arena of cc_collide_scenes
 	Buf g_T, g_A, g_B, g_C, g_R, g_ID, g_pos, g_rot, g_act, g_src, g_off;
 	SceneMap sm;  // set while a batch call runs
@@ -61,6 +64,9 @@ struct cc_ctx {
 	uint64_t retained_n = 0, retained_P = 0;
 	uint64_t last_E = 0, last_P = 0;
 	int last_dim[3] = {0, 0, 0};
+	// owner buckets of the pair sort (BpBuffers::owner_shift / key_bits), chosen
+	// per call from the last call's pairs per body
+	int owner_shift = 0, key_bits = 32;
 	uint64_t launches = 0;
 	int np_precision = CC_NP_EXACT;
 	// scratch generation: bumped whenever ensure() moves a buffer
@@ -275,7 +281,28 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.dense = ptr<uint2>(c->dense);
 	b.dense_cap = c->dense.bytes / sizeof(uint2);
 	b.dense_cell = c->gp.dense_cell;
+	b.owner_shift = c->owner_shift;
+	b.key_bits = c->key_bits;
 	return b;
+}
+
+// Owner buckets of the pair sort for n bodies: about 8 pairs per bucket at the
+// last call's pair count (n / 4 before any), so that the bucket scan and the
+// per-bucket sorts touch ~P/8 buckets instead of n owners. A sparse scene
+// (1M mixed shapes, 0.026 pairs per body) gets 2^8 owners per bucket, a dense
+// one (hundreds of pairs per body) one owner per bucket. The shift moves only
+// when the ideal differs by two or more, so a captured graph stays valid while
+// the pair count drifts. The packed in-bucket keys need shift + bits(n - 1) <= 32.
+void choose_owner_shift(cc_ctx *c, uint64_t n) {
+	int kb = 1;
+	while (kb < 32 && ((uint64_t)1 << kb) < n) kb++;
+	const double P = (double)std::max<uint64_t>(c->last_P ? c->last_P : n / 4, 1);
+	int ideal = (int)std::floor(std::log2(8.0 * (double)std::max<uint64_t>(n, 1) / P));
+	ideal = std::max(0, std::min(ideal, std::min(16, 32 - kb)));
+	int cur = std::min(c->owner_shift, 32 - kb);
+	if (std::abs(ideal - cur) >= 2 || c->key_bits != kb) cur = ideal;
+	c->owner_shift = n < 2 ? 0 : cur;
+	c->key_bits = kb;
 }
 
 // Words of a look-back status region for a scan over n elements (rounded to
@@ -310,6 +337,12 @@ cc_status np_prepare(cc_ctx *c, uint64_t P) {
 // ends with a synchronize, so nothing in flight uses a buffer replaced here.
 cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 0) {
 	c->gp.g_max = g_override ? (uint32_t)g_override : g_max_for(n);
+	if (g_override) {  // a batch: its per-scene pair counts are read at scene boundaries of the owner offsets
+		c->owner_shift = 0;
+		c->key_bits = 32;
+	} else {
+		choose_owner_shift(c, n);
+	}
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
 	CC_TRY(ensure(c, c->cell_count, sizeof(uint32_t) * c->gp.g_max));
 	CC_TRY(ensure(c, c->cell_start, sizeof(uint32_t) * (c->gp.g_max + 1)));
@@ -636,7 +669,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 		struct {
 			uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
 			const void *p[18];
-			int dims[3], prec;
+			int dims[3], prec, oshift, kbits;
 			float env;
 			GridParams gp;
 		} k;
@@ -648,6 +681,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 		                      pairs, norm, cpta, cptb, depth, bids, nullptr, nullptr};
 		memcpy(k.p, ps, sizeof(ps));
 		k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.env = envelope; k.gp = c->gp;
+		k.oshift = c->owner_shift; k.kbits = c->key_bits;
 		static_assert(sizeof(k) <= sizeof(c->gkey), "graph key");
 		if (c->gexec && memcmp(&k, c->gkey, sizeof(k)) == 0) {
 			replayed = true;
@@ -1224,9 +1258,25 @@ cc_status batch_impl(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, floa
 	enqueue_emit(c, n, out, pairs_cap, s);
 	enqueue_np(c, a, pairs_cap, &d->np_n, s);
 	c->pass_zeroed = false;
+	// per-scene pair counts and contact offsets go back behind the pass, so
+	// the common case synchronizes once (redone below if the pass is redone)
+	const bool want_offsets = scene_pairs || contact_offsets;
+	auto copy_offsets = [&]() -> cc_status {
+		launch_batch_offsets((uint32_t)S, d_shape, ptr<unsigned long long>(c->owner_off),
+		                     ptr<unsigned long long>(c->np_pos), d, d_pairs_s, d_coff, s);
+		CC_TRY(check_launch(c));
+		if (scene_pairs)
+			CC_CUDA(c, cudaMemcpyAsync(scene_pairs, d_pairs_s, sizeof(uint64_t) * S, cudaMemcpyDeviceToHost, s));
+		if (contact_offsets)
+			CC_CUDA(c, cudaMemcpyAsync(contact_offsets, d_coff, sizeof(uint64_t) * (S + 1), cudaMemcpyDeviceToHost, s));
+		return CC_OK;
+	};
+	if (want_offsets) CC_TRY(copy_offsets());
 	CC_TRY(check_launch(c));
 	CC_TRY(read_stats(c, s));
 	CC_TRY(device_err(c));
+	bool redone = c->h_stats->entries > c->entries.bytes / (2 * sizeof(float4)) ||
+	              c->h_stats->pairs > c->pairs_tmp.bytes / sizeof(unsigned long long);
 	CC_TRY(settle(c, n, res->aabb, out, pairs_cap, &a, s));
 	remember(c);
 	const uint64_t P = c->h_stats->pairs;
@@ -1240,18 +1290,13 @@ cc_status batch_impl(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, floa
 		enqueue_np(c, a, pairs_cap, &d->np_n, s);
 		CC_TRY(check_launch(c));
 		CC_TRY(read_stats(c, s));
+		redone = true;
 	}
 	if (c->h_stats->err & kErrBadIndex)
 		return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is outside its scene");
 	res->n_contacts = c->h_stats->contacts;
-	if (scene_pairs || contact_offsets) {
-		launch_batch_offsets((uint32_t)S, d_shape, ptr<unsigned long long>(c->owner_off),
-		                     ptr<unsigned long long>(c->np_pos), d, d_pairs_s, d_coff, s);
-		CC_TRY(check_launch(c));
-		if (scene_pairs)
-			CC_CUDA(c, cudaMemcpyAsync(scene_pairs, d_pairs_s, sizeof(uint64_t) * S, cudaMemcpyDeviceToHost, s));
-		if (contact_offsets)
-			CC_CUDA(c, cudaMemcpyAsync(contact_offsets, d_coff, sizeof(uint64_t) * (S + 1), cudaMemcpyDeviceToHost, s));
+	if (want_offsets && redone) {
+		CC_TRY(copy_offsets());
 		CC_CUDA(c, cudaStreamSynchronize(s));
 	}
 	return CC_OK;
@@ -1329,6 +1374,36 @@ cc_status cc_perturb_bodies(cc_ctx *c, uint64_t nb, float *body_pos, float *body
 	if (!aligned16(body_rot)) return set_err(c, CC_ERR_INVALID_ARGUMENT, "body_rot must be 16-byte aligned");
 	CC_CUDA(c, cudaSetDevice(c->device));
 	launch_perturb(nb, body_pos, body_rot, seed, sigma, max_angle, (cudaStream_t)stream);
+	return check_launch(c);
+}
+
+cc_status cc_perturb_scenes(cc_ctx *c, uint64_t count, const uint64_t *nb, float *const *body_pos,
+                            float *const *body_rot, const uint64_t *seeds, float sigma, float max_angle, void *stream) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	if (count == 0) return CC_OK;
+	if (!nb || !body_pos || !body_rot || !seeds) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null argument array");
+	if (count >= 0xffffffffull) return set_err(c, CC_ERR_INVALID_ARGUMENT, "too many scenes");
+	std::vector<PerturbScene> d;
+	d.reserve(count);
+	uint64_t total = 0;
+	for (uint64_t k = 0; k < count; k++) {
+		if (nb[k] == 0) continue;
+		if (!body_pos[k] || !body_rot[k])
+			return set_err(c, CC_ERR_INVALID_ARGUMENT, "scene %llu: null body arrays", (unsigned long long)k);
+		if (!aligned16(body_rot[k]))
+			return set_err(c, CC_ERR_INVALID_ARGUMENT, "scene %llu: body_rot must be 16-byte aligned",
+			               (unsigned long long)k);
+		d.push_back(PerturbScene{body_pos[k], body_rot[k], nb[k], total, seeds[k]});
+		total += nb[k];
+	}
+	if (d.empty()) return CC_OK;
+	CC_CUDA(c, cudaSetDevice(c->device));
+	cudaStream_t s = (cudaStream_t)stream;
+	CC_TRY(ensure(c, c->pt_desc, sizeof(PerturbScene) * d.size()));
+	// the descriptor table is staged by the copy itself (pageable source): the
+	// host vector may go away once the call returns
+	CC_CUDA(c, cudaMemcpyAsync(c->pt_desc.p, d.data(), sizeof(PerturbScene) * d.size(), cudaMemcpyHostToDevice, s));
+	launch_perturb_scenes((uint32_t)d.size(), total, ptr<PerturbScene>(c->pt_desc), sigma, max_angle, s);
 	return check_launch(c);
 }
 

@@ -146,7 +146,18 @@ struct BpBuffers {
 	uint2 *dense = nullptr;       // dense-cell work items (cell, first row)
 	uint64_t dense_cap = 0;
 	uint32_t dense_cell = 128;    // threshold (entries) of a dense cell
+	// Pairs are bucketed by owner (the smaller index a) coarsened to a >> owner_shift:
+	// ceil(n / 2^owner_shift) buckets. Inside a bucket the sort keys are packed to
+	// 32 bits as ((a mod 2^owner_shift) << key_bits) | b, with key_bits the bits of
+	// n - 1 (owner_shift + key_bits <= 32). owner_shift 0: one bucket per body, keys
+	// are the partner halves b (batches, incremental steps, the clustered scenes).
+	int owner_shift = 0;
+	int key_bits = 32;
 };
+// Owner buckets of n bodies at a shift.
+__host__ __device__ inline uint64_t owner_buckets(uint64_t n, int shift) {
+	return n ? ((n - 1) >> shift) + 1 : 0;
+}
 
 // Bounds pass over caller AABBs; its last block writes stats->plan.
 void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridParams &gp, const int grid[3],
@@ -215,6 +226,14 @@ struct SceneDst {
 	uint8_t *active;
 };
 void launch_perturb(uint64_t nb, float *pos, float *rot, uint64_t seed, float sigma, float max_angle, cudaStream_t s);
+// One scene of a multi-scene update: its bodies are [first, first + nb) of the
+// launch's body range (scenes in order, first[0] = 0).
+struct PerturbScene {
+	float *pos, *rot;
+	uint64_t nb, first, seed;
+};
+void launch_perturb_scenes(uint32_t count, uint64_t total, const PerturbScene *d, float sigma, float max_angle,
+                           cudaStream_t s);
 void launch_gather(uint64_t n, uint64_t nb, uint32_t S, const unsigned long long *shape_off,
                    const unsigned long long *body_off, const SceneSrc *src, const SceneDst &dst, cudaStream_t s);
 void launch_batch_prep(uint64_t n, uint32_t S, const unsigned long long *shape_off, const unsigned long long *body_off,

@@ -253,6 +253,17 @@ CC_API cc_status cc_collide_scenes(cc_ctx *ctx, uint64_t num_scenes, const cc_sc
 CC_API cc_status cc_perturb_bodies(cc_ctx *ctx, uint64_t nb, float *body_pos, float *body_rot, uint64_t seed,
                                    float sigma, float max_angle, void *stream);
 
+/* The updates of `count` scenes in one launch (a serving pass's time-step
+ * queries): scene k's nb[k] bodies at the device arrays body_pos[k] and
+ * body_rot[k] move exactly as cc_perturb_bodies(ctx, nb[k], body_pos[k],
+ * body_rot[k], seeds[k], sigma, max_angle) moves them. The four argument
+ * arrays are host memory and may be reused once the call returns. Entries
+ * are applied concurrently, so their body ranges must not overlap: a scene
+ * updated twice takes two calls. No reference counterpart. */
+CC_API cc_status cc_perturb_scenes(cc_ctx *ctx, uint64_t count, const uint64_t *nb, float *const *body_pos,
+                                   float *const *body_rot, const uint64_t *seeds, float sigma, float max_angle,
+                                   void *stream);
+
 /* Same with HOST pointers in `scene` and `res` (pinned memory recommended):
  * the inputs are copied to context-owned device buffers, the pipeline runs,
  * and aabb (if non-NULL), pairs and contacts are copied back. */

@@ -325,3 +325,24 @@ def test_repeated_calls_are_deterministic(cb):
         if first is None:
             first = p
         assert np.array_equal(p, first)
+
+
+def test_owner_buckets_follow_the_pair_density(cb):
+    # One context, one body count, scenes of rising density: each call buckets
+    # pair owners by the previous call's pairs per body, so the dense calls
+    # meet buckets of hundreds to thousands of keys sorted on packed 32-bit
+    # keys (warp, warp-pair and block tiers) before the bucket size adapts.
+    ctx = cb.Context()
+    n = 65536
+    rng = np.random.default_rng(11)
+    # (pairs per body 0.001 .. 7.4): with 4,096 owners per bucket after a
+    # sparse call, the 0.0056 scene fills warp, warp-pair and block tiers,
+    # 0.008 the block tier, and 0.0155 exceeds 16,384 keys in a bucket (the
+    # whole-list sort takes over)
+    for half in (0.0008, 0.0008, 0.0056, 0.0008, 0.0008, 0.008, 0.0008, 0.0008, 0.0155, 0.0008):
+        lo = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
+        a = np.ascontiguousarray(np.concatenate([lo, lo + np.float32(2 * half)]).astype(np.float32))
+        sh, p = gpu_broadphase(cb, a, (16, 16, 16), ctx=ctx)
+        sh_ref, p_ref = O.broadphase(a, (16, 16, 16))
+        assert same_bits(sh, sh_ref)
+        assert np.array_equal(p, p_ref), (half, len(p), len(p_ref), pair_set_diff(p, p_ref))

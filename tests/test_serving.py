@@ -123,3 +123,22 @@ def test_serve_short_stream(cb, mode):
     assert r["queries"] == len(st.queries) > 20
     assert all(np.isfinite(q.done) and q.done >= q.arrival for q in st.queries)
     assert r["p99_ms"] >= r["p50_ms"] > 0
+
+
+@pytest.mark.gpu
+def test_batched_updates_equal_one_at_a_time(cb):
+    # cc_perturb_scenes (one launch per round of distinct scenes) moves every
+    # body exactly as cc_perturb_bodies per update, in order, including a
+    # scene updated twice in one list
+    scenes = [S.mixed_slab(n, seed=n, extent=(1.0, 1.0, 0.1)) for n in (3000, 12000, 1, 25000)]
+    a = [cb.DeviceScene(s) for s in scenes]
+    b = [cb.DeviceScene(s) for s in scenes]
+    ctx = cb.Context()
+    plan = [(0, 11), (1, 12), (3, 13), (1, 14), (2, 15), (1, 16)]
+    for k, seed in plan:
+        SV.perturb_(ctx, a[k], seed)
+    SV.perturb_many(ctx, [(b[k], seed) for k, seed in plan])
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert torch.equal(x.pos.view(torch.int32), y.pos.view(torch.int32))
+        assert torch.equal(x.rot.view(torch.int32), y.rot.view(torch.int32))
