@@ -89,6 +89,8 @@ STAGE_BYTES = {
     "count": lambda N, E, G, P, C: 48 * N + 4 * G,     # shift in place (24 r + 24 w) + cell counts
     "scan_cells": lambda N, E, G, P, C: 8 * G,
     "scatter": lambda N, E, G, P, C: 24 * N + 4 * G + 32 * E,
+    # shift + count, cell scan and scatter fused in one cooperative launch
+    "front": lambda N, E, G, P, C: (48 * N + 4 * G) + 8 * G + (24 * N + 4 * G + 32 * E),
     "pair_test": lambda N, E, G, P, C: 32 * E + 4 * G + 8 * P + 4 * N,
     "scan_owner": lambda N, E, G, P, C: 12 * N,
     "owner_scatter": lambda N, E, G, P, C: 16 * P + 8 * N,
@@ -100,7 +102,7 @@ STAGE_BYTES = {
 
 # Stages of the broadphase proper (detectPossibleCollisions after the AABBs),
 # in pipeline order; stages absent from a run are skipped.
-BP_STAGES = ("count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
+BP_STAGES = ("front", "count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
 STAGE_TIERS = {"segsort": ("segsort_mid", "segsort_big")}
 
 
@@ -116,7 +118,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-scene batched measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream measurement")
     ap.add_argument("--no-clustered", action="store_true", help="skip the 16.7M clustered-sphere broadphase")
-    ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--clustered-bodies", type=int, default=1 << 24,
                     help="body count of the clustered-sphere measurement (profiling uses smaller cases)")
     ap.add_argument("--only-clustered", action="store_true",
@@ -311,28 +313,34 @@ def bench_small(cb, dev, steps=200):
             "l2": "not flushed (the scene is 1.4 MB)"}
 
 
+SERVE_WORKLOAD = ("served: Poisson arrivals, 70% time-step updates of a resident scene (positions N(0,1e-4^2), turns "
+                  "<= 1e-3 rad), 30% new scenes; 4,096 resident scenes of log-uniform [2,000, 500,000] mixed shapes "
+                  "(128 generated scenes, each placed 32 times with its own seeded displacement field); a new scene "
+                  "is a generated scene uploaded from pinned host memory and displaced by its query's own seeded "
+                  "field; admission by byte accounting against a 150 GB HBM budget, scenes placed in an arena "
+                  "reserved at start-up")
+
+
 def bench_served(cb, dev, seconds):
-    """Poisson streams (2,000 and 4,000 queries/s, 70% updates / 30% new
-    scenes) on device-resident scenes: continuous batching against the
-    per-query path, plus the capacity of both with about 1,000 queries queued
-    at once."""
+    """Poisson streams (2,000 and 4,000 queries/s) on 4,096 resident scenes:
+    continuous batching against the per-query path, plus the capacity of both
+    with about 1,000 queries queued at once."""
     from collide_b200 import serving as SV
-    pool = [SV.PinnedScene(s) for s in SV.scene_pool(64, seed=0)]
-    out = {"workload": "scene_pool: 64 mixed_slab scenes, bodies log-uniform [2,000, 500,000]; 256 resident at "
-                       "start; updates move bodies by N(0,1e-4^2) and turn them by <= 1e-3 rad; new scenes come "
-                       "from pinned host memory; HBM budget 150 GB, scenes placed in a 32 GB arena reserved at "
-                       "start-up",
-           "rate_qps": 2000.0, "duration_s": seconds}
+    pool = [SV.PinnedScene(sc) for sc in SV.scene_pool(128, seed=0)]
+    R = 4096
+    out = {"workload": SERVE_WORKLOAD, "rate_qps": 2000.0, "duration_s": seconds}
     for mode in ("batched", "plain"):
-        srv = SV.Server(pool, resident=256, budget_bytes=150e9, max_batch=256, grid=BINS, device=dev)
+        srv = SV.Server(pool, resident=R, budget_bytes=150e9, max_batch=256, grid=BINS, device=dev,
+                        reserve_bytes=int(64e9), distinct=True)
         # warm-up: passes of the sizes the timed streams produce, new-scene admissions included
-        srv.serve(SV.poisson_stream(4000.0, 0.25, resident=256, pool=64, seed=99), mode=mode)
-        r = srv.serve(SV.poisson_stream(2000.0, seconds, resident=256, pool=64, seed=1), mode=mode)
-        hot = srv.serve(SV.poisson_stream(4000.0, seconds / 2, resident=256, pool=64, seed=3), mode=mode)
+        srv.serve(SV.poisson_stream(4000.0, 0.25, resident=R, pool=len(pool), seed=99), mode=mode)
+        r = srv.serve(SV.poisson_stream(2000.0, seconds, resident=R, pool=len(pool), seed=1), mode=mode)
+        hot = srv.serve(SV.poisson_stream(4000.0, seconds / 2, resident=R, pool=len(pool), seed=3), mode=mode)
         r["at_4000_qps"] = {k: hot[k] for k in ("queries", "queries_per_s", "p50_ms", "p99_ms", "mean_pass_queries")}
-        cap = srv.serve(SV.poisson_stream(1e6, 1e-3, resident=256, pool=64, seed=2), mode=mode)
+        cap = srv.serve(SV.poisson_stream(1e6, 1e-3, resident=R, pool=len(pool), seed=2), mode=mode)
         r["capacity_queries_per_s"] = cap["queries_per_s"]
         r["capacity_queries"] = cap["queries"]
+        r["initial_resident"] = srv.initial
         out[mode] = r
         del srv
     del pool

@@ -72,51 +72,60 @@ def perturb_many(ctx: Context, updates, sigma=1e-4, max_angle=1e-3):
 
 
 class PinnedScene:
-    """A host scene in pinned memory, uploaded without a staging copy."""
+    """A host scene in one pinned buffer laid out exactly as its device copy
+    (the nine arrays at 256-byte aligned offsets), so an upload is a single
+    copy into arena space."""
+
+    FIELDS = (("T", np.int32), ("A", np.float32), ("B", np.float32), ("C", np.float32), ("R", np.float32),
+              ("ID", np.int32), ("pos", np.float32), ("rot", np.float32), ("active", np.uint8))
 
     def __init__(self, scene):
         self.scene = scene
         self.n, self.nb = scene.n, scene.nb
-        pin = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).pin_memory()  # noqa: E731
+        arrays = {k: np.ascontiguousarray(getattr(scene, k)) for k, _ in self.FIELDS}
+        arrays["ID"] = np.ascontiguousarray(arrays["ID"], dtype=np.uint32).view(np.int32)
+        self.layout, off = [], 0
+        for k, dt in self.FIELDS:
+            a = np.ascontiguousarray(arrays[k], dtype=dt)
+            self.layout.append((k, off, a.shape, dt))
+            off += _align(a.nbytes)
+        self.total = off
         with numa_local():  # pages on the GPU's NUMA node
-            self.t = self._pin(scene, pin)
-
-    @staticmethod
-    def _pin(scene, pin):
-        return dict(T=pin(scene.T, np.int32), A=pin(scene.A, np.float32), B=pin(scene.B, np.float32),
-                    C=pin(scene.C, np.float32), R=pin(scene.R, np.float32),
-                    ID=pin(np.ascontiguousarray(scene.ID, dtype=np.uint32).view(np.int32), np.int32),
-                    pos=pin(scene.pos, np.float32), rot=pin(scene.rot, np.float32),
-                    active=pin(scene.active, np.uint8))
+            self.buf = torch.empty(max(self.total, 1), dtype=torch.uint8, pin_memory=True)
+            host = self.buf.numpy()
+            for k, off, shape, dt in self.layout:
+                a = np.ascontiguousarray(arrays[k], dtype=dt)
+                host[off:off + a.nbytes] = a.view(np.uint8).reshape(-1)
 
     def nbytes(self):
         return self.scene.nbytes()
 
     def device_bytes(self) -> int:
         """Bytes of the device copy, each array starting on a 256-byte boundary."""
-        return sum(_align(v.numel() * v.element_size()) for v in self.t.values())
+        return self.total
 
     def upload(self, device, copy_stream=None, space=None) -> DeviceScene:
-        """The device copy, filled on copy_stream if given. space: a uint8
-        device tensor of device_bytes() to hold the arrays (views into it);
-        without it each array is a new allocation."""
+        """The device copy, filled by one copy on copy_stream if given. space:
+        a uint8 device tensor of device_bytes() to hold the arrays (views into
+        it); without it the scene gets one new allocation."""
+        if space is None:
+            space = torch.empty(max(self.total, 1), dtype=torch.uint8, device=device)
+        if copy_stream is None:
+            space[:self.total].copy_(self.buf[:self.total], non_blocking=True)
+        else:
+            with torch.cuda.stream(copy_stream):
+                space[:self.total].copy_(self.buf[:self.total], non_blocking=True)
         ds = DeviceScene.__new__(DeviceScene)
         ds.n, ds.nb = self.n, self.nb
-        off = 0
-        for k, v in self.t.items():
-            nbytes = v.numel() * v.element_size()
-            if space is None:
-                d = torch.empty(v.shape, dtype=v.dtype, device=device)
-            else:
-                d = space[off:off + nbytes].view(v.dtype).view(v.shape)
-                off += _align(nbytes)
-            if copy_stream is None:
-                d.copy_(v, non_blocking=True)
-            else:
-                with torch.cuda.stream(copy_stream):
-                    d.copy_(v, non_blocking=True)
-            setattr(ds, k, d)
+        for k, off, shape, dt in self.layout:
+            nbytes = int(np.prod(shape)) * np.dtype(dt).itemsize
+            t = space[off:off + nbytes].view(_TORCH_DTYPE[np.dtype(dt)])
+            setattr(ds, k, t.view(shape) if len(shape) > 1 else t)
         return ds
+
+
+_TORCH_DTYPE = {np.dtype(np.int32): torch.int32, np.dtype(np.float32): torch.float32,
+                np.dtype(np.uint8): torch.uint8}
 
 
 def _align(nbytes, a=256):
@@ -166,6 +175,8 @@ class Query:
     done: float = math.nan  # completion time, seconds after the start
     n_pairs: int = 0
     n_contacts: int = 0
+    record: bool = False    # keep this query's scene state and contacts (query.result) for checking
+    result: dict | None = None
 
 
 @dataclass
@@ -198,9 +209,14 @@ def scene_pool(count=64, nmin=2000, nmax=500_000, seed=0):
     return [S.mixed_slab(int(n), seed=seed * 7919 + 1 + i, extent=(10.0, 10.0, 0.5)) for i, n in enumerate(sizes)]
 
 
+# A new scene is a pool scene displaced by its query's own seeded field, so no
+# two admitted scenes are equal (the resident set is placed the same way).
+NEW_SIGMA, NEW_ANGLE = 1e-3, 1e-2
+
+
 class Server:
     def __init__(self, pool, resident=256, budget_bytes=150e9, max_batch=256, grid=(16, 16, 16), precision="exact",
-                 device="cuda", reserve_bytes=None):
+                 device="cuda", reserve_bytes=None, distinct=False):
         # the resident scenes live in one arena reserved up front, so admitting
         # a scene costs a copy, not a device allocation (reserve_bytes=0: one
         # allocation per array instead)
@@ -217,13 +233,16 @@ class Server:
         self.bytes = 0
         self.next_id = 0
         self.batch = ScenesPipeline(self.ctx, grid=self.grid)
-        self.plain: dict[int, DevicePipeline] = {}
+        self.plain = None  # the per-query path's outputs, shared by every scene (sized for the largest)
         self.rejected = 0
         for i in range(resident):
             if self.admit(self.pool[i % len(self.pool)]) is None:
                 break
         self.initial = len(self.resident)
         self.slots = list(self.resident)  # the scenes update queries address
+        if distinct:  # every placement of a pool scene gets its own displacement
+            perturb_many(self.ctx, [(self.resident[s], 1_000_003 * (k + 1)) for k, s in enumerate(self.slots)],
+                         NEW_SIGMA, NEW_ANGLE)
         # size the library's scratch once for a full pass over resident scenes
         # (it only grows, by half at a time, after that)
         warm = [self.resident[s] for s in self.slots[: self.max_batch]]
@@ -266,7 +285,6 @@ class Server:
     def _evict(self, sid):
         ds = self.resident.pop(sid)
         self.bytes -= ds.resident_bytes
-        self.plain.pop(sid, None)
         if self.arena is not None:
             self.arena.give(ds.arena_at, ds.arena_bytes)
 
@@ -274,7 +292,10 @@ class Server:
         """Applies a query's input; returns its resident scene id (None: the
         scene is gone or did not fit the budget)."""
         if q.kind == "new":
-            return self.admit(self.pool[q.scene], pinned)
+            sid = self.admit(self.pool[q.scene], pinned)
+            if sid is not None:
+                perturb_(self.ctx, self.resident[sid], q.seed, NEW_SIGMA, NEW_ANGLE)
+            return sid
         sid = self.slots[q.scene % len(self.slots)]
         if sid not in self.resident:  # evicted: the update has nothing to move
             return None
@@ -283,15 +304,46 @@ class Server:
         return sid
 
     # -- passes ---------------------------------------------------------
+    @staticmethod
+    def _scene_copy(ds):
+        return {k: getattr(ds, k).clone() for k, _ in PinnedScene.FIELDS}
+
+    def _record_batch(self, k, scenes):
+        """Scene k of the last batched pass: its arrays as collided and its
+        contacts in the scene's own numbering."""
+        b = self.batch
+        co = b.contact_offsets.astype(np.int64)
+        off = sum(d.n for d in scenes[:k])
+        c0, c1 = int(co[k]), int(co[k + 1])
+        keys = b.pairs[c0:c1]
+        local = ((keys >> 32) - off) * (1 << 32) + ((keys & 0xFFFFFFFF) - off)
+        return dict(scene=self._scene_copy(scenes[k]), n_pairs=int(b.scene_pairs[k]), n_contacts=c1 - c0,
+                    contact_pairs=local.clone(), norm=b.norm[c0:c1].clone(), depth=b.depth[c0:c1].clone(),
+                    cpta=b.cpta[c0:c1].clone(), cptb=b.cptb[c0:c1].clone())
+
+    def _record_plain(self, sid):
+        p = self.plain
+        C = p.n_contacts
+        return dict(scene=self._scene_copy(self.resident[sid]), n_pairs=p.n_pairs, n_contacts=C,
+                    contact_pairs=p.pairs[:C].clone(), norm=p.norm[:C].clone(), depth=p.depth[:C].clone(),
+                    cpta=p.cpta[:C].clone(), cptb=p.cptb[:C].clone())
+
     def collide_batch(self, sids):
         self.batch.run([self.resident[s] for s in sids])
         co = self.batch.contact_offsets.astype(np.int64)
         return [(int(self.batch.scene_pairs[i]), int(co[i + 1] - co[i])) for i in range(len(sids))]
 
     def collide_one(self, sid):
-        p = self.plain.get(sid)
-        if p is None:
-            p = self.plain[sid] = DevicePipeline(self.resident[sid], grid=self.grid, ctx=self.ctx)
+        """cc_collide on one resident scene into the shared output buffers."""
+        if self.plain is None:
+            big = max(self.pool, key=lambda ps: ps.n)
+            self.plain = DevicePipeline(self.resident[sid], grid=self.grid, ctx=self.ctx,
+                                        pairs_cap=max(1024, big.n // 4))
+            self.plain.aabb = torch.zeros((2 * big.n, 3), dtype=torch.float32, device=self.device)
+            self.plain.res.aabb = self.plain.aabb.data_ptr()
+        p = self.plain
+        p.ds = self.resident[sid]
+        p.scene = p.ds.c_scene()
         return p.run()
 
     def serve(self, stream: Stream, mode="batched"):
@@ -321,6 +373,8 @@ class Server:
             sid = self._prepare(q)
             if sid is not None:
                 q.n_pairs, q.n_contacts = self.collide_one(sid)
+                if q.record:
+                    q.result = self._record_plain(sid)
             torch.cuda.synchronize()
             q.done = time.perf_counter() - t0
         return self._report(qs, t0, [1] * len(qs), mode)
@@ -358,8 +412,9 @@ class Server:
                         job = jobs.get()
                         if job is None:
                             return
-                        ev, updates, uniq, scenes, live, take = job
+                        ev, arrivals, updates, uniq, scenes, live, take = job
                         pass_s.wait_event(ev)
+                        perturb_many(self.ctx, arrivals, NEW_SIGMA, NEW_ANGLE)
                         perturb_many(self.ctx, updates)
                         if uniq:
                             self.batch.run(scenes)
@@ -368,6 +423,8 @@ class Server:
                                    for k, sid in enumerate(uniq)}
                             for q, sid in live:
                                 q.n_pairs, q.n_contacts = res[sid]
+                                if q.record:
+                                    q.result = self._record_batch(uniq.index(sid), scenes)
                         pass_s.synchronize()
                         t = time.perf_counter() - t0
                         for q in take:
@@ -396,10 +453,12 @@ class Server:
                 i = j
                 with lock:
                     pinned = set(busy)
-                updates, live = [], []
+                updates, arrivals, live = [], [], []
                 for q in take:
                     if q.kind == "new":
                         sid = self.admit(self.pool[q.scene], pinned, copy_s)
+                        if sid is not None:
+                            arrivals.append((self.resident[sid], q.seed))
                     else:
                         sid = self.slots[q.scene % len(self.slots)]
                         if sid not in self.resident:
@@ -417,7 +476,7 @@ class Server:
                 with lock:
                     for sid in uniq:
                         busy[sid] = busy.get(sid, 0) + 1
-                jobs.put((ev, updates, uniq, scenes, live, take))
+                jobs.put((ev, arrivals, updates, uniq, scenes, live, take))
                 passes.append(len(take))
         finally:
             while th.is_alive():  # the worker may have stopped on an error

@@ -29,11 +29,12 @@ struct Buf {
 // Kernel stages timed by the optional profiler.
 enum Stage : int {
 	ST_AABB, ST_BOUNDS, ST_COUNT, ST_SCAN_CELLS, ST_SCATTER, ST_PAIR_TEST, ST_SCAN_OWNER, ST_OWNER_SCATTER,
-	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_SEGSORT_MID, ST_SEGSORT_BIG, ST_COUNT_
+	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_SEGSORT_MID, ST_SEGSORT_BIG, ST_FRONT,
+	ST_COUNT_
 };
 const char *kStageNames[ST_COUNT_] = {"aabb", "bounds", "count", "scan_cells", "scatter", "pair_test",
                                       "scan_owner", "owner_scatter", "segsort", "mpr", "np_compact", "bins",
-                                      "copy_in", "copy_out", "segsort_mid", "segsort_big"};
+                                      "copy_in", "copy_out", "segsort_mid", "segsort_big", "front"};
 constexpr int kMaxMarks = 64;
 
 }  // namespace
@@ -44,9 +45,10 @@ struct cc_ctx {
 	GridParams gp{};
 	cudaError_t cuda_err = cudaSuccess;
 	// device scratch
-	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list, dense;
+	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list, dense,
+	    front_sums;
 	Buf ref_cnt, ref_off, ref_keys, ref_tmp, ref_flags, ref_runpos, rx_hist, rx_hoff;
-	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes;
+	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes, np_bsum;
 	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
 	    out_depth, out_bids;
 	// batch scratch: offsets, scene of each shape, global body ids, per-scene
@@ -325,6 +327,7 @@ cc_status np_prepare(cc_ctx *c, uint64_t P) {
 	CC_TRY(ensure(c, c->np_pos, 8 * (P + 1)));
 	CC_TRY(ensure(c, c->np_order, 4 * P));
 	CC_TRY(ensure(c, c->np_classes, (2 * kNpClasses + 32) * sizeof(uint32_t)));
+	CC_TRY(ensure(c, c->np_bsum, kNpCoopBlocks * sizeof(unsigned long long)));
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
 	c->st_words[2] = std::max<uint64_t>(c->st_words[2], status_words_for(P + 1));
 	CC_TRY(ensure_status(c));
@@ -357,6 +360,7 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 
 	CC_TRY(ensure_status(c));
 	CC_TRY(ensure(c, c->ticket, 64));
 	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * (n + 1024)));
+	CC_TRY(ensure(c, c->front_sums, sizeof(unsigned long long) * kFrontMaxBlocks));
 	CC_TRY(ensure(c, c->dense, sizeof(uint2) * (c->entries.bytes / (2 * sizeof(float4)) / kDenseCell + 1024)));
 	if (np_cap) CC_TRY(np_prepare(c, np_cap));
 	return CC_OK;
@@ -374,6 +378,9 @@ NpScratch np_scratch(cc_ctx *c) {
 	sc.pos = ptr<unsigned long long>(c->np_pos);
 	sc.status = ptr<uint64_t>(c->status) + c->st_words[0] + c->st_words[1];
 	sc.ticket = ptr<uint32_t>(c->ticket) + 8;
+	sc.bar_classes = ptr<DevStats>(c->stats)->bar_np;
+	sc.bar_compact = ptr<DevStats>(c->stats)->bar_compact;
+	sc.block_sums = ptr<unsigned long long>(c->np_bsum);
 	sc.err = &ptr<DevStats>(c->stats)->err;
 	sc.order = ptr<uint32_t>(c->np_order);
 	sc.classes = ptr<uint32_t>(c->np_classes);
@@ -438,18 +445,25 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 		return;
 	}
 	c->inc_valid = false;  // the kept cell lists are overwritten
-	{
-		StageMark m(c, ST_COUNT, s);
+	if (!b.sm.plans) {  // one scene: shift + count, cell scan and scatter in one cooperative launch
+		StageMark m(c, ST_FRONT, s);
 		if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
-		launch_count(n, aabb, b, s);
-	}
-	{
-		StageMark m(c, ST_SCAN_CELLS, s);
-		launch_scan_cells(b, gmax, s);
-	}
-	{
-		StageMark m(c, ST_SCATTER, s);
-		launch_scatter(n, aabb, b, s);  // the cell scan left the counts zeroed
+		launch_front(n, aabb, b, ptr<unsigned long long>(c->front_sums), s);
+		c->launches -= 2;
+	} else {
+		{
+			StageMark m(c, ST_COUNT, s);
+			if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
+			launch_count(n, aabb, b, s);
+		}
+		{
+			StageMark m(c, ST_SCAN_CELLS, s);
+			launch_scan_cells(b, gmax, s);
+		}
+		{
+			StageMark m(c, ST_SCATTER, s);
+			launch_scatter(n, aabb, b, s);  // the cell scan left the counts zeroed
+		}
 	}
 	{
 		StageMark m(c, ST_PAIR_TEST, s);

@@ -135,6 +135,50 @@ __device__ __forceinline__ uint64_t lookback_prefix(uint64_t *status, uint32_t t
 	return excl;
 }
 
+// ---------------------------------------------------------------------------
+// Grid-wide barrier of a cooperative launch (cudaLaunchCooperativeKernel: every
+// block is resident at once). `arrived` counts the blocks at the barrier; the
+// last one resets it and bumps `gen`, which the others poll. Both words start
+// at zero (they live in per-call state that is zeroed before the pass) and
+// `arrived` is zero again after every completed barrier. The wait is bounded:
+// after kSpinLimit polls it sets kErrSpinLimit and lets the block go on, so a
+// broken launch returns an error status instead of hanging.
+// ---------------------------------------------------------------------------
+struct GridBarrier {
+	unsigned int arrived;
+	unsigned int gen;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
+	unsigned int v;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+
+__device__ __forceinline__ void grid_barrier(GridBarrier *b, uint32_t *err) {
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		const unsigned int g = ld_acquire_u32(&b->gen);  // before arriving: the gen this barrier bumps
+		__threadfence();                                 // the block's writes before its arrival
+		if (atomicAdd(&b->arrived, 1u) == gridDim.x - 1) {
+			atomicExch(&b->arrived, 0u);
+			__threadfence();
+			atomicAdd(&b->gen, 1u);
+		} else {
+			int spins = 0;
+			while (ld_acquire_u32(&b->gen) == g) {
+				if (++spins > kSpinLimit) {
+					atomicOr(err, (uint32_t)kErrSpinLimit);
+					break;
+				}
+				__nanosleep(64);
+			}
+		}
+		__threadfence();
+	}
+	__syncthreads();
+}
+
 // Grid-stride zeroing of the ranges of a ZeroList (called by every thread of
 // a pass's first kernel).
 template <class ZL>

@@ -56,6 +56,12 @@ struct DevStats {
 	uint32_t blocks_done;         // last-block detection of the bounds reduction
 	uint32_t pad_;
 	Plan plan;
+	// grid barriers of the cooperative kernels (GridBarrier: arrived, gen),
+	// zeroed with the rest at the start of a pass
+	uint32_t bar_front[2];
+	uint32_t bar_np[2];
+	uint32_t bar_compact[2];
+	uint32_t pad3_[2];
 };
 
 constexpr int kMaxDim = 1024;  // cells per axis (10-bit packed cell coordinates)
@@ -165,6 +171,11 @@ void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridPar
 // In-place shift + per-cell counts on the plan's search grid.
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
+// One scene (b.sm empty), after the bounds pass: launch_count + launch_scan_cells
+// + launch_scatter as one cooperative launch with the same results.
+// block_sums: kFrontMaxBlocks words.
+constexpr unsigned kFrontMaxBlocks = 148 * 8;
+void launch_front(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *block_sums, cudaStream_t s);
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
@@ -270,8 +281,14 @@ struct NpScratch {
 	uint32_t *order;        // P: pair indices grouped by (type A, type B)
 	uint32_t *classes;      // 2 * kNpClasses counters + the work-queue counter (zeroed per call)
 	bool pre_zeroed = false;  // classes, status and ticket already zeroed for this pass
+	void *bar_classes = nullptr;  // grid barriers (GridBarrier) of the cooperative class sort and compaction,
+	void *bar_compact = nullptr;  // zeroed at the start of the call
+	unsigned long long *block_sums = nullptr;  // per-block flag counts of the compaction (>= its grid)
 };
 constexpr int kNpClasses = 64;  // 7 x 7 shape-type combinations + one for invalid keys
+// Grid bound of the narrowphase's cooperative kernels (and the size of
+// NpScratch::block_sums).
+constexpr unsigned kNpCoopBlocks = 148 * 8;
 
 // Pair indices >= n and body ids >= nb set kErrBadIndex in *sc.err; such a
 // pair is reported as no contact. precision: 0 exact (the reference's FP64

@@ -142,3 +142,32 @@ def test_batched_updates_equal_one_at_a_time(cb):
     for x, y in zip(a, b):
         assert torch.equal(x.pos.view(torch.int32), y.pos.view(torch.int32))
         assert torch.equal(x.rot.view(torch.int32), y.rot.view(torch.int32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["batched", "plain"])
+def test_live_stream_results_equal_solo_calls(cb, mode):
+    # queries recorded DURING a Poisson stream (new scenes admitted, updates
+    # moving resident scenes, passes overlapping the next admissions): each
+    # recorded result equals a solo cc_collide on the same post-update scene
+    pool = [S.mixed_slab(n, seed=n, extent=(1.0, 1.0, 0.1)) for n in (3000, 12000, 800, 25000, 6000)]
+    srv = SV.Server(pool, resident=6, max_batch=32, reserve_bytes=1 << 28)
+    st = SV.poisson_stream(rate=600.0, duration=0.3, resident=6, pool=5, seed=4)
+    for q in st.queries[::5]:
+        q.record = True
+    r = srv.serve(st, mode=mode)
+    assert r["queries"] == len(st.queries)
+    rec = [q for q in st.queries if q.record and q.result is not None]
+    assert len(rec) >= 10 and {q.kind for q in rec} == {"update", "new"}
+    ctx = cb.Context()
+    for q in rec:
+        res = q.result
+        ds = cb.DeviceScene.__new__(cb.DeviceScene)
+        for k, t in res["scene"].items():
+            setattr(ds, k, t)
+        ds.n, ds.nb = int(ds.T.shape[0]), int(ds.pos.shape[0])
+        solo = cb.collide(ds, grid=srv.grid, ctx=ctx)
+        assert solo["n_pairs"] == res["n_pairs"] and solo["n_contacts"] == res["n_contacts"]
+        assert torch.equal(solo["contact_pairs"], res["contact_pairs"])
+        for k in ("norm", "depth", "cpta", "cptb"):
+            assert torch.equal(solo[k].view(torch.int32), res[k].view(torch.int32)), k
