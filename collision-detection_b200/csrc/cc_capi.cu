@@ -37,6 +37,23 @@ const char *kStageNames[ST_COUNT_] = {"aabb", "bounds", "count", "scan_cells", "
                                       "copy_in", "copy_out", "segsort_mid", "segsort_big", "front"};
 constexpr int kMaxMarks = 64;
 
+// A CUDA graph of one kind of call, replayed while the call's configuration
+// (its key: everything its launches depend on) repeats.
+struct GraphSlot {
+	cudaGraphExec_t exec = nullptr;
+	unsigned char key[512] = {};
+	unsigned char pending[512] = {};
+	size_t key_size = 0;
+	bool have_pending = false;
+	uint64_t launches = 0;
+	void drop() {
+		if (exec) cudaGraphExecDestroy(exec);
+		exec = nullptr;
+		have_pending = false;
+		key_size = 0;
+	}
+};
+
 }  // namespace
 
 struct cc_ctx {
@@ -119,12 +136,8 @@ struct cc_ctx {
 	// CUDA graph of the whole device pipeline (cc_collide), replayed while its
 	// configuration (GraphKey) is unchanged
 	cudaStream_t cap_stream = nullptr;
-	cudaGraphExec_t gexec = nullptr;
 	bool graph_off = false;
-	unsigned char gkey[sizeof(void *) * 40] = {};
-	unsigned char pending_key[sizeof(void *) * 40] = {};
-	bool have_pending = false;
-	uint64_t glaunches = 0;
+	GraphSlot g_collide, g_batch;  // cc_collide's step and the batch pass
 	// stage profiler
 	bool prof = false;
 	cudaEvent_t ev[2 * kMaxMarks] = {};
@@ -628,6 +641,60 @@ cc_status check_grid(cc_ctx *c, int gx, int gy, int gz) {
 	return CC_OK;
 }
 
+// Runs enqueue_all on `s`, or replays its graph: a configuration (key) that
+// reaches the slot twice in a row is captured on the context's capture stream
+// and replayed by one graph launch from then on. Where capture fails the
+// context stays on stream launches.
+template <class F>
+cc_status run_graphed(cc_ctx *c, GraphSlot &g, const void *key, size_t ksize, F &&enqueue_all, cudaStream_t s) {
+	bool replayed = false;
+	if (!c->prof && !c->graph_off && ksize <= sizeof(g.key)) {
+		if (g.exec && g.key_size == ksize && memcmp(key, g.key, ksize) == 0) {
+			replayed = true;
+		} else if (g.have_pending && memcmp(key, g.pending, ksize) == 0) {
+			if (!c->cap_stream) CC_CUDA(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+			const uint64_t l0 = c->launches;
+			cudaGraph_t gr = nullptr;
+			cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed);
+			cc_status st = CC_OK;
+			if (e == cudaSuccess) {
+				st = enqueue_all(c->cap_stream);
+				e = cudaStreamEndCapture(c->cap_stream, &gr);
+			}
+			if (st != CC_OK) {
+				if (gr) cudaGraphDestroy(gr);
+				c->launches = l0;
+				g.have_pending = false;
+				return st;
+			}
+			g.launches = c->launches - l0;
+			c->launches = l0;
+			g.drop();
+			if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, gr, 0);
+			if (gr) cudaGraphDestroy(gr);
+			if (e == cudaSuccess) {
+				memcpy(g.key, key, ksize);
+				g.key_size = ksize;
+				replayed = true;
+			} else {  // not capturable here: stay on stream launches
+				cudaGetLastError();
+				g.exec = nullptr;
+				c->graph_off = true;
+			}
+		} else {
+			memcpy(g.pending, key, ksize);
+			g.have_pending = true;
+		}
+	}
+	if (replayed) {
+		CC_CUDA(c, cudaGraphLaunch(g.exec, s));
+		c->launches += g.launches;
+	} else {
+		CC_TRY(enqueue_all(s));
+	}
+	return check_launch(c);
+}
+
 // The first half of collide_dev: sizes the scratch and enqueues the whole step
 // on `s` (or replays its graph when `graphs`), without waiting.
 cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
@@ -677,74 +744,28 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 		c->pass_zeroed = false;
 		return CC_OK;
 	};
-	bool replayed = false;
-	if (graphs && !c->prof && !c->graph_off) {
-		// everything the captured launches depend on
-		struct {
-			uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
-			const void *p[18];
-			int dims[3], prec, oshift, kbits;
-			float env;
-			GridParams gp;
-		} k;
-		memset(&k, 0, sizeof(k));
-		k.n = n; k.nb = sc.nb; k.pairs_cap = pairs_cap; k.hE = hint_E(c, n); k.hP = hint_P(c); k.gen = c->buf_gen;
-		for (int r = 0; r < 3; r++) k.st[r] = c->st_words[r];
-		k.incm = (inc ? 2u : 0u) | (inc_ready ? 1u : 0u);
-		const void *ps[18] = {sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, aabb,
-		                      pairs, norm, cpta, cptb, depth, bids, nullptr, nullptr};
-		memcpy(k.p, ps, sizeof(ps));
-		k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.env = envelope; k.gp = c->gp;
-		k.oshift = c->owner_shift; k.kbits = c->key_bits;
-		static_assert(sizeof(k) <= sizeof(c->gkey), "graph key");
-		if (c->gexec && memcmp(&k, c->gkey, sizeof(k)) == 0) {
-			replayed = true;
-		} else if (c->have_pending && memcmp(&k, c->pending_key, sizeof(k)) == 0) {
-			// the same configuration twice in a row: capture it
-			if (!c->cap_stream) CC_CUDA(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
-			const uint64_t l0 = c->launches;
-			cudaGraph_t g = nullptr;
-			cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed);
-			cc_status st = CC_OK;
-			if (e == cudaSuccess) {
-				st = enqueue_all(c->cap_stream);
-				e = cudaStreamEndCapture(c->cap_stream, &g);
-			}
-			if (st != CC_OK) {
-				if (g) cudaGraphDestroy(g);
-				c->launches = l0;
-				c->have_pending = false;
-				return st;
-			}
-			c->glaunches = c->launches - l0;
-			c->launches = l0;
-			if (c->gexec) {
-				cudaGraphExecDestroy(c->gexec);
-				c->gexec = nullptr;
-			}
-			if (e == cudaSuccess) e = cudaGraphInstantiate(&c->gexec, g, 0);
-			if (g) cudaGraphDestroy(g);
-			if (e == cudaSuccess) {
-				memcpy(c->gkey, &k, sizeof(k));
-				replayed = true;
-			} else {  // not capturable here: stay on stream launches
-				cudaGetLastError();
-				c->gexec = nullptr;
-				c->graph_off = true;
-			}
-			c->have_pending = false;
-		} else {
-			memcpy(c->pending_key, &k, sizeof(k));
-			c->have_pending = true;
-		}
-	}
-	if (replayed) {
-		CC_CUDA(c, cudaGraphLaunch(c->gexec, s));
-		c->launches += c->glaunches;
-	} else {
+	if (!graphs) {
 		CC_TRY(enqueue_all(s));
+		return check_launch(c);
 	}
-	return check_launch(c);
+	// everything the captured launches depend on
+	struct {
+		uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
+		const void *p[18];
+		int dims[3], prec, oshift, kbits;
+		float env;
+		GridParams gp;
+	} k;
+	memset(&k, 0, sizeof(k));
+	k.n = n; k.nb = sc.nb; k.pairs_cap = pairs_cap; k.hE = hint_E(c, n); k.hP = hint_P(c); k.gen = c->buf_gen;
+	for (int r = 0; r < 3; r++) k.st[r] = c->st_words[r];
+	k.incm = (inc ? 2u : 0u) | (inc_ready ? 1u : 0u);
+	const void *ps[18] = {sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, aabb,
+	                      pairs, norm, cpta, cptb, depth, bids, nullptr, nullptr};
+	memcpy(k.p, ps, sizeof(ps));
+	k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.env = envelope; k.gp = c->gp;
+	k.oshift = c->owner_shift; k.kbits = c->key_bits;
+	return run_graphed(c, c->g_collide, &k, sizeof(k), enqueue_all, s);
 }
 
 // The second half: with c->h_stats current (the step's DevStats), checks
@@ -843,10 +864,12 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_off,    &c->b_scene_of, &c->b_gid,      &c->b_sst,    &c->b_plans,     &c->b_G,
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
-	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges};
+	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges, &c->front_sums,
+	               &c->np_bsum,  &c->pt_desc};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
-	if (c->gexec) cudaGraphExecDestroy(c->gexec);
+	c->g_collide.drop();
+	c->g_batch.drop();
 	if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
 	for (auto &h : c->hs) {
 		Buf *hb[] = {&h.T, &h.A, &h.B, &h.C, &h.R, &h.ID, &h.pos, &h.rot, &h.act, &h.aabb, &h.pairs, &h.norm, &h.pa,
@@ -945,10 +968,10 @@ uint64_t cc_last_launch_count(const cc_ctx *c) { return c ? c->launches : 0; }
 cc_status cc_set_graph_replay(cc_ctx *c, int on) {
 	if (!c) return CC_ERR_INVALID_ARGUMENT;
 	c->graph_off = !on;
-	c->have_pending = false;
-	if (!on && c->gexec) {
-		cudaGraphExecDestroy(c->gexec);
-		c->gexec = nullptr;
+	c->g_collide.have_pending = c->g_batch.have_pending = false;
+	if (!on) {
+		c->g_collide.drop();
+		c->g_batch.drop();
 	}
 	return CC_OK;
 }
@@ -1248,44 +1271,74 @@ cc_status batch_impl(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, floa
 	zero.words[3] = c->gp.g_max;
 	for (int r = 0; r < 4; r++)
 		if (!zero.p[r]) zero.words[r] = 0;
-	{
-		StageMark m(c, ST_AABB, s);
-		CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), s));
-		CC_CUDA(c, cudaMemsetAsync(sst, 0, sizeof(SceneStats) * S, s));
-		launch_batch_prep(n, (uint32_t)S, d_shape, d_body, sc.ID, scene_of, gid, &d->err, s);
-		launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, gid, sc.nb, sc.body_pos, sc.body_rot, res->aabb, nullptr, &d->err,
-		            c->gp, grid, s, zero);
-	}
-	{
-		StageMark m(c, ST_BOUNDS, s);
-		launch_batch_bounds(n, res->aabb, scene_of, sst, &d->err, s);
-		launch_batch_plan((uint32_t)S, d_shape, sst, c->gp, grid, plans, G, s);
-		launch_scan_u32_to_u32(G, S, base, ptr<uint64_t>(c->b_status), ptr<uint32_t>(c->b_ticket), &d->err, s,
-		                       nullptr, &d->cells);
-	}
-	c->launches += 6;
+	// the rest of the pipeline takes each shape's plan from the scene map
 	c->sm.scene_of = scene_of;
 	c->sm.plans = plans;
 	c->sm.cell_base = base;
-	c->pass_zeroed = true;
-	enqueue_search(c, n, res->aabb, s);
-	enqueue_emit(c, n, out, pairs_cap, s);
-	enqueue_np(c, a, pairs_cap, &d->np_n, s);
-	c->pass_zeroed = false;
-	// per-scene pair counts and contact offsets go back behind the pass, so
-	// the common case synchronizes once (redone below if the pass is redone)
 	const bool want_offsets = scene_pairs || contact_offsets;
-	auto copy_offsets = [&]() -> cc_status {
-		launch_batch_offsets((uint32_t)S, d_shape, ptr<unsigned long long>(c->owner_off),
-		                     ptr<unsigned long long>(c->np_pos), d, d_pairs_s, d_coff, s);
-		CC_TRY(check_launch(c));
+	auto enqueue_all = [&](cudaStream_t st) -> cc_status {
+		{
+			StageMark m(c, ST_AABB, st);
+			CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), st));
+			CC_CUDA(c, cudaMemsetAsync(sst, 0, sizeof(SceneStats) * S, st));
+			launch_batch_prep(n, (uint32_t)S, d_shape, d_body, sc.ID, scene_of, gid, &d->err, st);
+			launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, gid, sc.nb, sc.body_pos, sc.body_rot, res->aabb, nullptr,
+			            &d->err, c->gp, grid, st, zero);
+		}
+		{
+			StageMark m(c, ST_BOUNDS, st);
+			launch_batch_bounds(n, res->aabb, scene_of, sst, &d->err, st);
+			launch_batch_plan((uint32_t)S, d_shape, sst, c->gp, grid, plans, G, st);
+			launch_scan_u32_to_u32(G, S, base, ptr<uint64_t>(c->b_status), ptr<uint32_t>(c->b_ticket), &d->err, st,
+			                       nullptr, &d->cells);
+		}
+		c->launches += 6;
+		c->pass_zeroed = true;
+		enqueue_search(c, n, res->aabb, st);
+		enqueue_emit(c, n, out, pairs_cap, st);
+		enqueue_np(c, a, pairs_cap, &d->np_n, st);
+		c->pass_zeroed = false;
+		// per-scene pair counts and contact offsets, read back behind the pass
+		if (want_offsets) {
+			launch_batch_offsets((uint32_t)S, d_shape, ptr<unsigned long long>(c->owner_off),
+			                     ptr<unsigned long long>(c->np_pos), d, d_pairs_s, d_coff, st);
+			c->launches += 1;
+		}
+		return CC_OK;
+	};
+	// everything the pass's launches depend on (the offsets' contents are
+	// copied in before every pass, outside the graph)
+	struct {
+		uint64_t n, nb, S, pairs_cap, hE, hP, gen, st[3];
+		const void *p[16];
+		int dims[3], prec, want;
+		float env;
+		GridParams gp;
+	} k;
+	memset(&k, 0, sizeof(k));
+	k.n = n; k.nb = sc.nb; k.S = S; k.pairs_cap = pairs_cap; k.hE = hint_E(c, n); k.hP = hint_P(c);
+	k.gen = c->buf_gen;
+	for (int r = 0; r < 3; r++) k.st[r] = c->st_words[r];
+	const void *ps[16] = {sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, res->aabb,
+	                      res->pairs, res->norm, res->cpta, res->cptb, res->depth, res->bids};
+	memcpy(k.p, ps, sizeof(ps));
+	k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.want = want_offsets ? 1 : 0;
+	k.env = envelope; k.gp = c->gp;
+	CC_TRY(run_graphed(c, c->g_batch, &k, sizeof(k), enqueue_all, s));
+	auto copy_back = [&]() -> cc_status {
 		if (scene_pairs)
 			CC_CUDA(c, cudaMemcpyAsync(scene_pairs, d_pairs_s, sizeof(uint64_t) * S, cudaMemcpyDeviceToHost, s));
 		if (contact_offsets)
 			CC_CUDA(c, cudaMemcpyAsync(contact_offsets, d_coff, sizeof(uint64_t) * (S + 1), cudaMemcpyDeviceToHost, s));
 		return CC_OK;
 	};
-	if (want_offsets) CC_TRY(copy_offsets());
+	auto copy_offsets = [&]() -> cc_status {
+		launch_batch_offsets((uint32_t)S, d_shape, ptr<unsigned long long>(c->owner_off),
+		                     ptr<unsigned long long>(c->np_pos), d, d_pairs_s, d_coff, s);
+		CC_TRY(check_launch(c));
+		return copy_back();
+	};
+	if (want_offsets) CC_TRY(copy_back());
 	CC_TRY(check_launch(c));
 	CC_TRY(read_stats(c, s));
 	CC_TRY(device_err(c));
