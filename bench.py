@@ -132,14 +132,24 @@ BATCH_WORKLOAD = ("batched_mixed: 512 independent scenes, bodies log-uniform [1,
                   "shape mix, slab thickness 0.5/d with d ~ U[0.2,1.0] over a 10x10 footprint")
 
 
+def tuner_report(best, table):
+    keys = ("cell_target", "min_ratio", "dense_cell", "pair_window", "pair_blocks_per_sm")
+    return {"chosen": dict(zip(keys, best)), "candidates_ms": [[list(c), round(t, 3)] for c, t in (table or [])]}
+
+
 def bench_batched(cb, ctx, dev, steps=10):
-    """512 uneven scenes: one cc_collide_batch pass against cc_collide per scene."""
+    """512 uneven scenes: one cc_collide_batch pass (grid and launch shapes
+    from the tuner, replayed as a CUDA graph) against cc_collide per scene."""
     import torch
     from collide_b200 import scenes as S
+    from collide_b200 import tuner
     scenes = S.batched_mixed(512, seed=0)
     N = sum(s.n for s in scenes)
     db = cb.DeviceBatch(scenes, device=dev)
-    bp = cb.BatchPipeline(db, grid=BINS, ctx=ctx)
+    bctx = cb.Context(ctx.device)
+    bp = cb.BatchPipeline(db, grid=BINS, ctx=bctx)
+    bp.run()
+    best, table = tuner.tune_cached(bctx, bp.run, N, kind="batch")
     for _ in range(3):
         bp.run()
     torch.cuda.synchronize()
@@ -169,7 +179,10 @@ def bench_batched(cb, ctx, dev, steps=10):
             "ms_per_batch": tb, "value": N / (tb / 1000.0), "unit": "bodies/s",
             "per_scene_launch": {"ms": tl, "value": N / (tl / 1000.0), "unit": "bodies/s",
                                  "how": "cc_collide once per scene, in order, outputs preallocated"},
-            "speedup_vs_per_scene": tl / tb, "steps": steps, "checked": check}
+            "speedup_vs_per_scene": tl / tb, "steps": steps, "checked": check,
+            "tuner": tuner_report(best, table),
+            "graph_replay": "the pass repeats with the same configuration, so from the second call on it is one "
+                            "CUDA graph launch (cc_collide_batch)"}
 
 
 def contact_error_stats(gk, norm, cpta, cptb, depth, ref, scale):
@@ -280,8 +293,7 @@ def bench_clustered(cb, dev, steps=3, bodies=1 << 24):
            "pairs_per_s": P / (t / 1000.0),
            "device_gb_in_use": (lambda f: (f[1] - f[0]) / 1e9)(torch.cuda.mem_get_info()),
            "reference": "infeasible: uint32 pair counters (Broadphase.cuh:45) cannot hold 3.9e9 pairs",
-           "tuner": {"chosen": {"cell_target": best[0], "min_ratio": best[1], "dense_cell": best[2]},
-                     "candidates_ms": [[list(c), round(t, 2)] for c, t in table]}}
+           "tuner": tuner_report(best, table)}
     del a, a0, bp, ctx
     torch.cuda.empty_cache()
     return out
@@ -331,7 +343,7 @@ def bench_served(cb, dev, seconds):
     out = {"workload": SERVE_WORKLOAD, "rate_qps": 2000.0, "duration_s": seconds}
     for mode in ("batched", "plain"):
         srv = SV.Server(pool, resident=R, budget_bytes=150e9, max_batch=256, grid=BINS, device=dev,
-                        reserve_bytes=int(64e9), distinct=True)
+                        reserve_bytes=int(64e9), distinct=True, tune=True)
         # warm-up: passes of the sizes the timed streams produce, new-scene admissions included
         srv.serve(SV.poisson_stream(4000.0, 0.25, resident=R, pool=len(pool), seed=99), mode=mode)
         r = srv.serve(SV.poisson_stream(2000.0, seconds, resident=R, pool=len(pool), seed=1), mode=mode)
@@ -341,6 +353,7 @@ def bench_served(cb, dev, seconds):
         r["capacity_queries_per_s"] = cap["queries_per_s"]
         r["capacity_queries"] = cap["queries"]
         r["initial_resident"] = srv.initial
+        r["tuner"] = tuner_report(srv.tuned, None) if srv.tuned else None
         out[mode] = r
         del srv
     del pool

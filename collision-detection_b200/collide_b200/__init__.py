@@ -188,6 +188,11 @@ class Context:
         (0: never)."""
         self.check(lib.cc_set_dense_cell(self.h, int(entries)), "cc_set_dense_cell")
 
+    def set_pair_test_shape(self, window=96, blocks_per_sm=8):
+        """Launch shape of the sparse pair test: entries staged per warp (64,
+        96, 128) and the grid cap in blocks per SM."""
+        self.check(lib.cc_set_pair_test_shape(self.h, int(window), int(blocks_per_sm)), "cc_set_pair_test_shape")
+
     def set_narrowphase_precision(self, mode="exact"):
         """"exact" (default): the reference's MPR arithmetic in FP64, equal to
         the FP64 oracle up to float rounding of the outputs; "fp64": FP64 in a

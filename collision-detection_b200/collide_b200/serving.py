@@ -216,7 +216,7 @@ NEW_SIGMA, NEW_ANGLE = 1e-3, 1e-2
 
 class Server:
     def __init__(self, pool, resident=256, budget_bytes=150e9, max_batch=256, grid=(16, 16, 16), precision="exact",
-                 device="cuda", reserve_bytes=None, distinct=False):
+                 device="cuda", reserve_bytes=None, distinct=False, tune=False):
         # the resident scenes live in one arena reserved up front, so admitting
         # a scene costs a copy, not a device allocation (reserve_bytes=0: one
         # allocation per array instead)
@@ -246,8 +246,13 @@ class Server:
         # size the library's scratch once for a full pass over resident scenes
         # (it only grows, by half at a time, after that)
         warm = [self.resident[s] for s in self.slots[: self.max_batch]]
+        self.tuned = None
         if warm:
             self.batch.run(warm)
+            if tune:  # search grid and launch shapes for passes of this size (cached per size bucket)
+                from . import tuner
+                self.tuned, _ = tuner.tune_cached(self.ctx, lambda: self.batch.run(warm),
+                                                  sum(d.n for d in warm), kind="served")
         torch.cuda.synchronize()
 
     # -- residency ------------------------------------------------------

@@ -66,30 +66,67 @@ def autotune(run_with, candidates=((2.0, 2.0), (4.0, 2.0), (8.0, 2.0), (4.0, 1.0
 
 GRID_CANDIDATES = ((4.0, 2.0), (2.0, 2.0), (8.0, 2.0), (4.0, 1.0), (16.0, 1.0))
 DENSE_CANDIDATES = (128, 256, 512)
+# sparse pair test: (entries staged per warp, grid cap in blocks per SM)
+SHAPE_CANDIDATES = ((96, 8), (64, 8), (128, 5), (96, 4), (64, 16))
+DEFAULT = (4.0, 2.0, 128, 96, 8)
 
 
-def tune(ctx, run, grid_candidates=GRID_CANDIDATES, dense_candidates=DENSE_CANDIDATES, reps=1):
-    """Times run() (one call on the caller's scene through `ctx`) under every
-    (cell_target, min_ratio, dense_cell) candidate with CUDA events, sets the
-    fastest on `ctx` and returns (best, [(candidate, ms), ...]). Pairs and
-    contacts do not depend on the choice."""
+def _time_ms(run, reps):
     import torch
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def apply(ctx, choice):
+    kt, mr, dc, win, bps = choice
+    ctx.set_tuning(kt, mr)
+    ctx.set_dense_cell(dc)
+    ctx.set_pair_test_shape(win, bps)
+
+
+def tune(ctx, run, grid_candidates=GRID_CANDIDATES, dense_candidates=DENSE_CANDIDATES,
+         shape_candidates=SHAPE_CANDIDATES, reps=1):
+    """Times run() (one call through `ctx`) with CUDA events: first every
+    (cell_target, min_ratio, dense_cell) candidate at the default launch
+    shape, then every pair-test launch shape at the fastest of those; leaves
+    the fastest setting on `ctx` and returns (best, [(candidate, ms), ...])
+    with candidates (cell_target, min_ratio, dense_cell, window, blocks_per_sm).
+    Pairs and contacts do not depend on the choice."""
     table = []
+    win0, bps0 = DEFAULT[3], DEFAULT[4]
     for kt, mr in grid_candidates:
         for dc in dense_candidates:
-            ctx.set_tuning(kt, mr)
-            ctx.set_dense_cell(dc)
+            cand = (kt, mr, dc, win0, bps0)
+            apply(ctx, cand)
             run()  # sizes the scratch for this grid
-            best_ms = float("inf")
-            for _ in range(reps):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                run()
-                e1.record()
-                torch.cuda.synchronize()
-                best_ms = min(best_ms, e0.elapsed_time(e1))
-            table.append(((kt, mr, dc), best_ms))
+            table.append((cand, _time_ms(run, reps)))
     best = min(table, key=lambda x: x[1])[0]
-    ctx.set_tuning(best[0], best[1])
-    ctx.set_dense_cell(best[2])
+    for win, bps in shape_candidates:
+        cand = best[:3] + (win, bps)
+        if cand == best:
+            continue
+        apply(ctx, cand)
+        run()
+        table.append((cand, _time_ms(run, reps)))
+    best = min(table, key=lambda x: x[1])[0]
+    apply(ctx, best)
+    return best, table
+
+
+def tune_cached(ctx, run, n, kind="scene", **kw):
+    """tune() once per (kind, size bucket of n): later calls of the same
+    bucket only apply the cached choice. Returns (best, table or None)."""
+    key = (kind, size_bucket(n))
+    if key in _cache:
+        apply(ctx, _cache[key])
+        return _cache[key], None
+    best, table = tune(ctx, run, **kw)
+    _cache[key] = best
     return best, table

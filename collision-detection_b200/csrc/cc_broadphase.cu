@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(kNT) k_front(FrontArgs a) {
 // warp-uniform so the emission can be warp-aggregated: found pairs collect in
 // a per-warp shared buffer that is flushed with one counter atomic per
 // kOutBuf - 31 pairs or more (dense scenes emit billions of pairs).
-constexpr int kWin = 96;
+constexpr int kWinDefault = 96;  // window (entries per warp staged in shared memory); tunable: 64, 96, 128
 constexpr int kOutBuf = 128;
 
 __device__ __forceinline__ void flush_pairs(unsigned long long *buf, uint32_t cnt, uint32_t lane,
@@ -512,7 +512,7 @@ __device__ __forceinline__ void flush_pairs(unsigned long long *buf, uint32_t cn
 	__syncwarp();
 }
 
-template <bool kBatch>
+template <bool kBatch, int kWin>
 __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, const uint32_t *__restrict__ cell_start,
                                                     const float4 *__restrict__ entries,
                                                     uint64_t entry_cap, uint32_t *__restrict__ owner_count,
@@ -1178,18 +1178,31 @@ void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStrea
 		                                               b.entry_cap, &b.stats->err, b.sm, nullptr);
 }
 
+template <bool kBatch, int kWin>
+void pair_test_as(const BpBuffers &b, unsigned grid, cudaStream_t s) {
+	k_pair_test<kBatch, kWin><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+	                                               b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
+	                                               b.dense_cap, &b.stats->dense_items, &b.stats->err, b.dense_cell,
+	                                               b.owner_shift);
+}
+template <bool kBatch>
+void pair_test_window(const BpBuffers &b, unsigned grid, cudaStream_t s) {
+	switch (b.pair_window) {
+	case 64: pair_test_as<kBatch, 64>(b, grid, s); break;
+	case 128: pair_test_as<kBatch, 128>(b, grid, s); break;
+	default: pair_test_as<kBatch, kWinDefault>(b, grid, s); break;
+	}
+}
+
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s) {
 	(void)n;
 	uint64_t want = (entries_hint + kNT - 1) / kNT;
-	unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(want, 1), (uint64_t)kNumSMs * 8);
+	const uint64_t per_sm = b.pair_blocks_per_sm > 0 ? (uint64_t)b.pair_blocks_per_sm : 8;
+	unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(want, 1), (uint64_t)kNumSMs * per_sm);
 	if (b.sm.plans)
-		k_pair_test<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
-		                                       b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
-		                                       &b.stats->dense_items, &b.stats->err, b.dense_cell, b.owner_shift);
+		pair_test_window<true>(b, grid, s);
 	else
-		k_pair_test<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
-		                                        b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense, b.dense_cap,
-		                                        &b.stats->dense_items, &b.stats->err, b.dense_cell, b.owner_shift);
+		pair_test_window<false>(b, grid, s);
 	launch_pair_test_dense(b, s);
 }
 

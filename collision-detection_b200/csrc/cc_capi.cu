@@ -298,6 +298,8 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.dense_cell = c->gp.dense_cell;
 	b.owner_shift = c->owner_shift;
 	b.key_bits = c->key_bits;
+	b.pair_window = c->gp.pair_window;
+	b.pair_blocks_per_sm = c->gp.pair_blocks_per_sm;
 	return b;
 }
 
@@ -839,6 +841,8 @@ cc_status cc_ctx_create(cc_ctx **out, int device) {
 	c->gp.k_target = 4.0f;
 	c->gp.min_ratio = 2.0f;
 	c->gp.dense_cell = kDenseCell;
+	c->gp.pair_window = 96;
+	c->gp.pair_blocks_per_sm = 8;
 	c->gp.user_dim[0] = c->gp.user_dim[1] = c->gp.user_dim[2] = 0;
 	if (const char *v = getenv("CC_GRAPH_REPLAY")) c->graph_off = v[0] == '0';
 	if (cudaSetDevice(device) != cudaSuccess || cudaMallocHost(&c->h_stats, sizeof(DevStats)) != cudaSuccess ||
@@ -926,6 +930,17 @@ cc_status cc_set_incremental(cc_ctx *c, int on, float margin) {
 	c->incremental = on != 0;
 	c->inc_margin = margin;
 	c->inc_valid = false;
+	return CC_OK;
+}
+
+cc_status cc_set_pair_test_shape(cc_ctx *c, int window, int blocks_per_sm) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	if (window != 64 && window != 96 && window != 128)
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "pair-test window must be 64, 96 or 128");
+	if (blocks_per_sm < 1 || blocks_per_sm > 16)
+		return set_err(c, CC_ERR_INVALID_ARGUMENT, "pair-test blocks per SM must be 1..16");
+	c->gp.pair_window = window;
+	c->gp.pair_blocks_per_sm = blocks_per_sm;
 	return CC_OK;
 }
 

@@ -73,6 +73,8 @@ struct GridParams {
 	int user_dim[3];  // > 0: search on exactly this grid (tuner bypassed)
 	uint32_t g_max;   // capacity of the per-cell arrays
 	uint32_t dense_cell;  // cells holding more entries go to the tiled dense-cell pair test
+	int pair_window;        // sparse pair test: entries staged per warp (64, 96, 128)
+	int pair_blocks_per_sm; // sparse pair test: grid cap in blocks per SM
 };
 
 // Word ranges the first kernel of a pass zeroes (scan control words, class
@@ -159,6 +161,10 @@ struct BpBuffers {
 	// are the partner halves b (batches, incremental steps, the clustered scenes).
 	int owner_shift = 0;
 	int key_bits = 32;
+	// launch shape of the sparse pair test: entries staged per warp (64, 96 or
+	// 128) and the grid cap in blocks per SM
+	int pair_window = 96;
+	int pair_blocks_per_sm = 8;
 };
 // Owner buckets of n bodies at a shift.
 __host__ __device__ inline uint64_t owner_buckets(uint64_t n, int shift) {

@@ -156,6 +156,9 @@ extern "C" cc_status cc_broadphase_noalloc(uint64_t n, float *aabb, int gx, int 
 	gp.min_ratio = 2.0f;
 	gp.user_dim[0] = gp.user_dim[1] = gp.user_dim[2] = 0;
 	gp.g_max = b.g_max;
+	gp.dense_cell = kDenseCell;
+	gp.pair_window = b.pair_window;
+	gp.pair_blocks_per_sm = b.pair_blocks_per_sm;
 	const int grid[3] = {gx, gy, gz};
 
 	// everything that accumulates starts at zero (the array keeps the last call's contents)

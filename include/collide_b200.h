@@ -105,6 +105,11 @@ CC_API int cc_last_step_rebuilt(const cc_ctx *ctx);
  * of lane per entry. Pairs do not depend on it; the tuner picks it with the
  * grid. No reference counterpart. */
 CC_API cc_status cc_set_dense_cell(cc_ctx *ctx, uint32_t entries);
+/* Launch shape of the sparse pair test: `window` entries staged per warp in
+ * shared memory (64, 96 = default, or 128) and a grid cap of `blocks_per_sm`
+ * blocks per SM (1..16, default 8). Pairs do not depend on it; the tuner
+ * picks it. No reference counterpart. */
+CC_API cc_status cc_set_pair_test_shape(cc_ctx *ctx, int window, int blocks_per_sm);
 /* Narrowphase precision. The reference runs MPR in `real` (float). Here:
  *  CC_NP_EXACT (default): the reference's MPR arithmetic in FP64 in world
  *    coordinates, operation for operation — contacts equal those of the

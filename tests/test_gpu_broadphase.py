@@ -166,10 +166,15 @@ def test_tuner_picks_a_setting_and_pairs_do_not_change(cb):
 
     run()
     before = out["p"].clone()
-    best, table = tuner.tune(ctx, run, grid_candidates=((4.0, 2.0), (1.0, 1.0)), dense_candidates=(128, 0))
-    assert len(table) == 4 and best in [c for c, _ in table]
+    best, table = tuner.tune(ctx, run, grid_candidates=((4.0, 2.0), (1.0, 1.0)), dense_candidates=(128, 0),
+                             shape_candidates=((96, 8), (64, 16), (128, 5)))
+    assert len(table) == 6 and best in [c for c, _ in table]  # (96, 8) is the default shape: timed once
     run()
     assert torch.equal(out["p"], before)
+    for cand, _ in table:  # every candidate gives the same list
+        tuner.apply(ctx, cand)
+        run()
+        assert torch.equal(out["p"], before), cand
 
 
 def test_clustered_4m_sorted_unique_and_subboxes(cb):
