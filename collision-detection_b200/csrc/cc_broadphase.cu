@@ -811,15 +811,16 @@ __device__ __forceinline__ unsigned long long unpack_key(uint32_t v, uint32_t bu
 	return ((unsigned long long)a << 32) | (v & ((1u << kp.kb) - 1u));
 }
 
-constexpr int kSmallSeg = 32;
+constexpr int kSmallSeg = 8;  // buckets sorted by one thread in registers
 constexpr int kMidSeg = 1024;
 constexpr int kBigSeg = 16384;
 
 // Sorts each owner bucket (all keys share the bucket's owners, n here is the
-// bucket count): <= 32 keys by one thread in place on the 64-bit keys; longer
-// buckets are listed for k_segsort_mid (<= 1024 keys, from the front of
-// big_list) or k_segsort_big (<= 16384, from the back), which sort the packed
-// 32-bit keys (pack_key).
+// bucket count): <= 8 keys by one thread, loaded into registers at once and
+// sorted there by a static network on the 64-bit keys; longer buckets are
+// listed for k_segsort_mid (<= 1024 keys, from the front of big_list) or
+// k_segsort_big (<= 16384, from the back), which sort the packed 32-bit keys
+// (pack_key).
 __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long long *__restrict__ owner_off,
                                                   unsigned long long *__restrict__ out, uint32_t *big_list,
                                                   uint64_t big_cap, DevStats *stats) {
@@ -829,16 +830,21 @@ __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long
 	if (a < n) {
 		const uint64_t beg = owner_off[a], end = owner_off[a + 1];
 		len = end - beg;
-		if (len > 1 && len <= kSmallSeg) {  // insertion sort in place
-			for (uint64_t i = beg + 1; i < end; i++) {
-				const unsigned long long k = out[i];
-				uint64_t j = i;
-				while (j > beg && out[j - 1] > k) {
-					out[j] = out[j - 1];
-					j--;
+		if (len > 1 && len <= kSmallSeg) {
+			unsigned long long v[kSmallSeg];
+#pragma unroll
+			for (int q = 0; q < kSmallSeg; q++) v[q] = (uint64_t)q < len ? out[beg + q] : ~0ull;
+#pragma unroll
+			for (int r = 0; r < kSmallSeg - 1; r++)
+#pragma unroll
+				for (int q = 0; q < kSmallSeg - 1 - r; q++) {
+					const unsigned long long x = v[q], y = v[q + 1];
+					v[q] = x < y ? x : y;
+					v[q + 1] = x < y ? y : x;
 				}
-				out[j] = k;
-			}
+#pragma unroll
+			for (int q = 0; q < kSmallSeg; q++)
+				if ((uint64_t)q < len) out[beg + q] = v[q];
 		}
 	}
 	const bool longer = len > kSmallSeg;
@@ -992,8 +998,8 @@ __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict_
 	}
 }
 
-// Buckets of 33..1024 keys: one warp per bucket, sorted in registers
-// (2..32 keys per lane by bucket size); then buckets of 1025..2048 keys
+// Buckets of 9..1024 keys: one warp per bucket, sorted in registers
+// (1..32 keys per lane by bucket size); then buckets of 1025..2048 keys
 // (listed for k_segsort_big, which leaves them) on pairs of warps.
 constexpr int kMidNT = 256;
 __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
@@ -1006,8 +1012,9 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
 	const uint64_t warps = (uint64_t)gridDim.x * (kMidNT / 32);
 	for (uint64_t g = (uint64_t)blockIdx.x * (kMidNT / 32) + (threadIdx.x >> 5); g < nmid; g += warps) {
 		const uint32_t a = big_list[g];
-		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;  // 33..1024, listed by k_segsort
-		if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane, kp);
+		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;  // 9..1024, listed by k_segsort
+		if (len <= 32) sort_bucket_reg<1>(out, beg, len, a, lane, kp);
+		else if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane, kp);
 		else if (len <= 128) sort_bucket_reg<4>(out, beg, len, a, lane, kp);
 		else if (len <= 256) sort_bucket_reg<8>(out, beg, len, a, lane, kp);
 		else if (len <= 512) sort_bucket_reg<16>(out, beg, len, a, lane, kp);
