@@ -456,7 +456,7 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 			StageMark m(c, ST_SCAN_OWNER, s);
 			launch_scan_owner(n, b, s);
 		}
-		c->launches += 8;
+		c->launches += 9;  // with the dense-cell pair test
 		return;
 	}
 	c->inc_valid = false;  // the kept cell lists are overwritten
@@ -464,7 +464,7 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 		StageMark m(c, ST_FRONT, s);
 		if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
 		launch_front(n, aabb, b, ptr<unsigned long long>(c->front_sums), s);
-		c->launches -= 2;
+		c->launches -= 2;  // one launch for three stages
 	} else {
 		{
 			StageMark m(c, ST_COUNT, s);
@@ -488,7 +488,7 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 		StageMark m(c, ST_SCAN_OWNER, s);
 		launch_scan_owner(n, b, s);
 	}
-	c->launches += 5;
+	c->launches += 6;  // count, cell scan, scatter, sparse + dense pair test, owner scan
 }
 
 // Sorted pair list into `out` (device-driven: writes nothing if the pair
@@ -529,7 +529,7 @@ void enqueue_np(cc_ctx *c, const NpArgs &a, uint64_t P_cap, const unsigned long 
 		launch_np_compact(P_cap, P_dev, sc, reinterpret_cast<long long *>(a.pairs), a.norm, a.cpta, a.cptb, a.depth,
 		                  a.bids, &ptr<DevStats>(c->stats)->contacts, P_dev ? hint_P(c) : P_cap, s);
 	}
-	c->launches += 5;
+	c->launches += 3;  // class grouping, MPR, compaction
 }
 
 // Zeroes the per-pass counters before the passes after the count are redone.
@@ -570,7 +570,7 @@ cc_status settle(cc_ctx *c, uint64_t n, float *aabb, unsigned long long *out, ui
 		if (!keep_lists) launch_scatter(n, aabb, b, s);
 		launch_pair_test(n, b, E, s);
 		launch_scan_owner(n, b, s);
-		c->launches += 3;
+		c->launches += keep_lists ? 3 : 4;
 		if (out) enqueue_emit(c, n, out, out_cap, s);
 		if (np) enqueue_np(c, *np, out_cap, &ptr<DevStats>(c->stats)->np_n, s);
 		CC_TRY(check_launch(c));
