@@ -188,6 +188,11 @@ class Context:
         (0: never)."""
         self.check(lib.cc_set_dense_cell(self.h, int(entries)), "cc_set_dense_cell")
 
+    def set_narrowphase_overlap(self, on=True):
+        """Run cc_collide's MPR on the unsorted pairs while they are sorted
+        (identical results)."""
+        self.check(lib.cc_set_narrowphase_overlap(self.h, int(bool(on))), "cc_set_narrowphase_overlap")
+
     def set_pair_test_shape(self, window=96, blocks_per_sm=8):
         """Launch shape of the sparse pair test: entries staged per warp (64,
         96, 128) and the grid cap in blocks per SM."""

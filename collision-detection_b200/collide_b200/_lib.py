@@ -47,6 +47,7 @@ SIGNATURES = {
     "cc_set_tuning": (I32, [P, F32, F32]),
     "cc_set_dense_cell": (I32, [P, ctypes.c_uint32]),
     "cc_set_pair_test_shape": (I32, [P, I32, I32]),
+    "cc_set_narrowphase_overlap": (I32, [P, I32]),
     "cc_set_incremental": (I32, [P, I32, F32]),
     "cc_set_static_shapes": (I32, [P, I32]),
     "cc_last_step_rebuilt": (I32, [P]),

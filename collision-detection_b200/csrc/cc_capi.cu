@@ -73,6 +73,14 @@ struct cc_ctx {
 	Buf b_off, b_scene_of, b_gid, b_sst, b_plans, b_G, b_base, b_status, b_ticket, b_res;
 	// descriptor table of cc_perturb_scenes
 	Buf pt_desc;
+	// overlapped narrowphase (cc_set_narrowphase_overlap): the MPR on the
+	// unsorted pairs on np_stream while the main stream sorts them; the
+	// contact hash (keys, values) sized for 4x the expected pair count
+	bool np_overlap = false;
+	cudaStream_t np_stream = nullptr;
+	cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+	Buf np_hkeys, np_hvals;
+	uint64_t np_hslots = 0;
 	// gather arena of cc_collide_scenes
 	Buf g_T, g_A, g_B, g_C, g_R, g_ID, g_pos, g_rot, g_act, g_src, g_off;
 	SceneMap sm;  // set while a batch call runs
@@ -429,7 +437,8 @@ uint64_t hint_E(const cc_ctx *c, uint64_t n) { return pow2ceil(std::max<uint64_t
 uint64_t hint_P(const cc_ctx *c) { return pow2ceil(std::max<uint64_t>(c->last_P, 1)); }
 
 // count .. owner scan: needs stats zeroed and the plan from the bounds pass.
-void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool incremental = false) {
+void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool incremental = false,
+                    bool owner_scan = true) {
 	BpBuffers b = bp_buffers(c);
 	const uint32_t gmax = c->gp.g_max;
 	if (incremental) {
@@ -484,11 +493,11 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 		StageMark m(c, ST_PAIR_TEST, s);
 		launch_pair_test(n, b, hint_E(c, n), s);
 	}
-	{
+	if (owner_scan) {
 		StageMark m(c, ST_SCAN_OWNER, s);
 		launch_scan_owner(n, b, s);
 	}
-	c->launches += 6;  // count, cell scan, scatter, sparse + dense pair test, owner scan
+	c->launches += owner_scan ? 6 : 5;  // count, cell scan, scatter, sparse + dense pair test, owner scan
 }
 
 // Sorted pair list into `out` (device-driven: writes nothing if the pair
@@ -530,6 +539,43 @@ void enqueue_np(cc_ctx *c, const NpArgs &a, uint64_t P_cap, const unsigned long 
 		                  a.bids, &ptr<DevStats>(c->stats)->contacts, P_dev ? hint_P(c) : P_cap, s);
 	}
 	c->launches += 3;  // class grouping, MPR, compaction
+}
+
+// The step after the pair test with the narrowphase overlapped (one scene):
+// the MPR runs on the unsorted pairs on c->np_stream (forked after the pair
+// test) while `s` sorts them into a.pairs; the compaction joins both and
+// finds each sorted key's result through the contact hash.
+cc_status enqueue_sort_and_np_overlapped(cc_ctx *c, uint64_t n, const NpArgs &a, uint64_t pairs_cap,
+                                         cudaStream_t s) {
+	DevStats *d = ptr<DevStats>(c->stats);
+	BpBuffers b = bp_buffers(c);
+	NpScratch sc = np_scratch(c);
+	sc.hkeys = ptr<unsigned long long>(c->np_hkeys);
+	sc.hvals = ptr<uint32_t>(c->np_hvals);
+	sc.hmask = c->np_hslots - 1;
+	CC_CUDA(c, cudaEventRecord(c->ev_fork, s));
+	CC_CUDA(c, cudaStreamWaitEvent(c->np_stream, c->ev_fork, 0));
+	{
+		StageMark m(c, ST_MPR, c->np_stream);
+		launch_mpr(std::min<uint64_t>(pairs_cap, b.pair_cap), &d->pairs, a.n, a.T, a.A, a.B, a.C, a.R, a.ID, a.nb,
+		           a.active, a.pos, a.rot, a.envelope, reinterpret_cast<const long long *>(b.pairs_tmp), sc,
+		           c->np_precision, hint_P(c), c->np_stream);
+	}
+	CC_CUDA(c, cudaEventRecord(c->ev_join, c->np_stream));
+	{
+		StageMark m(c, ST_SCAN_OWNER, s);
+		launch_scan_owner(n, b, s);
+	}
+	c->launches += 3;  // owner scan, class grouping, MPR
+	enqueue_emit(c, n, reinterpret_cast<unsigned long long *>(a.pairs), pairs_cap, s);
+	CC_CUDA(c, cudaStreamWaitEvent(s, c->ev_join, 0));
+	{
+		StageMark m(c, ST_NP_COMPACT, s);
+		launch_np_compact_sorted(pairs_cap, &d->np_n, sc, reinterpret_cast<long long *>(a.pairs), b.pairs_tmp,
+		                         a.norm, a.cpta, a.cptb, a.depth, a.bids, &d->contacts, hint_P(c), s);
+	}
+	c->launches += 1;
+	return CC_OK;
 }
 
 // Zeroes the per-pass counters before the passes after the count are redone.
@@ -711,6 +757,16 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 		CC_TRY(ensure(c, c->inc_state, sizeof(IncState)));
 	}
 	const bool inc_ready = inc && c->inc_valid && c->inc_n == n && c->inc_gen == c->buf_gen;
+	// overlapped narrowphase: one scene, an output of at most 2^24 pairs
+	const bool ov = c->np_overlap && pairs_cap > 0 && pairs_cap <= ((uint64_t)1 << 24);
+	if (ov) {
+		if (!c->np_stream) CC_CUDA(c, cudaStreamCreateWithFlags(&c->np_stream, cudaStreamNonBlocking));
+		if (!c->ev_fork) CC_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+		if (!c->ev_join) CC_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+		c->np_hslots = pow2ceil(std::max<uint64_t>(4 * std::min<uint64_t>(hint_P(c), pairs_cap), 4096));
+		CC_TRY(ensure(c, c->np_hkeys, sizeof(unsigned long long) * c->np_hslots));
+		CC_TRY(ensure(c, c->np_hvals, sizeof(uint32_t) * c->np_hslots));
+	}
 	c->inc_valid = false;  // set again once this step has finished cleanly
 	DevStats *d = ptr<DevStats>(c->stats);
 	const int grid[3] = {gx, gy, gz};
@@ -728,7 +784,11 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	zero.words[2] = 2 * kNpClasses + 1;
 	zero.p[3] = ptr<uint32_t>(c->cell_count);
 	zero.words[3] = c->gp.g_max;
-	for (int r = 0; r < 4; r++)
+	if (ov) {  // the contact hash starts empty
+		zero.p[4] = ptr<uint32_t>(c->np_hkeys);
+		zero.words[4] = 2 * c->np_hslots;
+	}
+	for (int r = 0; r < 5; r++)
 		if (!zero.p[r]) zero.words[r] = 0;
 	auto enqueue_all = [&](cudaStream_t st) -> cc_status {
 		{
@@ -740,6 +800,12 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 		}
 		c->launches += 1;
 		c->pass_zeroed = true;
+		if (ov) {
+			enqueue_search(c, n, aabb, st, inc, false);
+			const cc_status r = enqueue_sort_and_np_overlapped(c, n, a, pairs_cap, st);
+			c->pass_zeroed = false;
+			return r;
+		}
 		enqueue_search(c, n, aabb, st, inc);
 		enqueue_emit(c, n, out, pairs_cap, st);
 		enqueue_np(c, a, pairs_cap, &d->np_n, st);
@@ -754,9 +820,10 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	struct {
 		uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
 		const void *p[18];
-		int dims[3], prec, oshift, kbits;
+		int dims[3], prec, oshift, kbits, ov;
 		float env;
 		GridParams gp;
+		uint64_t hslots;
 	} k;
 	memset(&k, 0, sizeof(k));
 	k.n = n; k.nb = sc.nb; k.pairs_cap = pairs_cap; k.hE = hint_E(c, n); k.hP = hint_P(c); k.gen = c->buf_gen;
@@ -766,7 +833,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	                      pairs, norm, cpta, cptb, depth, bids, nullptr, nullptr};
 	memcpy(k.p, ps, sizeof(ps));
 	k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.env = envelope; k.gp = c->gp;
-	k.oshift = c->owner_shift; k.kbits = c->key_bits;
+	k.oshift = c->owner_shift; k.kbits = c->key_bits; k.ov = ov ? 1 : 0; k.hslots = ov ? c->np_hslots : 0;
 	return run_graphed(c, c->g_collide, &k, sizeof(k), enqueue_all, s);
 }
 
@@ -793,6 +860,14 @@ cc_status collide_finish(cc_ctx *c, const cc_scene &sc, float envelope, float *a
 	if (c->h_stats->err & kErrSegmentTooLong) {
 		// the list was sorted bucket-wise only up to 4096 per bucket: sort it whole, redo the narrowphase
 		CC_TRY(sort_fallback(c, n, P, out, s));
+		CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
+		enqueue_np(c, a, pairs_cap, &d->np_n, s);
+		CC_TRY(check_launch(c));
+		CC_TRY(read_stats(c, s));
+	} else if (c->h_stats->err & kErrHashFull) {
+		// more contacts than the overlapped narrowphase's hash took: run it again on the sorted list,
+		// which its compaction kept in the unsorted-pair scratch before permuting the output
+		CC_CUDA(c, cudaMemcpyAsync(out, c->pairs_tmp.p, sizeof(unsigned long long) * P, cudaMemcpyDeviceToDevice, s));
 		CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
 		enqueue_np(c, a, pairs_cap, &d->np_n, s);
 		CC_TRY(check_launch(c));
@@ -869,12 +944,15 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
 	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges, &c->front_sums,
-	               &c->np_bsum,  &c->pt_desc};
+	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
 	c->g_collide.drop();
 	c->g_batch.drop();
 	if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+	if (c->np_stream) cudaStreamDestroy(c->np_stream);
+	if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+	if (c->ev_join) cudaEventDestroy(c->ev_join);
 	for (auto &h : c->hs) {
 		Buf *hb[] = {&h.T, &h.A, &h.B, &h.C, &h.R, &h.ID, &h.pos, &h.rot, &h.act, &h.aabb, &h.pairs, &h.norm, &h.pa,
 		             &h.pb, &h.depth, &h.bids};
@@ -930,6 +1008,12 @@ cc_status cc_set_incremental(cc_ctx *c, int on, float margin) {
 	c->incremental = on != 0;
 	c->inc_margin = margin;
 	c->inc_valid = false;
+	return CC_OK;
+}
+
+cc_status cc_set_narrowphase_overlap(cc_ctx *c, int on) {
+	if (!c) return CC_ERR_INVALID_ARGUMENT;
+	c->np_overlap = on != 0;
 	return CC_OK;
 }
 

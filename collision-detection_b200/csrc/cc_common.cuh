@@ -18,6 +18,7 @@ enum DeviceError : uint32_t {
 	kErrSegmentTooLong = 1u << 4,  // a pair segment exceeded the block sort size (host falls back)
 	kErrBinCount = 1u << 5,      // a body covers a negative / overflowing number of reference bins
 	kErrBadIndex = 1u << 6,      // a body id >= nb or a pair index >= n (the access is skipped)
+	kErrHashFull = 1u << 7,      // the overlapped narrowphase's contact hash overflowed (host redoes it in order)
 };
 
 // Order-preserving map float -> uint32 (for atomicMin/atomicMax reductions).
@@ -185,7 +186,7 @@ template <class ZL>
 __device__ __forceinline__ void zero_ranges(const ZL &z) {
 	const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, step = (uint64_t)gridDim.x * blockDim.x;
 #pragma unroll
-	for (int r = 0; r < 4; r++)
+	for (int r = 0; r < 5; r++)
 		for (uint64_t i = t; i < z.words[r]; i += step) z.p[r][i] = 0u;
 }
 

@@ -80,8 +80,8 @@ struct GridParams {
 // Word ranges the first kernel of a pass zeroes (scan control words, class
 // counters, cell counts), replacing a chain of memset launches.
 struct ZeroList {
-	uint32_t *p[4] = {nullptr, nullptr, nullptr, nullptr};
-	uint64_t words[4] = {0, 0, 0, 0};
+	uint32_t *p[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+	uint64_t words[5] = {0, 0, 0, 0, 0};
 };
 
 // ------------------------------------------------------------------ scan
@@ -290,6 +290,13 @@ struct NpScratch {
 	void *bar_classes = nullptr;  // grid barriers (GridBarrier) of the cooperative class sort and compaction,
 	void *bar_compact = nullptr;  // zeroed at the start of the call
 	unsigned long long *block_sums = nullptr;  // per-block flag counts of the compaction (>= its grid)
+	// Overlapped narrowphase (the MPR on the unsorted pairs while they are
+	// sorted): every contact's key -> its pair index, open addressing with
+	// linear probing over hmask + 1 slots (0 = empty, else key + 1), zeroed at
+	// the start of the pass. Null: the MPR runs on the sorted list.
+	unsigned long long *hkeys = nullptr;
+	uint32_t *hvals = nullptr;
+	uint64_t hmask = 0;
 };
 constexpr int kNpClasses = 64;  // 7 x 7 shape-type combinations + one for invalid keys
 // Grid bound of the narrowphase's cooperative kernels (and the size of
@@ -315,5 +322,14 @@ void launch_mpr_exact(unsigned grid, uint64_t P_cap, const unsigned long long *P
 void launch_np_compact(uint64_t P_cap, const unsigned long long *P_dev, const NpScratch &sc, long long *pairs,
                        float *norm, float *cpta, float *cptb, float *depth, int32_t *bids,
                        unsigned long long *contacts_out, uint64_t P_hint, cudaStream_t s);
+// The overlapped narrowphase's compaction: the MPR ran on the unsorted pairs
+// (results at their unsorted index, contacts in sc's hash); `pairs` holds the
+// sorted list of *P_dev keys. Writes the hit-first order into `pairs` and the
+// contacts in that order, exactly as launch_np_compact does after an MPR on
+// the sorted list. tmp: P_cap keys of scratch.
+void launch_np_compact_sorted(uint64_t P_cap, const unsigned long long *P_dev, const NpScratch &sc,
+                              long long *pairs, unsigned long long *tmp, float *norm, float *cpta, float *cptb,
+                              float *depth, int32_t *bids, unsigned long long *contacts_out, uint64_t P_hint,
+                              cudaStream_t s);
 
 }  // namespace cc

@@ -313,6 +313,20 @@ __device__ __forceinline__ void write_contact(const Lane<S, kExact> &L, D3 N, D3
 	sc.ids[2 * i] = (int32_t)ida;
 	sc.ids[2 * i + 1] = (int32_t)idb;
 	sc.flag[i] = 1u;
+	if (sc.hkeys) {  // overlapped narrowphase: key -> i for the compaction in sorted order
+		const unsigned long long tag = sc.pairs[i] + 1ull;
+		uint64_t h = (tag * 0x9E3779B97F4A7C15ull) >> 20;
+		bool placed = false;
+		for (uint64_t probe = 0; probe <= sc.hmask && probe < 256; probe++, h++) {
+			const uint64_t slot = h & sc.hmask;
+			if (atomicCAS(&sc.hkeys[slot], 0ull, tag) == 0ull) {
+				sc.hvals[slot] = (uint32_t)i;
+				placed = true;
+				break;
+			}
+		}
+		if (!placed) atomicOr(sc.err, (uint32_t)kErrHashFull);
+	}
 }
 
 // Starts pair i: the checks and transforms of :338-377; sphere-sphere pairs

@@ -189,6 +189,92 @@ __global__ void __launch_bounds__(kCoopNT) k_np_compact_coop(uint64_t P_cap, con
 	}
 }
 
+// The overlapped narrowphase's compaction (one cooperative launch): the MPR
+// ran on the unsorted pairs, so each sorted key finds its result through the
+// contact hash. Phase 1: block b copies its chunk of sorted keys to `tmp`,
+// looks each one up and counts its hits; grid barrier; phase 2: it adds the
+// counts of the blocks before it and writes the hit-first order and the
+// contacts, as k_np_compact_coop does for results in sorted order.
+__device__ __forceinline__ uint32_t hash_find(const NpScratch &sc, unsigned long long key) {
+	const unsigned long long tag = key + 1ull;
+	uint64_t h = (tag * 0x9E3779B97F4A7C15ull) >> 20;
+	for (uint64_t probe = 0; probe <= sc.hmask && probe < 256; probe++, h++) {
+		const unsigned long long v = __ldcg(&sc.hkeys[h & sc.hmask]);
+		if (v == tag) return __ldcg(&sc.hvals[h & sc.hmask]);
+		if (v == 0ull) break;
+	}
+	return 0xffffffffu;
+}
+
+__global__ void __launch_bounds__(kCoopNT) k_np_compact_sorted(uint64_t P_cap, const unsigned long long *P_dev,
+                                                                NpScratch sc, long long *__restrict__ pairs,
+                                                                unsigned long long *__restrict__ tmp,
+                                                                float *__restrict__ norm, float *__restrict__ cpta,
+                                                                float *__restrict__ cptb, float *__restrict__ depth,
+                                                                int32_t *__restrict__ bids,
+                                                                unsigned long long *contacts_out) {
+	__shared__ unsigned long long sm[40];
+	__shared__ unsigned long long s_pre, s_total;
+	const uint64_t P = P_dev ? min(P_cap, (uint64_t)*P_dev) : P_cap;
+	const uint64_t chunk = (P + gridDim.x - 1) / gridDim.x;
+	const uint64_t c0 = min((uint64_t)blockIdx.x * chunk, P), c1 = min(c0 + chunk, P);
+	unsigned long long cnt = 0;
+	for (uint64_t i = c0 + threadIdx.x; i < c1; i += kCoopNT) {
+		const unsigned long long key = (unsigned long long)pairs[i];
+		tmp[i] = key;
+		const uint32_t t = hash_find(sc, key);
+		sc.order[i] = t;
+		cnt += t != 0xffffffffu ? 1ull : 0ull;
+	}
+	unsigned long long tot;
+	block_excl_scan<unsigned long long, kCoopNT>(cnt, sm, &tot);
+	if (threadIdx.x == 0) sc.block_sums[blockIdx.x] = tot;
+	grid_barrier(reinterpret_cast<GridBarrier *>(sc.bar_compact), sc.err);
+	{
+		unsigned long long pre = 0, all = 0, t1, t2;
+		for (uint32_t b = threadIdx.x; b < gridDim.x; b += kCoopNT) {
+			const unsigned long long v = __ldcg(&sc.block_sums[b]);
+			all += v;
+			if (b < blockIdx.x) pre += v;
+		}
+		block_excl_scan<unsigned long long, kCoopNT>(pre, sm, &t1);
+		block_excl_scan<unsigned long long, kCoopNT>(all, sm, &t2);
+		if (threadIdx.x == 0) {
+			s_pre = t1;
+			s_total = t2;
+		}
+		__syncthreads();
+	}
+	unsigned long long run = s_pre;
+	const unsigned long long nh = s_total;
+	if (blockIdx.x == 0 && threadIdx.x == 0 && contacts_out) *contacts_out = nh;
+	for (uint64_t t0 = c0; t0 < c1; t0 += kCoopNT) {
+		const uint64_t i = t0 + threadIdx.x;
+		const uint32_t t = i < c1 ? sc.order[i] : 0xffffffffu;
+		const unsigned long long f = t != 0xffffffffu ? 1ull : 0ull;
+		unsigned long long tile_total;
+		const unsigned long long ex = block_excl_scan<unsigned long long, kCoopNT>(f, sm, &tile_total);
+		if (i < c1) {
+			const uint64_t before = run + ex;
+			if (f) {
+				const uint64_t j = before;
+				pairs[j] = (long long)tmp[i];
+				for (int d = 0; d < 3; d++) {
+					norm[3 * j + d] = sc.norm[3 * (uint64_t)t + d];
+					cpta[3 * j + d] = sc.pa[3 * (uint64_t)t + d];
+					cptb[3 * j + d] = sc.pb[3 * (uint64_t)t + d];
+				}
+				depth[j] = sc.depth[t];
+				bids[2 * j] = sc.ids[2 * (uint64_t)t];
+				bids[2 * j + 1] = sc.ids[2 * (uint64_t)t + 1];
+			} else {
+				pairs[nh + (i - before)] = (long long)tmp[i];
+			}
+		}
+		run += tile_total;
+	}
+}
+
 __device__ __forceinline__ void compact_one(uint64_t i, uint64_t P, const NpScratch &sc, long long *__restrict__ pairs,
                                             float *__restrict__ norm, float *__restrict__ cpta,
                                             float *__restrict__ cptb, float *__restrict__ depth,
@@ -242,7 +328,8 @@ void launch_coop(void (*k)(A...), unsigned grid, cudaStream_t s, A... args) {
 }  // namespace
 
 unsigned np_coop_max_blocks() {
-	static const unsigned m = std::min(coop_blocks(k_np_classes), coop_blocks(k_np_compact_coop));
+	static const unsigned m = std::min(std::min(coop_blocks(k_np_classes), coop_blocks(k_np_compact_coop)),
+	                                   coop_blocks(k_np_compact_sorted));
 	return m;
 }
 
@@ -289,6 +376,21 @@ void launch_np_compact(uint64_t P_cap, const unsigned long long *P_dev, const Np
 	const unsigned grid = (unsigned)std::max<uint64_t>(
 	    1, std::min<uint64_t>((Pe + 1023) / 1024, std::min<uint64_t>(np_coop_max_blocks(), kNpCoopBlocks)));
 	launch_coop(k_np_compact_coop, grid, s, P_cap, P_dev, sc, pairs, norm, cpta, cptb, depth, bids, contacts_out);
+}
+
+void launch_np_compact_sorted(uint64_t P_cap, const unsigned long long *P_dev, const NpScratch &sc,
+                              long long *pairs, unsigned long long *tmp, float *norm, float *cpta, float *cptb,
+                              float *depth, int32_t *bids, unsigned long long *contacts_out, uint64_t P_hint,
+                              cudaStream_t s) {
+	if (!P_cap) {
+		if (contacts_out) cudaMemsetAsync(contacts_out, 0, sizeof(unsigned long long), s);
+		return;
+	}
+	const uint64_t Pe = std::min<uint64_t>(P_hint ? P_hint : P_cap, P_cap);
+	const unsigned grid = (unsigned)std::max<uint64_t>(
+	    1, std::min<uint64_t>((Pe + 1023) / 1024, std::min<uint64_t>(np_coop_max_blocks(), kNpCoopBlocks)));
+	launch_coop(k_np_compact_sorted, grid, s, P_cap, P_dev, sc, pairs, tmp, norm, cpta, cptb, depth, bids,
+	            contacts_out);
 }
 
 }  // namespace cc

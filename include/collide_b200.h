@@ -119,6 +119,13 @@ CC_API cc_status cc_set_pair_test_shape(cc_ctx *ctx, int window, int blocks_per_
  *  CC_NP_MIXED: as CC_NP_FP64 but FP32 support maps. */
 enum { CC_NP_EXACT = 0, CC_NP_FP64 = 1, CC_NP_MIXED = 2 };
 CC_API cc_status cc_set_narrowphase_precision(cc_ctx *ctx, int mode);
+/* Overlapped narrowphase for cc_collide (default off): after the pair test
+ * the MPR runs on the unsorted pair list on a second stream while the list is
+ * sorted, and the compaction joins both in sorted order, finding each pair's
+ * result through a hash of the contacts. Results are identical either way
+ * (a step whose contacts overflow the hash is redone in order). Applies to
+ * outputs of at most 2^24 pairs. No reference counterpart. */
+CC_API cc_status cc_set_narrowphase_overlap(cc_ctx *ctx, int on);
 /* CUDA-graph replay of cc_collide (default on; environment CC_GRAPH_REPLAY=0
  * turns it off at context creation). When the same configuration (sizes,
  * pointers, grid, precision, envelope, tuning) reaches cc_collide twice in a
