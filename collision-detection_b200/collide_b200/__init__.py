@@ -188,10 +188,14 @@ class Context:
         (0: never)."""
         self.check(lib.cc_set_dense_cell(self.h, int(entries)), "cc_set_dense_cell")
 
+    def narrowphase_overlap(self):
+        return bool(getattr(self, "_np_overlap", False))
+
     def set_narrowphase_overlap(self, on=True):
         """Run cc_collide's MPR on the unsorted pairs while they are sorted
         (identical results)."""
         self.check(lib.cc_set_narrowphase_overlap(self.h, int(bool(on))), "cc_set_narrowphase_overlap")
+        self._np_overlap = bool(on)
 
     def set_pair_test_shape(self, window=96, blocks_per_sm=8):
         """Launch shape of the sparse pair test: entries staged per warp (64,
