@@ -89,8 +89,6 @@ STAGE_BYTES = {
     "count": lambda N, E, G, P, C: 48 * N + 4 * G,     # shift in place (24 r + 24 w) + cell counts
     "scan_cells": lambda N, E, G, P, C: 8 * G,
     "scatter": lambda N, E, G, P, C: 24 * N + 4 * G + 32 * E,
-    # shift + count, cell scan and scatter fused in one cooperative launch
-    "front": lambda N, E, G, P, C: (48 * N + 4 * G) + 8 * G + (24 * N + 4 * G + 32 * E),
     "pair_test": lambda N, E, G, P, C: 32 * E + 4 * G + 8 * P + 4 * N,
     "scan_owner": lambda N, E, G, P, C: 12 * N,
     "owner_scatter": lambda N, E, G, P, C: 16 * P + 8 * N,
@@ -102,7 +100,7 @@ STAGE_BYTES = {
 
 # Stages of the broadphase proper (detectPossibleCollisions after the AABBs),
 # in pipeline order; stages absent from a run are skipped.
-BP_STAGES = ("front", "count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
+BP_STAGES = ("count", "scan_cells", "scatter", "pair_test", "scan_owner", "owner_scatter", "segsort")
 STAGE_TIERS = {"segsort": ("segsort_mid", "segsort_big")}
 
 
@@ -173,7 +171,9 @@ def bench_batched(cb, ctx, dev, steps=10):
     e1.record()
     torch.cuda.synchronize()
     tl = e0.elapsed_time(e1)
-    del pipes
+    del pipes, bctx
+    import gc
+    gc.collect()
     torch.cuda.empty_cache()
     return {"workload": BATCH_WORKLOAD, "scenes": 512, "bodies": N, "pairs": P, "contacts": C,
             "ms_per_batch": tb, "value": N / (tb / 1000.0), "unit": "bodies/s",
@@ -357,7 +357,9 @@ def bench_served(cb, dev, seconds):
         out[mode] = r
         del srv
     del pool
+    import gc
     import torch
+    gc.collect()  # the servers (arena, contexts) go now, not at some later collection
     torch.cuda.empty_cache()  # the servers' reserved working set goes back before the clustered run
     out["p99_ratio_plain_over_batched"] = out["plain"]["p99_ms"] / out["batched"]["p99_ms"]
     out["p99_ratio_plain_over_batched_at_4000_qps"] = (out["plain"]["at_4000_qps"]["p99_ms"] /

@@ -264,15 +264,15 @@ class Server:
         place = ps.device_bytes()
 
         # evict least recently used idle scenes until the scene fits the
-        # budget and a free range of the arena
-        victims = (s for s in list(self.resident) if s not in pinned)
+        # budget and a free range of the arena; the oldest idle scene is found
+        # from the front of the LRU order, skipping only the pinned ones
         at = None
         while True:
             if self.bytes + need <= self.budget:
                 at = self.arena.take(place) if self.arena is not None else -1
                 if at is not None:
                     break
-            sid = next(victims, None)
+            sid = next((s for s in self.resident if s not in pinned), None)
             if sid is None:
                 self.rejected += 1
                 return None

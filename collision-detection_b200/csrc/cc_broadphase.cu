@@ -345,149 +345,6 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 	if (over) atomicOr(err, (uint32_t)kErrCapacity);
 }
 
-// ---- the single-scene front of the broadphase as one cooperative launch
-// (all blocks resident): in-place shift + per-cell counts, the cell scan
-// (block sums, grid barrier, block prefixes) and the scatter, separated by
-// bounded grid barriers instead of kernel boundaries. Data another block wrote
-// earlier in the launch (boxes, counts, offsets) is read with ld.global.cg,
-// from L2. Same results as k_count + scan + k_scatter.
-__device__ __forceinline__ void load_tile_aabb_cg(const float *__restrict__ aabb, uint64_t n, uint64_t i0, float *stage) {
-	if (tile_vec_ok(aabb, n, i0)) {
-		const float4 *lo = reinterpret_cast<const float4 *>(aabb + 3 * i0);
-		const float4 *hi = reinterpret_cast<const float4 *>(aabb + 3 * (n + i0));
-		float4 *st = reinterpret_cast<float4 *>(stage);
-		for (int k = threadIdx.x; k < 3 * kNT / 4; k += kNT) {
-			st[k] = __ldcg(lo + k);
-			st[3 * kNT / 4 + k] = __ldcg(hi + k);
-		}
-	} else {
-		const uint64_t m = i0 < n ? min((uint64_t)kNT, n - i0) : 0;
-		for (int k = threadIdx.x; k < 3 * (int)m; k += kNT) {
-			stage[k] = __ldcg(aabb + 3 * i0 + k);
-			stage[3 * kNT + k] = __ldcg(aabb + 3 * (n + i0) + k);
-		}
-	}
-}
-
-struct FrontArgs {
-	uint64_t n;
-	float *aabb;
-	DevStats *stats;
-	uint32_t *cell_count, *cell_start, *owner_count;
-	float4 *entries;
-	uint64_t entry_cap;
-	unsigned long long *block_sums;  // >= gridDim.x
-	int oshift;
-};
-
-__global__ void __launch_bounds__(kNT) k_front(FrontArgs a) {
-	__shared__ Plan sp;
-	__shared__ __align__(16) float stage[6 * kNT];
-	__shared__ unsigned long long sm[40];
-	__shared__ unsigned long long s_pre, s_total;
-	GridBarrier *bar = reinterpret_cast<GridBarrier *>(a.stats->bar_front);
-	uint32_t *err = &a.stats->err;
-	if (threadIdx.x < sizeof(Plan) / 4)
-		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = __ldcg(reinterpret_cast<const uint32_t *>(&a.stats->plan) + threadIdx.x);
-	__syncthreads();
-	if (!sp.valid) return;  // invalid input (uniform over the grid): nothing is modified
-	const uint64_t n = a.n, ntiles = (n + kNT - 1) / kNT;
-
-	// 1. shift in place (:382-386) and count cell entries
-	for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-		const uint64_t i0 = tile * kNT;
-		__syncthreads();  // the previous tile's stage is no longer read
-		load_tile_aabb(a.aabb, n, i0, stage);
-		__syncthreads();
-		for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
-		__syncthreads();
-		store_tile_aabb(a.aabb, n, i0, stage);
-		const uint64_t i = i0 + threadIdx.x;
-		if (i < n) {
-			const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
-			const float *hs = stage + 3 * kNT;
-			const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
-			if ((i & ((1ull << a.oshift) - 1)) == 0) a.owner_count[i >> a.oshift] = 0u;
-			const CellRange r = cell_range(sp, mn, mx);
-			for (int z = r.c0[2]; z <= r.c1[2]; z++)
-				for (int y = r.c0[1]; y <= r.c1[1]; y++)
-					for (int x = r.c0[0]; x <= r.c1[0]; x++) atomicAdd(&a.cell_count[cell_index(sp, 0, x, y, z)], 1u);
-		}
-	}
-	grid_barrier(bar, err);
-
-	// 2. cell offsets: block b scans the contiguous chunk b of the G cells
-	const uint64_t G = sp.G;
-	const uint64_t chunk = (G + gridDim.x - 1) / gridDim.x;
-	const uint64_t c0 = min((uint64_t)blockIdx.x * chunk, G), c1 = min(c0 + chunk, G);
-	unsigned long long cnt = 0;
-	for (uint64_t c = c0 + threadIdx.x; c < c1; c += kNT) cnt += __ldcg(a.cell_count + c);
-	unsigned long long tot;
-	block_excl_scan<unsigned long long, kNT>(cnt, sm, &tot);
-	if (threadIdx.x == 0) a.block_sums[blockIdx.x] = tot;
-	grid_barrier(bar, err);
-	{
-		unsigned long long pre = 0, all = 0, t1, t2;
-		for (uint32_t b = threadIdx.x; b < gridDim.x; b += kNT) {
-			const unsigned long long v = __ldcg(a.block_sums + b);
-			all += v;
-			if (b < blockIdx.x) pre += v;
-		}
-		block_excl_scan<unsigned long long, kNT>(pre, sm, &t1);
-		block_excl_scan<unsigned long long, kNT>(all, sm, &t2);
-		if (threadIdx.x == 0) {
-			s_pre = t1;
-			s_total = t2;
-		}
-		__syncthreads();
-	}
-	unsigned long long run = s_pre;
-	if (blockIdx.x == 0 && threadIdx.x == 0) {
-		a.cell_start[G] = (uint32_t)s_total;
-		a.stats->entries = s_total;
-	}
-	for (uint64_t t0 = c0; t0 < c1; t0 += kNT) {
-		const uint64_t c = t0 + threadIdx.x;
-		const unsigned long long v = c < c1 ? __ldcg(a.cell_count + c) : 0ull;
-		unsigned long long tt;
-		const unsigned long long ex = block_excl_scan<unsigned long long, kNT>(v, sm, &tt);
-		if (c < c1) {
-			a.cell_start[c] = (uint32_t)(run + ex);
-			a.cell_count[c] = 0u;  // the scatter's cursor
-		}
-		run += tt;
-	}
-	grid_barrier(bar, err);
-
-	// 3. cell-ordered entries (as k_scatter)
-	bool over = false;
-	for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-		const uint64_t i0 = tile * kNT;
-		__syncthreads();
-		load_tile_aabb_cg(a.aabb, n, i0, stage);
-		__syncthreads();
-		const uint64_t i = i0 + threadIdx.x;
-		if (i >= n) continue;
-		const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
-		const float *hs = stage + 3 * kNT;
-		const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
-		const CellRange r = cell_range(sp, mn, mx);
-		for (int z = r.c0[2]; z <= r.c1[2]; z++)
-			for (int y = r.c0[1]; y <= r.c1[1]; y++)
-				for (int x = r.c0[0]; x <= r.c1[0]; x++) {
-					const uint32_t c = cell_index(sp, 0, x, y, z);
-					const uint64_t slot = (uint64_t)__ldcg(a.cell_start + c) + atomicAdd(&a.cell_count[c], 1u);
-					if (slot < a.entry_cap) {
-						a.entries[2 * slot] = make_float4(mn.x, mn.y, mn.z, __uint_as_float((uint32_t)i));
-						a.entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(pack_cell(x, y, z)));
-					} else {
-						over = true;
-					}
-				}
-	}
-	if (over) atomicOr(err, (uint32_t)kErrCapacity);
-}
-
 // Each entry is tested against the later entries of its cell; a warp takes
 // 32 entries and deals their tests out evenly over its lanes (so a warp's
 // rounds follow the SUM of its entries' partner counts, not 32 x the largest). A warp's 32 entries and the kWin - 32 that follow them are
@@ -1211,36 +1068,6 @@ void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cud
 	else
 		pair_test_window<false>(b, grid, s);
 	launch_pair_test_dense(b, s);
-}
-
-unsigned front_max_blocks() {
-	static const unsigned m = [] {
-		int per_sm = 0, dev = 0, sms = kNumSMs;
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_front, kNT, 0) != cudaSuccess || per_sm < 1)
-			per_sm = 1;
-		if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		return (unsigned)std::min<int>(per_sm * sms, (int)kFrontMaxBlocks);
-	}();
-	return m;
-}
-
-void launch_front(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *block_sums, cudaStream_t s) {
-	if (!n) return;
-	FrontArgs a;
-	a.n = n;
-	a.aabb = aabb;
-	a.stats = b.stats;
-	a.cell_count = b.cell_count;
-	a.cell_start = b.cell_start;
-	a.owner_count = b.owner_count;
-	a.entries = b.entries;
-	a.entry_cap = b.entry_cap;
-	a.block_sums = block_sums;
-	a.oshift = b.owner_shift;
-	// enough blocks for every tile, up to one full wave of resident blocks
-	const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(blocks_for(n), front_max_blocks()));
-	void *args[] = {&a};
-	cudaLaunchCooperativeKernel((const void *)k_front, dim3(grid), dim3(kNT), args, 0, s);
 }
 
 void launch_count_inc(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s) {

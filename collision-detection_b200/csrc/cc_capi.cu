@@ -29,12 +29,11 @@ struct Buf {
 // Kernel stages timed by the optional profiler.
 enum Stage : int {
 	ST_AABB, ST_BOUNDS, ST_COUNT, ST_SCAN_CELLS, ST_SCATTER, ST_PAIR_TEST, ST_SCAN_OWNER, ST_OWNER_SCATTER,
-	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_SEGSORT_MID, ST_SEGSORT_BIG, ST_FRONT,
-	ST_COUNT_
+	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_SEGSORT_MID, ST_SEGSORT_BIG, ST_COUNT_
 };
 const char *kStageNames[ST_COUNT_] = {"aabb", "bounds", "count", "scan_cells", "scatter", "pair_test",
                                       "scan_owner", "owner_scatter", "segsort", "mpr", "np_compact", "bins",
-                                      "copy_in", "copy_out", "segsort_mid", "segsort_big", "front"};
+                                      "copy_in", "copy_out", "segsort_mid", "segsort_big"};
 constexpr int kMaxMarks = 64;
 
 // A CUDA graph of one kind of call, replayed while the call's configuration
@@ -62,8 +61,7 @@ struct cc_ctx {
 	GridParams gp{};
 	cudaError_t cuda_err = cudaSuccess;
 	// device scratch
-	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list, dense,
-	    front_sums;
+	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list, dense;
 	Buf ref_cnt, ref_off, ref_keys, ref_tmp, ref_flags, ref_runpos, rx_hist, rx_hoff;
 	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes, np_bsum;
 	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
@@ -383,7 +381,6 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 
 	CC_TRY(ensure_status(c));
 	CC_TRY(ensure(c, c->ticket, 64));
 	CC_TRY(ensure(c, c->big_list, sizeof(uint32_t) * (n + 1024)));
-	CC_TRY(ensure(c, c->front_sums, sizeof(unsigned long long) * kFrontMaxBlocks));
 	CC_TRY(ensure(c, c->dense, sizeof(uint2) * (c->entries.bytes / (2 * sizeof(float4)) / kDenseCell + 1024)));
 	if (np_cap) CC_TRY(np_prepare(c, np_cap));
 	return CC_OK;
@@ -469,25 +466,18 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 		return;
 	}
 	c->inc_valid = false;  // the kept cell lists are overwritten
-	if (!b.sm.plans) {  // one scene: shift + count, cell scan and scatter in one cooperative launch
-		StageMark m(c, ST_FRONT, s);
+	{
+		StageMark m(c, ST_COUNT, s);
 		if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
-		launch_front(n, aabb, b, ptr<unsigned long long>(c->front_sums), s);
-		c->launches -= 2;  // one launch for three stages
-	} else {
-		{
-			StageMark m(c, ST_COUNT, s);
-			if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
-			launch_count(n, aabb, b, s);
-		}
-		{
-			StageMark m(c, ST_SCAN_CELLS, s);
-			launch_scan_cells(b, gmax, s);
-		}
-		{
-			StageMark m(c, ST_SCATTER, s);
-			launch_scatter(n, aabb, b, s);  // the cell scan left the counts zeroed
-		}
+		launch_count(n, aabb, b, s);
+	}
+	{
+		StageMark m(c, ST_SCAN_CELLS, s);
+		launch_scan_cells(b, gmax, s);
+	}
+	{
+		StageMark m(c, ST_SCATTER, s);
+		launch_scatter(n, aabb, b, s);  // the cell scan left the counts zeroed
 	}
 	{
 		StageMark m(c, ST_PAIR_TEST, s);
@@ -943,7 +933,7 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_off,    &c->b_scene_of, &c->b_gid,      &c->b_sst,    &c->b_plans,     &c->b_G,
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
-	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges, &c->front_sums,
+	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges,
 	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);

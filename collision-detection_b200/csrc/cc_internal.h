@@ -58,7 +58,7 @@ struct DevStats {
 	Plan plan;
 	// grid barriers of the cooperative kernels (GridBarrier: arrived, gen),
 	// zeroed with the rest at the start of a pass
-	uint32_t bar_front[2];
+	uint32_t bar_spare_[2];
 	uint32_t bar_np[2];
 	uint32_t bar_compact[2];
 	uint32_t pad3_[2];
@@ -177,11 +177,6 @@ void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridPar
 // In-place shift + per-cell counts on the plan's search grid.
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
-// One scene (b.sm empty), after the bounds pass: launch_count + launch_scan_cells
-// + launch_scatter as one cooperative launch with the same results.
-// block_sums: kFrontMaxBlocks words.
-constexpr unsigned kFrontMaxBlocks = 148 * 8;
-void launch_front(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *block_sums, cudaStream_t s);
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);

@@ -371,10 +371,11 @@ void launch_np_compact(uint64_t P_cap, const unsigned long long *P_dev, const Np
 		if (contacts_out) cudaMemsetAsync(contacts_out, 0, sizeof(unsigned long long), s);
 		return;
 	}
-	// one block per ~1024 flags of the expected count, within the co-resident limit
+	// one block per 256 flags of the expected count (one tile each: the scan
+	// and scatter of a tile are a chain of dependent loads), within the co-resident limit
 	const uint64_t Pe = std::min<uint64_t>(P_hint ? P_hint : P_cap, P_cap);
 	const unsigned grid = (unsigned)std::max<uint64_t>(
-	    1, std::min<uint64_t>((Pe + 1023) / 1024, std::min<uint64_t>(np_coop_max_blocks(), kNpCoopBlocks)));
+	    1, std::min<uint64_t>((Pe + kCoopNT - 1) / kCoopNT, std::min<uint64_t>(np_coop_max_blocks(), kNpCoopBlocks)));
 	launch_coop(k_np_compact_coop, grid, s, P_cap, P_dev, sc, pairs, norm, cpta, cptb, depth, bids, contacts_out);
 }
 
@@ -388,7 +389,7 @@ void launch_np_compact_sorted(uint64_t P_cap, const unsigned long long *P_dev, c
 	}
 	const uint64_t Pe = std::min<uint64_t>(P_hint ? P_hint : P_cap, P_cap);
 	const unsigned grid = (unsigned)std::max<uint64_t>(
-	    1, std::min<uint64_t>((Pe + 1023) / 1024, std::min<uint64_t>(np_coop_max_blocks(), kNpCoopBlocks)));
+	    1, std::min<uint64_t>((Pe + kCoopNT - 1) / kCoopNT, std::min<uint64_t>(np_coop_max_blocks(), kNpCoopBlocks)));
 	launch_coop(k_np_compact_sorted, grid, s, P_cap, P_dev, sc, pairs, tmp, norm, cpta, cptb, depth, bids,
 	            contacts_out);
 }
