@@ -21,7 +21,6 @@ its own bounds, shift and grid).
 """
 from __future__ import annotations
 
-import bisect
 import ctypes
 import gc
 import math
@@ -133,37 +132,59 @@ def _align(nbytes, a=256):
 
 
 class Arena:
-    """One device buffer holding the resident scenes' arrays, placed first-fit
-    with free neighbours merged. Admitting a scene is then a copy into space
-    the server already owns: no device allocation (cudaMalloc stalls every
-    thread that uses the device) while queries are served."""
+    """One device buffer holding the resident scenes' arrays. Free ranges are
+    indexed by size (best fit, O(log F)) and by both ends (a freed range merges
+    with free neighbours in O(1)), so admissions stay cheap while evictions of
+    scenes of very different sizes fragment the buffer. Admitting a scene is a
+    copy into space the server already owns: no device allocation (cudaMalloc
+    stalls every thread that uses the device) while queries are served."""
 
     def __init__(self, nbytes, device):
+        from sortedcontainers import SortedList
         self.size = _align(nbytes)
         self.buf = torch.empty(self.size, dtype=torch.uint8, device=device)
-        self.free = [(0, self.size)]  # (offset, bytes), by offset
+        self._by_size = SortedList([(self.size, 0)])  # (bytes, offset)
+        self._at_start = {0: self.size}               # offset -> bytes
+        self._at_end = {self.size: 0}                 # offset + bytes -> offset
+
+    @property
+    def free(self):
+        """Free ranges (offset, bytes) in address order."""
+        return sorted(self._at_start.items())
+
+    def _add(self, off, nbytes):
+        self._by_size.add((nbytes, off))
+        self._at_start[off] = nbytes
+        self._at_end[off + nbytes] = off
+
+    def _remove(self, off, nbytes):
+        self._by_size.remove((nbytes, off))
+        del self._at_start[off]
+        del self._at_end[off + nbytes]
 
     def take(self, nbytes):
         nbytes = _align(nbytes)
-        for k, (off, sz) in enumerate(self.free):
-            if sz >= nbytes:
-                if sz == nbytes:
-                    del self.free[k]
-                else:
-                    self.free[k] = (off + nbytes, sz - nbytes)
-                return off
-        return None
+        k = self._by_size.bisect_left((nbytes, -1))
+        if k == len(self._by_size):
+            return None
+        sz, off = self._by_size[k]
+        self._remove(off, sz)
+        if sz > nbytes:
+            self._add(off + nbytes, sz - nbytes)
+        return off
 
     def give(self, off, nbytes):
         nbytes = _align(nbytes)
-        k = bisect.bisect_left(self.free, (off, 0))
-        self.free.insert(k, (off, nbytes))
-        if k + 1 < len(self.free) and off + nbytes == self.free[k + 1][0]:  # merge the next range
-            self.free[k] = (off, nbytes + self.free[k + 1][1])
-            del self.free[k + 1]
-        if k > 0 and self.free[k - 1][0] + self.free[k - 1][1] == self.free[k][0]:  # and the previous
-            self.free[k - 1] = (self.free[k - 1][0], self.free[k - 1][1] + self.free[k][1])
-            del self.free[k]
+        nxt = self._at_start.get(off + nbytes)
+        if nxt is not None:  # merge the next range
+            self._remove(off + nbytes, nxt)
+            nbytes += nxt
+        prv = self._at_end.get(off)
+        if prv is not None:  # and the previous
+            psz = self._at_start[prv]
+            self._remove(prv, psz)
+            off, nbytes = prv, nbytes + psz
+        self._add(off, nbytes)
 
 
 @dataclass

@@ -27,7 +27,7 @@ def test_scene_bytes_counts_inputs_and_boxes():
     assert SV.scene_bytes(sc) == sc.nbytes() + 24 * 1000
 
 
-def test_arena_first_fit_merges_and_never_overlaps():
+def test_arena_best_fit_merges_and_never_overlaps():
     # the resident-scene arena's free list on a host buffer: random takes and
     # gives keep the ranges aligned, disjoint, merged with free neighbours,
     # and the free and taken bytes always add up to the arena
