@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(kNT) k_aabb(uint64_t n, const int32_t *__restr
                                                uint64_t nb, const float *__restrict__ pos,
                                                const float *__restrict__ rot, float *__restrict__ aabb,
                                                DevStats *stats, uint32_t *err, PlanArgs pa, ZeroList zero) {
+	pdl_begin();
 	zero_ranges(zero);
 	float3 bmn = f3(INFINITY, INFINITY, INFINITY), bmx = f3(-INFINITY, -INFINITY, -INFINITY);
 	float3 esum = f3(0.f, 0.f, 0.f);  // extent sum for the grid tuner's mean box size
@@ -138,9 +139,9 @@ void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, c
 	pa.inc = inc;
 	pa.inc_margin = inc_margin;
 	if (stats)
-		k_aabb<true><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, stats, err, pa, zero);
+		launch_pdl(k_aabb<true>, dim3(blocks), dim3(kNT), 0, s, n, T, A, B, C, R, ID, nb, pos, rot, aabb, stats, err, pa, zero);
 	else
-		k_aabb<false><<<blocks, kNT, 0, s>>>(n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, pa, zero);
+		launch_pdl(k_aabb<false>, dim3(blocks), dim3(kNT), 0, s, n, T, A, B, C, R, ID, nb, pos, rot, aabb, nullptr, err, pa, zero);
 }
 
 }  // namespace cc

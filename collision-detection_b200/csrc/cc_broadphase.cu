@@ -173,6 +173,7 @@ template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, const DevStats *stats,
                                                 uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count,
                                                 SceneMap sm, int oshift) {
+	pdl_begin();
 	__shared__ Plan sp;
 	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
 	if (threadIdx.x < sizeof(Plan) / 4)
@@ -312,6 +313,7 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
                                                   const uint32_t *__restrict__ cell_start,
                                                   uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
                                                   uint64_t cap, uint32_t *err, SceneMap sm, const uint32_t *gate) {
+	pdl_begin();
 	if (gate && *gate == 0u) return;  // an incremental step that keeps its cell lists
 	__shared__ Plan sp;
 	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
@@ -377,6 +379,7 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
                                                     unsigned long long *pair_counter, SceneMap sm, uint2 *dense,
                                                     uint64_t dense_cap, unsigned long long *dense_count,
                                                     uint32_t *err, uint32_t dense_cell, int oshift) {
+	pdl_begin();
 	__shared__ Plan sp;
 	__shared__ float4 win_all[kNT / 32][2 * kWin];
 	__shared__ unsigned long long out_all[kNT / 32][kOutBuf];
@@ -534,6 +537,7 @@ __global__ void __launch_bounds__(kNT) k_pair_test_dense(const DevStats *stats, 
                                                           unsigned long long *pair_counter, SceneMap sm,
                                                           const uint2 *__restrict__ dense, uint64_t dense_cap,
                                                           int oshift) {
+	pdl_begin();
 	__shared__ Plan sp;
 	__shared__ float4 tlo[kNT], thi[kNT];
 	__shared__ uint32_t colown[kNT], tcode[kNT];
@@ -629,6 +633,7 @@ __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t
                                                         const unsigned long long *__restrict__ owner_off,
                                                         uint32_t *__restrict__ owner_count,
                                                         unsigned long long *__restrict__ out, int oshift) {
+	pdl_begin();
 	const unsigned long long P = stats->pairs;
 	const bool fits = P <= pair_cap && P <= out_cap;
 	if (blockIdx.x == 0 && threadIdx.x == 0) stats->np_n = fits ? P : 0ull;
@@ -681,6 +686,7 @@ constexpr int kBigSeg = 16384;
 __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long long *__restrict__ owner_off,
                                                   unsigned long long *__restrict__ out, uint32_t *big_list,
                                                   uint64_t big_cap, DevStats *stats) {
+	pdl_begin();
 	if (stats->np_n != stats->pairs) return;  // the pairs were not emitted (uniform over the grid)
 	const uint64_t a = (uint64_t)blockIdx.x * kNT + threadIdx.x;
 	uint64_t len = 0;
@@ -863,6 +869,7 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
                                                          const uint32_t *__restrict__ big_list,
                                                          const unsigned long long *__restrict__ owner_off,
                                                          unsigned long long *__restrict__ out, KeyPack kp) {
+	pdl_begin();
 	if (stats->np_n != stats->pairs) return;
 	const uint64_t nmid = min((uint64_t)stats->big_segments, big_cap);
 	const int lane = threadIdx.x & 31;
@@ -896,6 +903,7 @@ __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint
                                                       const uint32_t *__restrict__ big_list,
                                                       const unsigned long long *__restrict__ owner_off,
                                                       unsigned long long *__restrict__ out, KeyPack kp) {
+	pdl_begin();
 	extern __shared__ uint32_t s[];
 	if (stats->np_n != stats->pairs) return;
 	const uint64_t nbig = min((uint64_t)stats->seg_big, big_cap);
@@ -1020,9 +1028,9 @@ void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridPar
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
 	if (!n) return;
 	if (b.sm.plans)
-		k_count<true><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm, 0);
+		launch_pdl(k_count<true>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_count, b.owner_count, b.sm, 0);
 	else
-		k_count<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, b.owner_count, b.sm,
+		launch_pdl(k_count<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_count, b.owner_count, b.sm,
 		                                             b.owner_shift);
 }
 
@@ -1035,16 +1043,16 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
 	if (!n) return;
 	if (b.sm.plans)
-		k_scatter<true><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
+		launch_pdl(k_scatter<true>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
 		                                              b.entry_cap, &b.stats->err, b.sm, nullptr);
 	else
-		k_scatter<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
+		launch_pdl(k_scatter<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
 		                                               b.entry_cap, &b.stats->err, b.sm, nullptr);
 }
 
 template <bool kBatch, int kWin>
 void pair_test_as(const BpBuffers &b, unsigned grid, cudaStream_t s) {
-	k_pair_test<kBatch, kWin><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+	launch_pdl((k_pair_test<kBatch, kWin>), dim3(grid), dim3(kNT), 0, s, b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 	                                               b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
 	                                               b.dense_cap, &b.stats->dense_items, &b.stats->err, b.dense_cell,
 	                                               b.owner_shift);
@@ -1081,7 +1089,7 @@ void launch_scan_cells_gated(const BpBuffers &b, uint32_t g_max, cudaStream_t s)
 	                       &b.stats->cells_scan, &b.stats->entries, b.pre_zeroed, b.cell_count);
 }
 void launch_scatter_gated(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
-	if (n) k_scatter<false><<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
+	if (n) launch_pdl(k_scatter<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
 	                                                      b.entry_cap, &b.stats->err, b.sm, &b.stats->rebuild);
 }
 void launch_refresh_entries(uint64_t n, const float *aabb, const BpBuffers &b, const IncState *inc, cudaStream_t s) {
@@ -1095,11 +1103,11 @@ void launch_pair_test_dense(const BpBuffers &b, cudaStream_t s) {
 	// persistent blocks over the device-side item count (41 KB of shared memory each)
 	const unsigned grid = kNumSMs * 4;
 	if (b.sm.plans)
-		k_pair_test_dense<true><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+		launch_pdl(k_pair_test_dense<true>, dim3(grid), dim3(kNT), 0, s, b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                             b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
 		                                             b.dense_cap, b.owner_shift);
 	else
-		k_pair_test_dense<false><<<grid, kNT, 0, s>>>(b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
+		launch_pdl(k_pair_test_dense<false>, dim3(grid), dim3(kNT), 0, s, b.stats, b.cell_start, b.entries, b.entry_cap, b.owner_count,
 		                                              b.pairs_tmp, b.pair_cap, &b.stats->pairs, b.sm, b.dense,
 		                                              b.dense_cap, b.owner_shift);
 }
@@ -1112,17 +1120,17 @@ void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s) {
 void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
 	const uint64_t bound = std::min<uint64_t>(b.pair_cap, out_cap);
 	const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(blocks_for(bound), 1), (uint64_t)kNumSMs * 8);
-	k_owner_scatter<<<grid, kNT, 0, s>>>(b.stats, b.pair_cap, out_cap, b.pairs_tmp, b.owner_off, b.owner_count, out,
+	launch_pdl(k_owner_scatter, dim3(grid), dim3(kNT), 0, s, b.stats, b.pair_cap, out_cap, b.pairs_tmp, b.owner_off, b.owner_count, out,
 	                                     b.owner_shift);
 }
 
 void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
 	const uint64_t nbk = owner_buckets(n, b.owner_shift);
-	k_segsort<<<blocks_for(nbk), kNT, 0, s>>>(nbk, b.owner_off, out, b.big_list, b.big_cap, b.stats);
+	launch_pdl(k_segsort, dim3(blocks_for(nbk)), dim3(kNT), 0, s, nbk, b.owner_off, out, b.big_list, b.big_cap, b.stats);
 }
 
 void launch_segsort_mid(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
-	k_segsort_mid<<<kNumSMs * 6, kMidNT, 0, s>>>(b.stats, b.big_cap, b.big_list, b.owner_off, out,
+	launch_pdl(k_segsort_mid, dim3(kNumSMs * 6), dim3(kMidNT), 0, s, b.stats, b.big_cap, b.big_list, b.owner_off, out,
 	                                             KeyPack{b.owner_shift, b.key_bits});
 }
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
@@ -1132,7 +1140,7 @@ void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_
 	}();
 	(void)attr;
 	// 64 KB of shared memory a block: three blocks fit on an SM
-	k_segsort_big<<<kNumSMs * 3, 512, kBigSeg * sizeof(uint32_t), s>>>(b.stats, b.big_cap, b.big_list, b.owner_off,
+	launch_pdl(k_segsort_big, dim3(kNumSMs * 3), dim3(512), kBigSeg * sizeof(uint32_t), s, b.stats, b.big_cap, b.big_list, b.owner_off,
 	                                                                   out, KeyPack{b.owner_shift, b.key_bits});
 }
 

@@ -1,6 +1,8 @@
 // Shared device utilities for the collision kernels (sm_100a).
 #pragma once
 #include <cstdint>
+#include <cstdlib>
+#include <utility>
 #include <cuda_runtime.h>
 
 namespace cc {
@@ -178,6 +180,50 @@ __device__ __forceinline__ void grid_barrier(GridBarrier *b, uint32_t *err) {
 		__threadfence();
 	}
 	__syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch. The pipeline's kernels are launched with
+// programmatic stream serialization (launch_pdl): a kernel's blocks may be
+// scheduled while the previous kernel of the stream is still finishing, so
+// the launch and ramp-up of each stage overlap the tail of the one before.
+// Every kernel launched this way calls pdl_begin() first: griddepcontrol.wait
+// blocks until the preceding grid has completed and its writes are visible
+// (a no-op when the launch had no programmatic dependency), and
+// griddepcontrol.launch_dependents then lets the next kernel start launching
+// once all of this grid's blocks have started. Environment CC_PDL=0 turns the
+// attribute off (plain stream order).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_begin() {
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+inline bool pdl_enabled() {
+	static const bool on = [] {
+		const char *v = getenv("CC_PDL");
+		return !(v && v[0] == '0');
+	}();
+	return on;
+}
+
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args) {
+	if (!pdl_enabled()) {
+		kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
+		return;
+	}
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = s;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	at[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // Grid-stride zeroing of the ranges of a ZeroList (called by every thread of

@@ -19,6 +19,7 @@ __global__ void __launch_bounds__(kNT) k_mpr_exact(uint64_t P_cap, const unsigne
                                                     const float *__restrict__ pos, const float *__restrict__ rot,
                                                     float envelope, const long long *__restrict__ pairs,
                                                     NpScratch sc) {
+	pdl_begin();
 	mpr::run<double, true, kNT>(P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, sc,
 	                            sc.classes + 2 * kNpClasses);
 }
@@ -37,7 +38,7 @@ void launch_mpr_exact(unsigned grid, uint64_t P_cap, const unsigned long long *P
                       const float *A, const float *B, const float *C, const float *R, const uint32_t *ID, uint64_t nb,
                       const uint8_t *active, const float *pos, const float *rot, float envelope,
                       const long long *pairs, const NpScratch &sc, cudaStream_t s) {
-	k_mpr_exact<<<grid, kNT, 0, s>>>(P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, sc);
+	launch_pdl(k_mpr_exact, dim3(grid), dim3(kNT), 0, s, P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, sc);
 }
 
 }  // namespace cc

@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(kNT) k_mpr(uint64_t P_cap, const unsigned long
                                               uint64_t nb, const uint8_t *__restrict__ active,
                                               const float *__restrict__ pos, const float *__restrict__ rot,
                                               float envelope, const long long *__restrict__ pairs, NpScratch sc) {
+	pdl_begin();
 	mpr::run<S, false, kNT>(P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, sc,
 	                        sc.classes + 2 * kNpClasses);
 }
@@ -356,10 +357,10 @@ void launch_mpr(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, con
 	if (precision == 0)
 		launch_mpr_exact(grid, P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs, sc, s);
 	else if (precision == 2)
-		k_mpr<float><<<grid, kNT, 0, s>>>(P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs,
+		launch_pdl(k_mpr<float>, dim3(grid), dim3(kNT), 0, s, P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs,
 		                                  sc);
 	else
-		k_mpr<double><<<grid, kNT, 0, s>>>(P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs,
+		launch_pdl(k_mpr<double>, dim3(grid), dim3(kNT), 0, s, P_cap, P_dev, n, T, A, B, C, R, ID, nb, active, pos, rot, envelope, pairs,
 		                                   sc);
 }
 

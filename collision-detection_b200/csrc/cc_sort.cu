@@ -16,6 +16,7 @@ __global__ void __launch_bounds__(kScanNT) k_scan(const uint32_t *__restrict__ i
                                                   OutT *__restrict__ out,
                                                   unsigned long long *total_out, uint64_t *status, uint32_t *ticket,
                                                   uint32_t *err, uint32_t *zero_in) {
+	pdl_begin();
 	__shared__ uint32_t s_tile;
 	__shared__ unsigned long long s_pre;
 	__shared__ unsigned long long sm[40];
@@ -81,7 +82,7 @@ void scan_impl(const uint32_t *in, uint64_t n, OutT *out, uint64_t *status, uint
 		cudaMemsetAsync(status, 0, tiles * sizeof(uint64_t), s);
 		cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s);
 	}
-	k_scan<OutT><<<(unsigned)tiles, kScanNT, 0, s>>>(in, n, n_dev, out, total_out, status, ticket, err, zero_in);
+	launch_pdl(k_scan<OutT>, dim3((unsigned)tiles), dim3(kScanNT), 0, s, in, n, n_dev, out, total_out, status, ticket, err, zero_in);
 }
 }  // namespace
 
