@@ -31,7 +31,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import Context, DevicePipeline, DeviceScene, ScenesPipeline, _stream, lib, numa_local
+from . import Context, DevicePipeline, DeviceScene, ScenesPipeline, _lib, _stream, lib, numa_local
 from . import scenes as S
 
 
@@ -44,6 +44,14 @@ def perturb_(ctx: Context, ds: DeviceScene, seed: int, sigma=1e-4, max_angle=1e-
     """Time-step update of a device-resident scene (cc_perturb_bodies)."""
     ctx.check(lib.cc_perturb_bodies(ctx.h, ds.nb, ds.pos.data_ptr(), ds.rot.data_ptr(), ctypes.c_uint64(seed),
                                     float(sigma), float(max_angle), _stream()), "cc_perturb_bodies")
+
+
+def _pos_ptr(ds):
+    return ds.pos_ptr if isinstance(ds, ArenaScene) else ds.pos.data_ptr()
+
+
+def _rot_ptr(ds):
+    return ds.rot_ptr if isinstance(ds, ArenaScene) else ds.rot.data_ptr()
 
 
 def perturb_many(ctx: Context, updates, sigma=1e-4, max_angle=1e-3):
@@ -63,8 +71,8 @@ def perturb_many(ctx: Context, updates, sigma=1e-4, max_angle=1e-3):
         items = list(r.values())
         k = len(items)
         nb = (ctypes.c_uint64 * k)(*[ds.nb for ds, _ in items])
-        pos = (ctypes.c_void_p * k)(*[ds.pos.data_ptr() for ds, _ in items])
-        rot = (ctypes.c_void_p * k)(*[ds.rot.data_ptr() for ds, _ in items])
+        pos = (ctypes.c_void_p * k)(*[_pos_ptr(ds) for ds, _ in items])
+        rot = (ctypes.c_void_p * k)(*[_rot_ptr(ds) for ds, _ in items])
         seeds = (ctypes.c_uint64 * k)(*[int(sd) & (2**64 - 1) for _, sd in items])
         ctx.check(lib.cc_perturb_scenes(ctx.h, k, nb, pos, rot, seeds, float(sigma), float(max_angle), _stream()),
                   "cc_perturb_scenes")
@@ -114,13 +122,53 @@ class PinnedScene:
         else:
             with torch.cuda.stream(copy_stream):
                 space[:self.total].copy_(self.buf[:self.total], non_blocking=True)
-        ds = DeviceScene.__new__(DeviceScene)
-        ds.n, ds.nb = self.n, self.nb
-        for k, off, shape, dt in self.layout:
-            nbytes = int(np.prod(shape)) * np.dtype(dt).itemsize
-            t = space[off:off + nbytes].view(_TORCH_DTYPE[np.dtype(dt)])
-            setattr(ds, k, t.view(shape) if len(shape) > 1 else t)
-        return ds
+        return ArenaScene(space, self.layout, self.n, self.nb)
+
+
+class ArenaScene(DeviceScene):
+    """A DeviceScene whose nine arrays sit at fixed offsets of one device
+    buffer. The C scene descriptor comes straight from the buffer's address;
+    the torch views of the arrays are made only when something asks for one
+    (an admission costs one copy, not nine view constructions)."""
+
+    _FIELDS = tuple(k for k, _ in PinnedScene.FIELDS)
+
+    def __init__(self, space, layout, n, nb):
+        self.n, self.nb = n, nb
+        self._space, self._layout = space, layout
+        base = space.data_ptr()
+        self._ptr = {k: base + off for k, off, _, _ in layout}
+
+    def __getattr__(self, name):
+        if name in ArenaScene._FIELDS:
+            for k, off, shape, dt in self._layout:
+                if k == name:
+                    nbytes = int(np.prod(shape)) * np.dtype(dt).itemsize
+                    t = self._space[off:off + nbytes].view(_TORCH_DTYPE[np.dtype(dt)])
+                    t = t.view(shape) if len(shape) > 1 else t
+                    setattr(self, name, t)
+                    return t
+        raise AttributeError(name)
+
+    def c_scene(self):
+        c = self.__dict__.get("_c")
+        if c is not None:
+            return c
+        p = self._ptr
+        c = _lib.Scene()
+        c.n, c.nb = self.n, self.nb
+        c.T, c.A, c.B, c.C, c.R, c.ID = p["T"], p["A"], p["B"], p["C"], p["R"], p["ID"]
+        c.body_pos, c.body_rot, c.active = p["pos"], p["rot"], p["active"]
+        self._c = c
+        return c
+
+    @property
+    def pos_ptr(self):
+        return self._ptr["pos"]
+
+    @property
+    def rot_ptr(self):
+        return self._ptr["rot"]
 
 
 _TORCH_DTYPE = {np.dtype(np.int32): torch.int32, np.dtype(np.float32): torch.float32,
