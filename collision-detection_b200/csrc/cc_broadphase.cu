@@ -673,16 +673,24 @@ __device__ __forceinline__ unsigned long long unpack_key(uint32_t v, uint32_t bu
 	return ((unsigned long long)a << 32) | (v & ((1u << kp.kb) - 1u));
 }
 
-constexpr int kSmallSeg = 8;  // buckets sorted by one thread in registers
+constexpr int kTinySeg = 8;    // buckets sorted by one thread with a bubble network in registers
+constexpr int kSmallSeg = 32;  // buckets sorted by one thread with a bitonic network in registers
+
+// Compare-exchange of two 64-bit keys held in registers (ascending).
+__device__ __forceinline__ void cx64(unsigned long long &x, unsigned long long &y) {
+	const unsigned long long a = x, b = y;
+	x = a < b ? a : b;
+	y = a < b ? b : a;
+}
 constexpr int kMidSeg = 1024;
 constexpr int kBigSeg = 16384;
 
 // Sorts each owner bucket (all keys share the bucket's owners, n here is the
-// bucket count): <= 8 keys by one thread, loaded into registers at once and
-// sorted there by a static network on the 64-bit keys; longer buckets are
-// listed for k_segsort_mid (<= 1024 keys, from the front of big_list) or
-// k_segsort_big (<= 16384, from the back), which sort the packed 32-bit keys
-// (pack_key).
+// bucket count): <= 32 keys by one thread, loaded into registers at once and
+// sorted there by a static network on the 64-bit keys (a bubble network up to
+// 8 keys, a bitonic network padded to 32 above); longer buckets are listed for
+// k_segsort_mid (<= 1024 keys, from the front of big_list) or k_segsort_big
+// (<= 16384, from the back), which sort the packed 32-bit keys (pack_key).
 __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long long *__restrict__ owner_off,
                                                   unsigned long long *__restrict__ out, uint32_t *big_list,
                                                   uint64_t big_cap, DevStats *stats) {
@@ -693,18 +701,33 @@ __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long
 	if (a < n) {
 		const uint64_t beg = owner_off[a], end = owner_off[a + 1];
 		len = end - beg;
-		if (len > 1 && len <= kSmallSeg) {
+		if (len > 1 && len <= kTinySeg) {
+			unsigned long long v[kTinySeg];
+#pragma unroll
+			for (int q = 0; q < kTinySeg; q++) v[q] = (uint64_t)q < len ? out[beg + q] : ~0ull;
+#pragma unroll
+			for (int r = 0; r < kTinySeg - 1; r++)
+#pragma unroll
+				for (int q = 0; q < kTinySeg - 1 - r; q++) cx64(v[q], v[q + 1]);
+#pragma unroll
+			for (int q = 0; q < kTinySeg; q++)
+				if ((uint64_t)q < len) out[beg + q] = v[q];
+		} else if (len > kTinySeg && len <= kSmallSeg) {
 			unsigned long long v[kSmallSeg];
 #pragma unroll
 			for (int q = 0; q < kSmallSeg; q++) v[q] = (uint64_t)q < len ? out[beg + q] : ~0ull;
 #pragma unroll
-			for (int r = 0; r < kSmallSeg - 1; r++)
+			for (int k = 2; k <= kSmallSeg; k <<= 1)
 #pragma unroll
-				for (int q = 0; q < kSmallSeg - 1 - r; q++) {
-					const unsigned long long x = v[q], y = v[q + 1];
-					v[q] = x < y ? x : y;
-					v[q + 1] = x < y ? y : x;
-				}
+				for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+					for (int i = 0; i < kSmallSeg; i++) {
+						const int l = i ^ j;
+						if (l > i) {
+							if ((i & k) == 0) cx64(v[i], v[l]);
+							else cx64(v[l], v[i]);
+						}
+					}
 #pragma unroll
 			for (int q = 0; q < kSmallSeg; q++)
 				if ((uint64_t)q < len) out[beg + q] = v[q];
@@ -861,8 +884,8 @@ __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict_
 	}
 }
 
-// Buckets of 9..1024 keys: one warp per bucket, sorted in registers
-// (1..32 keys per lane by bucket size); then buckets of 1025..2048 keys
+// Buckets of 33..1024 keys: one warp per bucket, sorted in registers
+// (2..32 keys per lane by bucket size); then buckets of 1025..2048 keys
 // (listed for k_segsort_big, which leaves them) on pairs of warps.
 constexpr int kMidNT = 256;
 __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
@@ -876,9 +899,8 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
 	const uint64_t warps = (uint64_t)gridDim.x * (kMidNT / 32);
 	for (uint64_t g = (uint64_t)blockIdx.x * (kMidNT / 32) + (threadIdx.x >> 5); g < nmid; g += warps) {
 		const uint32_t a = big_list[g];
-		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;  // 9..1024, listed by k_segsort
-		if (len <= 32) sort_bucket_reg<1>(out, beg, len, a, lane, kp);
-		else if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane, kp);
+		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;  // 33..1024, listed by k_segsort
+		if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane, kp);
 		else if (len <= 128) sort_bucket_reg<4>(out, beg, len, a, lane, kp);
 		else if (len <= 256) sort_bucket_reg<8>(out, beg, len, a, lane, kp);
 		else if (len <= 512) sort_bucket_reg<16>(out, beg, len, a, lane, kp);

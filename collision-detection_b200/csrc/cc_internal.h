@@ -44,7 +44,7 @@ struct DevStats {
 	unsigned long long entries;   // (cell, body) entries of the search grid
 	unsigned long long ref_entries;
 	unsigned long long contacts;
-	unsigned long long big_segments;  // owner buckets of 9..1024 pairs (listed from the front)
+	unsigned long long big_segments;  // owner buckets of 33..1024 pairs (listed from the front)
 	unsigned long long max_segment;
 	unsigned long long seg_big;       // owner buckets of 1025..16384 pairs (listed from the back)
 	unsigned long long cells;     // plan.G as a 64-bit scan count
