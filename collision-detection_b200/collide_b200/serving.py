@@ -436,6 +436,8 @@ class Server:
             return self._serve_batched(stream)
         qs = stream.queries
         t0 = time.perf_counter()
+        timing = {"prepare_s": 0.0, "collide_s": 0.0}
+        self.last_timing = timing
         i = 0  # next query not yet taken
         while i < len(qs):
             now = time.perf_counter() - t0
@@ -444,22 +446,29 @@ class Server:
                 continue
             q = qs[i]
             i += 1
+            tp = time.perf_counter()
             sid = self._prepare(q)
+            tc = time.perf_counter()
             if sid is not None:
                 q.n_pairs, q.n_contacts = self.collide_one(sid)
                 if q.record:
                     q.result = self._record_plain(sid)
             torch.cuda.synchronize()
             q.done = time.perf_counter() - t0
+            timing["prepare_s"] += tc - tp
+            timing["collide_s"] += time.perf_counter() - tc
         return self._report(qs, t0, [1] * len(qs), mode)
 
     def _report(self, qs, t0, passes, mode):
         wall = time.perf_counter() - t0
         lat = np.array([q.done - q.arrival for q in qs]) * 1e3
-        return dict(mode=mode, queries=len(qs), wall_s=wall, queries_per_s=len(qs) / wall,
-                    p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
-                    mean_ms=float(lat.mean()), passes=len(passes), mean_pass_queries=float(np.mean(passes)),
-                    rejected=self.rejected, resident=len(self.resident), resident_gb=self.bytes / 1e9)
+        out = dict(mode=mode, queries=len(qs), wall_s=wall, queries_per_s=len(qs) / wall,
+                   p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
+                   mean_ms=float(lat.mean()), passes=len(passes), mean_pass_queries=float(np.mean(passes)),
+                   rejected=self.rejected, resident=len(self.resident), resident_gb=self.bytes / 1e9)
+        if getattr(self, "last_timing", None):
+            out["host_timing"] = dict(self.last_timing)
+        return out
 
     def _serve_batched(self, stream: Stream):
         """Continuous batching with the host side overlapped: a worker thread
@@ -478,6 +487,9 @@ class Server:
         passes = []
         failure = []
         t0 = time.perf_counter()
+        # where the host time goes (seconds; bytes copied in for new scenes)
+        timing = {"prepare_s": 0.0, "admit_s": 0.0, "pass_s": 0.0, "upload_bytes": 0}
+        self.last_timing = timing
 
         def worker():
             try:
@@ -487,6 +499,7 @@ class Server:
                         if job is None:
                             return
                         ev, arrivals, updates, uniq, scenes, live, take = job
+                        tw = time.perf_counter()
                         pass_s.wait_event(ev)
                         perturb_many(self.ctx, arrivals, NEW_SIGMA, NEW_ANGLE)
                         perturb_many(self.ctx, updates)
@@ -501,6 +514,7 @@ class Server:
                                     q.result = self._record_batch(uniq.index(sid), scenes)
                         pass_s.synchronize()
                         t = time.perf_counter() - t0
+                        timing["pass_s"] += time.perf_counter() - tw
                         for q in take:
                             q.done = t
                         with lock:
@@ -525,14 +539,18 @@ class Server:
                     j += 1
                 take = qs[i:j]
                 i = j
+                tp = time.perf_counter()
                 with lock:
                     pinned = set(busy)
                 updates, arrivals, live = [], [], []
                 for q in take:
                     if q.kind == "new":
+                        ta = time.perf_counter()
                         sid = self.admit(self.pool[q.scene], pinned, copy_s)
+                        timing["admit_s"] += time.perf_counter() - ta
                         if sid is not None:
                             arrivals.append((self.resident[sid], q.seed))
+                            timing["upload_bytes"] += self.pool[q.scene].total
                     else:
                         sid = self.slots[q.scene % len(self.slots)]
                         if sid not in self.resident:
@@ -550,6 +568,7 @@ class Server:
                 with lock:
                     for sid in uniq:
                         busy[sid] = busy.get(sid, 0) + 1
+                timing["prepare_s"] += time.perf_counter() - tp
                 jobs.put((ev, arrivals, updates, uniq, scenes, live, take))
                 passes.append(len(take))
         finally:
