@@ -274,6 +274,31 @@ __global__ void __launch_bounds__(kNT) k_perturb_scenes(uint32_t count, uint64_t
 }
 }  // namespace
 
+// Small host tables go to the device inside kernel parameters: the driver
+// copies a launch's parameters with the launch, so the table needs no copy
+// engine and no staging of pageable memory, and cannot queue behind bulk
+// uploads running on another stream.
+struct ParamChunk {
+	uint32_t words[kParamChunkBytes / 4];
+};
+__global__ void k_param_copy(uint32_t *__restrict__ dst, uint32_t nwords, ParamChunk c) {
+	for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = c.words[i];
+}
+
+cudaError_t copy_small_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+	if (bytes > kParamCopyMax || (bytes & 3) || (reinterpret_cast<uintptr_t>(dst) & 3))
+		return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+	const unsigned char *from = static_cast<const unsigned char *>(src);
+	uint32_t *to = static_cast<uint32_t *>(dst);
+	for (size_t off = 0; off < bytes; off += kParamChunkBytes) {
+		const size_t n = std::min<size_t>(kParamChunkBytes, bytes - off);
+		ParamChunk c;
+		memcpy(c.words, from + off, n);
+		k_param_copy<<<1, 256, 0, s>>>(to + off / 4, (uint32_t)(n / 4), c);
+	}
+	return cudaGetLastError();
+}
+
 void launch_perturb_scenes(uint32_t count, uint64_t total, const PerturbScene *d, float sigma, float max_angle,
                            cudaStream_t s) {
 	if (!count || !total) return;

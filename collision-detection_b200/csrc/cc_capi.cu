@@ -1329,8 +1329,8 @@ cc_status batch_impl(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, floa
 	CC_TRY(ensure(c, c->b_ticket, 64));
 	CC_TRY(ensure(c, c->b_res, sizeof(unsigned long long) * (2 * S + 2)));
 	unsigned long long *d_shape = ptr<unsigned long long>(c->b_off), *d_body = d_shape + (S + 1);
-	CC_CUDA(c, cudaMemcpyAsync(d_shape, bt->shape_offsets, sizeof(uint64_t) * (S + 1), cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(d_body, bt->body_offsets, sizeof(uint64_t) * (S + 1), cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, copy_small_h2d(d_shape, bt->shape_offsets, sizeof(uint64_t) * (S + 1), s));
+	CC_CUDA(c, copy_small_h2d(d_body, bt->body_offsets, sizeof(uint64_t) * (S + 1), s));
 	DevStats *d = ptr<DevStats>(c->stats);
 	const int grid[3] = {gx, gy, gz};
 	uint32_t *scene_of = ptr<uint32_t>(c->b_scene_of), *gid = ptr<uint32_t>(c->b_gid);
@@ -1504,9 +1504,9 @@ cc_status cc_collide_scenes(cc_ctx *c, uint64_t num_scenes, const cc_scene *scen
 	CC_TRY(ensure(c, c->g_src, sizeof(SceneSrc) * num_scenes));
 	CC_TRY(ensure(c, c->g_off, sizeof(unsigned long long) * 2 * (num_scenes + 1)));
 	unsigned long long *d_so = ptr<unsigned long long>(c->g_off), *d_bo = d_so + (num_scenes + 1);
-	CC_CUDA(c, cudaMemcpyAsync(c->g_src.p, src.data(), sizeof(SceneSrc) * num_scenes, cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(d_so, so.data(), sizeof(uint64_t) * (num_scenes + 1), cudaMemcpyHostToDevice, s));
-	CC_CUDA(c, cudaMemcpyAsync(d_bo, bo.data(), sizeof(uint64_t) * (num_scenes + 1), cudaMemcpyHostToDevice, s));
+	CC_CUDA(c, copy_small_h2d(c->g_src.p, src.data(), sizeof(SceneSrc) * num_scenes, s));
+	CC_CUDA(c, copy_small_h2d(d_so, so.data(), sizeof(uint64_t) * (num_scenes + 1), s));
+	CC_CUDA(c, copy_small_h2d(d_bo, bo.data(), sizeof(uint64_t) * (num_scenes + 1), s));
 	SceneDst dst{ptr<int32_t>(c->g_T), ptr<float>(c->g_A), ptr<float>(c->g_B), ptr<float>(c->g_C), ptr<float>(c->g_R),
 	             ptr<uint32_t>(c->g_ID), ptr<float>(c->g_pos), ptr<float>(c->g_rot), ptr<uint8_t>(c->g_act)};
 	{
@@ -1556,9 +1556,9 @@ cc_status cc_perturb_scenes(cc_ctx *c, uint64_t count, const uint64_t *nb, float
 	CC_CUDA(c, cudaSetDevice(c->device));
 	cudaStream_t s = (cudaStream_t)stream;
 	CC_TRY(ensure(c, c->pt_desc, sizeof(PerturbScene) * d.size()));
-	// the descriptor table is staged by the copy itself (pageable source): the
-	// host vector may go away once the call returns
-	CC_CUDA(c, cudaMemcpyAsync(c->pt_desc.p, d.data(), sizeof(PerturbScene) * d.size(), cudaMemcpyHostToDevice, s));
+	// the descriptor table travels in kernel parameters (or a staged copy when
+	// large): the host vector may go away once the call returns
+	CC_CUDA(c, copy_small_h2d(c->pt_desc.p, d.data(), sizeof(PerturbScene) * d.size(), s));
 	launch_perturb_scenes((uint32_t)d.size(), total, ptr<PerturbScene>(c->pt_desc), sigma, max_angle, s);
 	return check_launch(c);
 }

@@ -246,6 +246,13 @@ struct PerturbScene {
 };
 void launch_perturb_scenes(uint32_t count, uint64_t total, const PerturbScene *d, float sigma, float max_angle,
                            cudaStream_t s);
+// Host -> device copy of a small table (bytes a multiple of 4, at most
+// kParamCopyMax) through kernel parameters, in chunks of kParamChunkBytes;
+// larger or unaligned tables fall back to cudaMemcpyAsync. The host table may
+// be reused as soon as the call returns.
+constexpr size_t kParamChunkBytes = 8192;
+constexpr size_t kParamCopyMax = 64 * 1024;
+cudaError_t copy_small_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s);
 void launch_gather(uint64_t n, uint64_t nb, uint32_t S, const unsigned long long *shape_off,
                    const unsigned long long *body_off, const SceneSrc *src, const SceneDst &dst, cudaStream_t s);
 void launch_batch_prep(uint64_t n, uint32_t S, const unsigned long long *shape_off, const unsigned long long *body_off,
