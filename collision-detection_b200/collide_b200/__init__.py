@@ -189,7 +189,7 @@ class Context:
         self.check(lib.cc_set_dense_cell(self.h, int(entries)), "cc_set_dense_cell")
 
     def narrowphase_overlap(self):
-        return bool(getattr(self, "_np_overlap", False))
+        return bool(getattr(self, "_np_overlap", True))
 
     def set_narrowphase_overlap(self, on=True):
         """Run cc_collide's MPR on the unsorted pairs while they are sorted

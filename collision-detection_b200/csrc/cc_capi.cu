@@ -74,7 +74,7 @@ struct cc_ctx {
 	// overlapped narrowphase (cc_set_narrowphase_overlap): the MPR on the
 	// unsorted pairs on np_stream while the main stream sorts them; the
 	// contact hash (keys, values) sized for 4x the expected pair count
-	bool np_overlap = false;
+	bool np_overlap = true;
 	cudaStream_t np_stream = nullptr;
 	cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 	Buf np_hkeys, np_hvals;
@@ -908,6 +908,7 @@ cc_status cc_ctx_create(cc_ctx **out, int device) {
 	c->gp.dense_cell = kDenseCell;
 	c->gp.pair_window = 96;
 	c->gp.pair_blocks_per_sm = 8;
+	c->np_overlap = true;
 	c->gp.user_dim[0] = c->gp.user_dim[1] = c->gp.user_dim[2] = 0;
 	if (const char *v = getenv("CC_GRAPH_REPLAY")) c->graph_off = v[0] == '0';
 	if (cudaSetDevice(device) != cudaSuccess || cudaMallocHost(&c->h_stats, sizeof(DevStats)) != cudaSuccess ||

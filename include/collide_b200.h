@@ -119,7 +119,7 @@ CC_API cc_status cc_set_pair_test_shape(cc_ctx *ctx, int window, int blocks_per_
  *  CC_NP_MIXED: as CC_NP_FP64 but FP32 support maps. */
 enum { CC_NP_EXACT = 0, CC_NP_FP64 = 1, CC_NP_MIXED = 2 };
 CC_API cc_status cc_set_narrowphase_precision(cc_ctx *ctx, int mode);
-/* Overlapped narrowphase for cc_collide (default off): after the pair test
+/* Overlapped narrowphase for cc_collide (default on): after the pair test
  * the MPR runs on the unsorted pair list on a second stream while the list is
  * sorted, and the compaction joins both in sorted order, finding each pair's
  * result through a hash of the contacts. Results are identical either way

@@ -62,6 +62,7 @@ def test_overlapped_narrowphase_equals_in_order(cb, n, extent):
     # contacts overflows it and is redone in order; later calls replay graphs
     m = S.mixed_slab(n, seed=n, extent=extent)
     ref_ctx, ov_ctx = cb.Context(), cb.Context()
+    ref_ctx.set_narrowphase_overlap(False)
     ov_ctx.set_narrowphase_overlap(True)
     a = cb.DevicePipeline(cb.DeviceScene(m), ctx=ref_ctx)
     b = cb.DevicePipeline(cb.DeviceScene(m), ctx=ov_ctx)
