@@ -668,8 +668,8 @@ def run_ours(args):
     G = dims[0] * dims[1] * dims[2]
 
     # ---- value: device-resident, per-step CUDA events, L2 flushed between steps
-    def timed_pass(profile):
-        ctx.set_profiling(profile)
+    def timed_pass(profile, spans=False):
+        ctx.set_profiling(profile, spans=spans)
         ctx.reset_stage_times()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(args.steps)]
@@ -700,6 +700,17 @@ def run_ours(args):
     # the same steps again with CUDA events around every kernel stage (the
     # event records add host work, so this pass is not the value above)
     prof_ms, _, stage, _ = timed_pass(True)
+    # and once more with one event pair around the whole broadphase and one
+    # around the narrowphase (in order for this pass, so that the two spans
+    # do not overlap): the broadphase's kernels then run back to back
+    ov_default = ctx.narrowphase_overlap()
+    ctx.set_narrowphase_overlap(False)
+    for i in range(3):
+        pipe.run()
+    torch.cuda.synchronize()
+    assert (pipe.n_pairs, pipe.n_contacts) == (P, C)
+    span_ms, _, spans, _ = timed_pass(True, spans=True)
+    ctx.set_narrowphase_overlap(ov_default)
     # the same steps with the narrowphase overlapped on (or off, whichever the
     # library's default is not): its MPR runs on the unsorted pairs while they are sorted
     alt_ctx = cb.Context(local)
@@ -825,7 +836,9 @@ def run_ours(args):
     # the single-pass byte model 88N + 56E + 16C + 8P (C = candidates; the
     # home-cell test emits no pair twice, so C = P) over the summed stage times.
     bp_present = [k for k in BP_STAGES if k in kern]
-    bp_ms = sum(kern[k][0] / kern[k][1] for k in bp_present)
+    bp_stage_sum_ms = sum(kern[k][0] / kern[k][1] for k in bp_present)
+    bp_ms = spans["broadphase_span"][0] / spans["broadphase_span"][1]
+    np_span_ms = spans["narrowphase_span"][0] / spans["narrowphase_span"][1]
     bp_bytes = 88 * scene.n + 56 * E + 16 * P + 8 * P
     bp_traffic = sum_traffic(prof, bp_present)
     bp_achieved = bp_bytes / (bp_ms / 1000.0) / 1e9
@@ -835,7 +848,11 @@ def run_ours(args):
                 "traffic": bp_traffic, "traffic_source": prof.get("source") if bp_traffic else None,
                 "ms_per_launch": bp_ms, "floor_bytes": 24 * scene.n + 8 * P,
                 "floor_frac": (24 * scene.n + 8 * P) / (bp_ms / 1000.0) / 1e9 / hbm,
-                "pairs_per_s": P / (bp_ms / 1000.0), "timing": timing}
+                "pairs_per_s": P / (bp_ms / 1000.0),
+                "timing": ("one CUDA event pair around the broadphase's kernels (cell count through the sorted "
+                           f"pair list) of each of {args.steps} in-order steps, L2 flushed between steps "
+                           f"({span_ms / args.steps:.4f} ms/step; narrowphase span {np_span_ms:.4f} ms)"),
+                "stage_sum_ms": bp_stage_sum_ms, "stage_timing": timing}
 
     # The exact MPR stage is bound by FP64 dependent-chain latency, not by
     # memory: its FP64 FLOPs per launch (ncu thread-instruction counts of the

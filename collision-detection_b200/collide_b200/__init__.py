@@ -223,8 +223,10 @@ class Context:
         (default on; results are identical)."""
         self.check(lib.cc_set_graph_replay(self.h, int(bool(on))), "cc_set_graph_replay")
 
-    def set_profiling(self, on=True):
-        self.check(lib.cc_set_profiling(self.h, int(bool(on))), "cc_set_profiling")
+    def set_profiling(self, on=True, spans=False):
+        """Stage timing: every kernel stage (on), or with spans=True only the
+        broadphase and narrowphase spans of an in-order cc_collide step."""
+        self.check(lib.cc_set_profiling(self.h, (2 if spans else 1) if on else 0), "cc_set_profiling")
 
     def reset_stage_times(self):
         lib.cc_reset_stage_times(self.h)

@@ -29,11 +29,17 @@ struct Buf {
 // Kernel stages timed by the optional profiler.
 enum Stage : int {
 	ST_AABB, ST_BOUNDS, ST_COUNT, ST_SCAN_CELLS, ST_SCATTER, ST_PAIR_TEST, ST_SCAN_OWNER, ST_OWNER_SCATTER,
-	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_SEGSORT_MID, ST_SEGSORT_BIG, ST_COUNT_
+	ST_SEGSORT, ST_MPR, ST_NP_COMPACT, ST_BINS, ST_COPY_IN, ST_COPY_OUT, ST_SEGSORT_MID, ST_SEGSORT_BIG,
+	ST_SPAN_BROADPHASE, ST_SPAN_NARROWPHASE, ST_COUNT_
 };
 const char *kStageNames[ST_COUNT_] = {"aabb", "bounds", "count", "scan_cells", "scatter", "pair_test",
                                       "scan_owner", "owner_scatter", "segsort", "mpr", "np_compact", "bins",
-                                      "copy_in", "copy_out", "segsort_mid", "segsort_big"};
+                                      "copy_in", "copy_out", "segsort_mid", "segsort_big",
+                                      "broadphase_span", "narrowphase_span"};
+// Profiling modes (cc_set_profiling): events around every stage, or only
+// around the two spans (one event pair each, so that the kernels inside run
+// back to back as they do unprofiled).
+constexpr int kProfStages = 1, kProfSpans = 2;
 constexpr int kMaxMarks = 64;
 
 // A CUDA graph of one kind of call, replayed while the call's configuration
@@ -145,7 +151,7 @@ struct cc_ctx {
 	bool graph_off = false;
 	GraphSlot g_collide, g_batch;  // cc_collide's step and the batch pass
 	// stage profiler
-	bool prof = false;
+	int prof = 0;  // 0, kProfStages or kProfSpans
 	cudaEvent_t ev[2 * kMaxMarks] = {};
 	int mark_stage[kMaxMarks] = {};
 	int nmarks = 0;
@@ -210,7 +216,8 @@ struct StageMark {
 	int slot = -1;
 	cudaStream_t s;
 	StageMark(cc_ctx *c_, int stage, cudaStream_t s_) : c(c_), s(s_) {
-		if (!c->prof || c->nmarks >= kMaxMarks) return;
+		const bool span = stage == ST_SPAN_BROADPHASE || stage == ST_SPAN_NARROWPHASE;
+		if (c->prof != (span ? kProfSpans : kProfStages) || c->nmarks >= kMaxMarks) return;
 		slot = c->nmarks++;
 		c->mark_stage[slot] = stage;
 		cudaEventRecord(c->ev[2 * slot], s);
@@ -796,9 +803,15 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 			c->pass_zeroed = false;
 			return r;
 		}
-		enqueue_search(c, n, aabb, st, inc);
-		enqueue_emit(c, n, out, pairs_cap, st);
-		enqueue_np(c, a, pairs_cap, &d->np_n, st);
+		{
+			StageMark m(c, ST_SPAN_BROADPHASE, st);
+			enqueue_search(c, n, aabb, st, inc);
+			enqueue_emit(c, n, out, pairs_cap, st);
+		}
+		{
+			StageMark m(c, ST_SPAN_NARROWPHASE, st);
+			enqueue_np(c, a, pairs_cap, &d->np_n, st);
+		}
 		c->pass_zeroed = false;
 		return CC_OK;
 	};
@@ -1072,7 +1085,8 @@ cc_status cc_set_profiling(cc_ctx *c, int on) {
 		CC_CUDA(c, cudaSetDevice(c->device));
 		for (int i = 0; i < 2 * kMaxMarks; i++) CC_CUDA(c, cudaEventCreate(&c->ev[i]));
 	}
-	c->prof = on != 0;
+	if (on < 0 || on > kProfSpans) return set_err(c, CC_ERR_INVALID_ARGUMENT, "profiling mode %d (0, 1 or 2)", on);
+	c->prof = on;
 	return CC_OK;
 }
 
@@ -1584,8 +1598,8 @@ namespace {
 // Turns stage profiling off for the scope of a call.
 struct NoProfile {
 	cc_ctx *c;
-	bool was;
-	explicit NoProfile(cc_ctx *c_) : c(c_), was(c_->prof) { c->prof = false; }
+	int was;
+	explicit NoProfile(cc_ctx *c_) : c(c_), was(c_->prof) { c->prof = 0; }
 	~NoProfile() { c->prof = was; }
 };
 

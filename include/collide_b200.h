@@ -313,11 +313,16 @@ CC_API cc_status cc_set_static_shapes(cc_ctx *ctx, int on);
 /* Number of kernels the last call on this context launched. */
 CC_API uint64_t cc_last_launch_count(const cc_ctx *ctx);
 
-/* Stage timing (no reference counterpart). With profiling on, every call
- * brackets each kernel stage with CUDA events on the caller's stream and
- * accumulates the device time per stage. cc_stage_times fills up to `cap`
- * totals in milliseconds and launch counts, indexed by stage id; stage names
- * come from cc_stage_name. cc_reset_stage_times zeroes the totals. */
+/* Stage timing (no reference counterpart). With mode 1, every call brackets
+ * each kernel stage with CUDA events on the caller's stream and accumulates
+ * the device time per stage. With mode 2, a cc_collide step with the
+ * narrowphase in order (cc_set_narrowphase_overlap off) records only two
+ * spans, "broadphase_span" (cell count through the sorted pair list) and
+ * "narrowphase_span" (MPR and compaction), one event pair each, so that the
+ * kernels inside a span run back to back as they do unprofiled. Mode 0 turns
+ * timing off. cc_stage_times fills up to `cap` totals in milliseconds and
+ * launch counts, indexed by stage id; stage names come from cc_stage_name.
+ * cc_reset_stage_times zeroes the totals. */
 CC_API cc_status cc_set_profiling(cc_ctx *ctx, int on);
 CC_API int cc_stage_count(void);
 CC_API const char *cc_stage_name(int stage);

@@ -74,3 +74,27 @@ def test_overlapped_narrowphase_equals_in_order(cb, n, extent):
             assert torch.equal(getattr(a, k)[:C].view(torch.int32), getattr(b, k)[:C].view(torch.int32)), (step, k)
         assert torch.equal(a.bids[:C], b.bids[:C])
         assert torch.equal(a.aabb.view(torch.int32), b.aabb.view(torch.int32))
+
+
+def test_stage_and_span_profiling_leave_results_unchanged(cb):
+    # per-stage events, span events (in-order narrowphase) and no events give
+    # the same step; spans report exactly the broadphase and narrowphase
+    m = S.mixed_slab(100_000, seed=4, extent=(1.0, 1.0, 0.1))
+    ref = cb.collide(cb.DeviceScene(m), grid=(16, 16, 16))
+    for mode in ("stages", "spans"):
+        ctx = cb.Context()
+        ctx.set_narrowphase_overlap(False)
+        pipe = cb.DevicePipeline(cb.DeviceScene(m), ctx=ctx)
+        ctx.set_profiling(True, spans=mode == "spans")
+        ctx.reset_stage_times()
+        for _ in range(3):
+            pipe.run()
+            assert torch.equal(pipe.pairs[: pipe.n_pairs], ref["pairs"])
+            assert torch.equal(pipe.norm[: pipe.n_contacts], ref["norm"])
+        t = ctx.stage_times()
+        if mode == "spans":
+            assert set(t) == {"broadphase_span", "narrowphase_span"}
+        else:
+            assert {"count", "pair_test", "mpr"} <= set(t) and "broadphase_span" not in t
+        assert all(n == 3 and ms > 0 for ms, n in t.values())
+        ctx.set_profiling(False)
