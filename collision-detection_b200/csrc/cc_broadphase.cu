@@ -31,6 +31,7 @@
 // the reference's host build does).
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 
 #include "cc_common.cuh"
 #include "cc_internal.h"
@@ -172,7 +173,7 @@ __device__ __forceinline__ uint32_t cell_index(const Plan &p, uint32_t base, int
 template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ aabb, const DevStats *stats,
                                                 uint32_t *__restrict__ cell_count, uint32_t *__restrict__ owner_count,
-                                                SceneMap sm, int oshift) {
+                                                SceneMap sm, int oshift, uint32_t *__restrict__ owner_cursor) {
 	pdl_begin();
 	__shared__ Plan sp;
 	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
@@ -181,28 +182,52 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
 	__syncthreads();
 	if (!kBatch && !sp.valid) return;  // invalid input: nothing is modified
 	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
-	load_tile_aabb(aabb, n, i0, stage);
-	__syncthreads();
-	// in-place shift by fabs(min) (:382-386), element by element
-	if constexpr (kBatch) {
-		for (int k = threadIdx.x; k < 6 * kNT; k += kNT) {
-			const uint64_t shape = i0 + (uint64_t)((k % (3 * kNT)) / 3);
-			if (shape < n) {
-				const Plan &p = sm.plans[__ldg(sm.scene_of + shape)];
-				if (p.valid) stage[k] = stage[k] + p.origin[k % 3];
-			}
+	if (!kBatch && tile_vec_ok(aabb, n, i0)) {
+		// in-place shift by fabs(min) (:382-386) on 16-byte vectors, in
+		// registers on the way to shared memory: float 4k + j of a corner run
+		// is component (k + j) mod 3
+		const int k = threadIdx.x;
+		if (k < 3 * kNT / 4) {
+			float4 *lo = reinterpret_cast<float4 *>(aabb + 3 * i0);
+			float4 *hi = reinterpret_cast<float4 *>(aabb + 3 * (n + i0));
+			const int r = k % 3;
+			const float o0 = sp.origin[r], o1 = sp.origin[r == 2 ? 0 : r + 1], o2 = sp.origin[r == 0 ? 2 : r - 1];
+			float4 a = lo[k], b = hi[k];
+			a = make_float4(a.x + o0, a.y + o1, a.z + o2, a.w + o0);
+			b = make_float4(b.x + o0, b.y + o1, b.z + o2, b.w + o0);
+			lo[k] = a;
+			hi[k] = b;
+			reinterpret_cast<float4 *>(stage)[k] = a;
+			reinterpret_cast<float4 *>(stage)[3 * kNT / 4 + k] = b;
 		}
+		__syncthreads();
 	} else {
-		for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
+		load_tile_aabb(aabb, n, i0, stage);
+		__syncthreads();
+		// in-place shift by fabs(min) (:382-386), element by element
+		if constexpr (kBatch) {
+			for (int k = threadIdx.x; k < 6 * kNT; k += kNT) {
+				const uint64_t shape = i0 + (uint64_t)((k % (3 * kNT)) / 3);
+				if (shape < n) {
+					const Plan &p = sm.plans[__ldg(sm.scene_of + shape)];
+					if (p.valid) stage[k] = stage[k] + p.origin[k % 3];
+				}
+			}
+		} else {
+			for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
+		}
+		__syncthreads();
+		store_tile_aabb(aabb, n, i0, stage);
 	}
-	__syncthreads();
-	store_tile_aabb(aabb, n, i0, stage);
 	const uint64_t i = i0 + threadIdx.x;
 	if (i >= n) return;
 	const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
 	const float *hs = stage + 3 * kNT;
 	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
-	if ((i & ((1ull << oshift) - 1)) == 0) owner_count[i >> oshift] = 0u;  // the first body of its owner bucket
+	if ((i & ((1ull << oshift) - 1)) == 0) {  // the first body of its owner bucket
+		owner_count[i >> oshift] = 0u;
+		if (owner_cursor) owner_cursor[i >> oshift] = 0u;
+	}
 	uint32_t base;
 	const Plan &p = plan_of<kBatch>(sp, sm, i, base);
 	if (kBatch && !p.valid) return;
@@ -332,18 +357,42 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 	if (kBatch && !p.valid) return;
 	const CellRange r = entry_range(p, mn, mx);
 	bool over = false;
-	for (int z = r.c0[2]; z <= r.c1[2]; z++)
-		for (int y = r.c0[1]; y <= r.c1[1]; y++)
-			for (int x = r.c0[0]; x <= r.c1[0]; x++) {
-				const uint32_t c = cell_index(p, base, x, y, z);
-				const uint64_t slot = (uint64_t)cell_start[c] + atomicAdd(&cursor[c], 1u);
-				if (slot < cap) {
-					entries[2 * slot] = make_float4(mn.x, mn.y, mn.z, __uint_as_float((uint32_t)i));
-					entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(pack_cell(x, y, z)));
-				} else {
-					over = true;
+	const float4 elo = make_float4(mn.x, mn.y, mn.z, __uint_as_float((uint32_t)i));
+	const auto put = [&](uint64_t slot, uint32_t packed) {
+		if (slot < cap) {
+			entries[2 * slot] = elo;
+			entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(packed));
+		} else {
+			over = true;
+		}
+	};
+	const int nx = r.c1[0] - r.c0[0] + 1, ny = r.c1[1] - r.c0[1] + 1, nz = r.c1[2] - r.c0[2] + 1;
+	if (nx <= 2 && ny <= 2 && nz <= 2) {
+		// up to 2x2x2 cells (nearly every box): the offset loads and cursor
+		// atomics of all its cells are issued before any result is used, so a
+		// thread waits one memory round trip instead of one per cell
+		uint32_t cell[8], packed[8], slot[8];
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const int x = r.c0[0] + (q & 1), y = r.c0[1] + ((q >> 1) & 1), z = r.c0[2] + (q >> 2);
+			cell[q] = cell_index(p, base, x, y, z);
+			packed[q] = pack_cell(x, y, z);
+		}
+#pragma unroll
+		for (int q = 0; q < 8; q++)
+			if ((q & 1) < nx && ((q >> 1) & 1) < ny && (q >> 2) < nz)
+				slot[q] = cell_start[cell[q]] + atomicAdd(&cursor[cell[q]], 1u);
+#pragma unroll
+		for (int q = 0; q < 8; q++)
+			if ((q & 1) < nx && ((q >> 1) & 1) < ny && (q >> 2) < nz) put(slot[q], packed[q]);
+	} else {
+		for (int z = r.c0[2]; z <= r.c1[2]; z++)
+			for (int y = r.c0[1]; y <= r.c1[1]; y++)
+				for (int x = r.c0[0]; x <= r.c1[0]; x++) {
+					const uint32_t c = cell_index(p, base, x, y, z);
+					put((uint64_t)cell_start[c] + atomicAdd(&cursor[c], 1u), pack_cell(x, y, z));
 				}
-			}
+	}
 	if (over) atomicOr(err, (uint32_t)kErrCapacity);
 }
 
@@ -661,16 +710,28 @@ __global__ void __launch_bounds__(kNT) k_owner_scatter(DevStats *stats, uint64_t
 struct KeyPack {
 	int shift, kb;  // BpBuffers::owner_shift, key_bits
 };
+// kPack false: one owner per bucket (shift 0), the key is the partner half.
+// The choice is a template parameter, resolved per kernel launch: a runtime
+// test inside the register sorts' unrolled load and store loops made the
+// warp-tier kernel almost twice as slow on the 16.7M clustered scene.
+template <bool kPack>
 __device__ __forceinline__ uint32_t pack_key(unsigned long long key, KeyPack kp) {
 	const uint32_t b = (uint32_t)key;
-	if (!kp.shift) return b;
-	const uint32_t alo = (uint32_t)(key >> 32) & ((1u << kp.shift) - 1u);
-	return (alo << kp.kb) | b;
+	if constexpr (!kPack) {
+		return b;
+	} else {
+		const uint32_t alo = (uint32_t)(key >> 32) & ((1u << kp.shift) - 1u);
+		return (alo << kp.kb) | b;
+	}
 }
+template <bool kPack>
 __device__ __forceinline__ unsigned long long unpack_key(uint32_t v, uint32_t bucket, KeyPack kp) {
-	if (!kp.shift) return ((unsigned long long)bucket << 32) | v;
-	const uint32_t a = (bucket << kp.shift) | (v >> kp.kb);
-	return ((unsigned long long)a << 32) | (v & ((1u << kp.kb) - 1u));
+	if constexpr (!kPack) {
+		return ((unsigned long long)bucket << 32) | v;
+	} else {
+		const uint32_t a = (bucket << kp.shift) | (v >> kp.kb);
+		return ((unsigned long long)a << 32) | (v & ((1u << kp.kb) - 1u));
+	}
 }
 
 constexpr int kTinySeg = 8;    // buckets sorted by one thread with a bubble network in registers
@@ -684,6 +745,43 @@ __device__ __forceinline__ void cx64(unsigned long long &x, unsigned long long &
 }
 constexpr int kMidSeg = 1024;
 constexpr int kBigSeg = 16384;
+
+// One bucket of at most kSmallSeg 64-bit keys sorted by one thread in
+// registers: a bubble network up to kTinySeg keys, a bitonic network padded
+// to kSmallSeg above (one load and one store round trip either way).
+__device__ __forceinline__ void sort_thread_bucket(unsigned long long *__restrict__ out, uint64_t beg, uint64_t len) {
+	if (len > 1 && len <= kTinySeg) {
+		unsigned long long v[kTinySeg];
+#pragma unroll
+		for (int q = 0; q < kTinySeg; q++) v[q] = (uint64_t)q < len ? out[beg + q] : ~0ull;
+#pragma unroll
+		for (int r = 0; r < kTinySeg - 1; r++)
+#pragma unroll
+			for (int q = 0; q < kTinySeg - 1 - r; q++) cx64(v[q], v[q + 1]);
+#pragma unroll
+		for (int q = 0; q < kTinySeg; q++)
+			if ((uint64_t)q < len) out[beg + q] = v[q];
+	} else if (len > kTinySeg && len <= kSmallSeg) {
+		unsigned long long v[kSmallSeg];
+#pragma unroll
+		for (int q = 0; q < kSmallSeg; q++) v[q] = (uint64_t)q < len ? out[beg + q] : ~0ull;
+#pragma unroll
+		for (int k = 2; k <= kSmallSeg; k <<= 1)
+#pragma unroll
+			for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+				for (int i = 0; i < kSmallSeg; i++) {
+					const int l = i ^ j;
+					if (l > i) {
+						if ((i & k) == 0) cx64(v[i], v[l]);
+						else cx64(v[l], v[i]);
+					}
+				}
+#pragma unroll
+		for (int q = 0; q < kSmallSeg; q++)
+			if ((uint64_t)q < len) out[beg + q] = v[q];
+	}
+}
 
 // Sorts each owner bucket (all keys share the bucket's owners, n here is the
 // bucket count): <= 32 keys by one thread, loaded into registers at once and
@@ -701,37 +799,7 @@ __global__ void __launch_bounds__(kNT) k_segsort(uint64_t n, const unsigned long
 	if (a < n) {
 		const uint64_t beg = owner_off[a], end = owner_off[a + 1];
 		len = end - beg;
-		if (len > 1 && len <= kTinySeg) {
-			unsigned long long v[kTinySeg];
-#pragma unroll
-			for (int q = 0; q < kTinySeg; q++) v[q] = (uint64_t)q < len ? out[beg + q] : ~0ull;
-#pragma unroll
-			for (int r = 0; r < kTinySeg - 1; r++)
-#pragma unroll
-				for (int q = 0; q < kTinySeg - 1 - r; q++) cx64(v[q], v[q + 1]);
-#pragma unroll
-			for (int q = 0; q < kTinySeg; q++)
-				if ((uint64_t)q < len) out[beg + q] = v[q];
-		} else if (len > kTinySeg && len <= kSmallSeg) {
-			unsigned long long v[kSmallSeg];
-#pragma unroll
-			for (int q = 0; q < kSmallSeg; q++) v[q] = (uint64_t)q < len ? out[beg + q] : ~0ull;
-#pragma unroll
-			for (int k = 2; k <= kSmallSeg; k <<= 1)
-#pragma unroll
-				for (int j = k >> 1; j > 0; j >>= 1)
-#pragma unroll
-					for (int i = 0; i < kSmallSeg; i++) {
-						const int l = i ^ j;
-						if (l > i) {
-							if ((i & k) == 0) cx64(v[i], v[l]);
-							else cx64(v[l], v[i]);
-						}
-					}
-#pragma unroll
-			for (int q = 0; q < kSmallSeg; q++)
-				if ((uint64_t)q < len) out[beg + q] = v[q];
-		}
+		sort_thread_bucket(out, beg, len);
 	}
 	const bool longer = len > kSmallSeg;
 	const uint32_t wmax = __reduce_max_sync(0xffffffffu, longer ? (uint32_t)min(len, (uint64_t)0xffffffffu) : 0u);
@@ -827,20 +895,20 @@ __device__ __forceinline__ void bitonic_reg(uint32_t (&v)[K], int lane) {
 }
 // One bucket of len <= 32*K keys: partner halves into registers (padding
 // sorts last), sorted, written back with the owner in the high half.
-template <int K>
+template <int K, bool kPack>
 __device__ __forceinline__ void sort_bucket_reg(unsigned long long *__restrict__ out, uint64_t beg, uint64_t len,
                                                 uint32_t a, int lane, KeyPack kp) {
 	uint32_t v[K];
 #pragma unroll
 	for (int r = 0; r < K; r++) {
 		const uint64_t e = 32u * r + lane;
-		v[r] = e < len ? pack_key(out[beg + e], kp) : 0xffffffffu;
+		v[r] = e < len ? pack_key<kPack>(out[beg + e], kp) : 0xffffffffu;
 	}
 	bitonic_reg<K>(v, lane);
 #pragma unroll
 	for (int r = 0; r < K; r++) {
 		const uint64_t e = 32u * r + lane;
-		if (e < len) out[beg + e] = unpack_key(v[r], a, kp);
+		if (e < len) out[beg + e] = unpack_key<kPack>(v[r], a, kp);
 	}
 }
 
@@ -850,6 +918,7 @@ __device__ __forceinline__ void sort_bucket_reg(unsigned long long *__restrict__
 // named barrier `bar` (both warps run the same steps).
 constexpr int kPairSeg = 2048;
 __device__ __forceinline__ void pair_sync(int bar) { asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory"); }
+template <bool kPack>
 __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict__ out, uint64_t beg, uint64_t len,
                                                  uint32_t a, int half, int lane, uint32_t *x, int bar, KeyPack kp) {
 	const int el = half * 1024 + lane;
@@ -857,7 +926,7 @@ __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict_
 #pragma unroll
 	for (int r = 0; r < 32; r++) {
 		const uint64_t e = (uint64_t)el + 32u * r;
-		v[r] = e < len ? pack_key(out[beg + e], kp) : 0xffffffffu;
+		v[r] = e < len ? pack_key<kPack>(out[beg + e], kp) : 0xffffffffu;
 	}
 	for (int k = 2; k <= kPairSeg; k <<= 1)
 		for (int j = k >> 1; j > 0; j >>= 1) {
@@ -880,7 +949,7 @@ __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict_
 #pragma unroll
 	for (int r = 0; r < 32; r++) {
 		const uint64_t e = (uint64_t)el + 32u * r;
-		if (e < len) out[beg + e] = unpack_key(v[r], a, kp);
+		if (e < len) out[beg + e] = unpack_key<kPack>(v[r], a, kp);
 	}
 }
 
@@ -888,6 +957,7 @@ __device__ __forceinline__ void sort_bucket_pair(unsigned long long *__restrict_
 // (2..32 keys per lane by bucket size); then buckets of 1025..2048 keys
 // (listed for k_segsort_big, which leaves them) on pairs of warps.
 constexpr int kMidNT = 256;
+template <bool kPack>
 __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats, uint64_t big_cap,
                                                          const uint32_t *__restrict__ big_list,
                                                          const unsigned long long *__restrict__ owner_off,
@@ -900,11 +970,11 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
 	for (uint64_t g = (uint64_t)blockIdx.x * (kMidNT / 32) + (threadIdx.x >> 5); g < nmid; g += warps) {
 		const uint32_t a = big_list[g];
 		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;  // 33..1024, listed by k_segsort
-		if (len <= 64) sort_bucket_reg<2>(out, beg, len, a, lane, kp);
-		else if (len <= 128) sort_bucket_reg<4>(out, beg, len, a, lane, kp);
-		else if (len <= 256) sort_bucket_reg<8>(out, beg, len, a, lane, kp);
-		else if (len <= 512) sort_bucket_reg<16>(out, beg, len, a, lane, kp);
-		else sort_bucket_reg<32>(out, beg, len, a, lane, kp);
+		if (len <= 64) sort_bucket_reg<2, kPack>(out, beg, len, a, lane, kp);
+		else if (len <= 128) sort_bucket_reg<4, kPack>(out, beg, len, a, lane, kp);
+		else if (len <= 256) sort_bucket_reg<8, kPack>(out, beg, len, a, lane, kp);
+		else if (len <= 512) sort_bucket_reg<16, kPack>(out, beg, len, a, lane, kp);
+		else sort_bucket_reg<32, kPack>(out, beg, len, a, lane, kp);
 	}
 	__shared__ uint32_t xch[kMidNT / 64][kPairSeg];
 	const uint64_t nbig = min((uint64_t)stats->seg_big, big_cap);
@@ -914,13 +984,14 @@ __global__ void __launch_bounds__(kMidNT, 2) k_segsort_mid(const DevStats *stats
 		const uint32_t a = big_list[big_cap - 1 - g];
 		const uint64_t beg = owner_off[a], len = owner_off[a + 1] - beg;
 		if (len > kPairSeg) continue;  // the block tier's (uniform over the pair)
-		sort_bucket_pair(out, beg, len, a, half, lane, xch[pair], 1 + pair, kp);
+		sort_bucket_pair<kPack>(out, beg, len, a, half, lane, xch[pair], 1 + pair, kp);
 	}
 }
 
 // Buckets of 2049..16384 keys: one block per bucket (grid-stride over the
 // device-side count), bitonic sort of the partner halves in 64 KB of
 // dynamic shared memory.
+template <bool kPack>
 __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint64_t big_cap,
                                                       const uint32_t *__restrict__ big_list,
                                                       const unsigned long long *__restrict__ owner_off,
@@ -935,10 +1006,106 @@ __global__ void __launch_bounds__(512) k_segsort_big(const DevStats *stats, uint
 		if (len <= kPairSeg) continue;  // sorted by warp pairs in k_segsort_mid (uniform over the block)
 		int m = 1;
 		while ((uint64_t)m < len) m <<= 1;
-		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? pack_key(out[beg + i], kp) : 0xffffffffu;
+		for (int i = threadIdx.x; i < m; i += blockDim.x) s[i] = (uint64_t)i < len ? pack_key<kPack>(out[beg + i], kp) : 0xffffffffu;
 		__syncthreads();
 		bitonic_u32(s, m, threadIdx.x, blockDim.x, [] { __syncthreads(); });
-		for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = unpack_key(s[i], a, kp);
+		for (int i = threadIdx.x; (uint64_t)i < len; i += blockDim.x) out[beg + i] = unpack_key<kPack>(s[i], a, kp);
+		__syncthreads();
+	}
+}
+
+// ---------------------------------------------------------------- fused owner sort
+// Pair lists far shorter than the body count (the owner shift then keeps about
+// eight pairs per bucket, so there are few buckets): the owner scan, the
+// bucketing and every bucket sort of the path above run as ONE cooperative
+// kernel. Each block scans all bucket counts itself into shared memory (a few
+// KB read from L2 per block; no scan launch), buckets its share of the pairs
+// through per-bucket cursors (zeroed by k_count, so the counts stay intact
+// while other blocks still scan them), waits at one grid barrier, and sorts
+// the buckets: <= 32 keys per thread, 33..1024 per warp in registers,
+// 1025..kFusedSeg per block in shared memory. A longer bucket sets
+// kErrSegmentTooLong (the caller then sorts the whole list).
+constexpr int kFusedNT = 256;
+constexpr int kFusedSeg = 4096;
+constexpr uint32_t kFusedBuckets = 8191;  // offsets + block-tier keys fit the default 48 KB of shared memory
+
+template <bool kPack>
+__global__ void __launch_bounds__(kFusedNT) k_owner_sort_fused(DevStats *stats, uint64_t pair_cap, uint64_t out_cap,
+                                                             const unsigned long long *__restrict__ tmp,
+                                                             const uint32_t *__restrict__ owner_count,
+                                                             uint32_t *__restrict__ cursor, uint32_t nbk,
+                                                             unsigned long long *__restrict__ out, int oshift,
+                                                             KeyPack kp) {
+	extern __shared__ uint32_t fsm[];  // off[nbk + 1], then kFusedSeg keys of the block tier
+	__shared__ unsigned long long scan_sm[40];
+	uint32_t *off = fsm, *keys = fsm + nbk + 1;
+	const unsigned long long P = stats->pairs;
+	const bool fits = P <= pair_cap && P <= out_cap && P < 0xffffffffull;
+	if (blockIdx.x == 0 && threadIdx.x == 0) stats->np_n = fits ? P : 0ull;
+	if (!fits) return;  // uniform over the grid: no block reaches the barrier
+	// 1. exclusive scan of the bucket counts: coalesced loads into shared
+	// memory (all in flight at once), then one contiguous run per thread
+	for (uint32_t b = threadIdx.x; b < nbk; b += kFusedNT) off[b] = owner_count[b];
+	__syncthreads();
+	const uint32_t per = (nbk + kFusedNT - 1) / kFusedNT;
+	const uint32_t b0 = min(nbk, threadIdx.x * per), b1 = min(nbk, b0 + per);
+	unsigned long long run = 0;
+	for (uint32_t b = b0; b < b1; b++) run += off[b];
+	unsigned long long total;
+	unsigned long long excl = block_excl_scan<unsigned long long, kFusedNT>(run, scan_sm, &total);
+	for (uint32_t b = b0; b < b1; b++) {
+		const uint32_t c = off[b];
+		off[b] = (uint32_t)excl;
+		excl += c;
+	}
+	if (threadIdx.x == 0) off[nbk] = (uint32_t)total;
+	__syncthreads();
+	// 2. bucket the pairs (lanes of a warp with one bucket share one atomic)
+	const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+	const uint64_t step = (uint64_t)gridDim.x * kFusedNT;
+	for (uint64_t t0 = (uint64_t)blockIdx.x * kFusedNT + (threadIdx.x & ~31u); t0 < P; t0 += step) {
+		const uint64_t t = t0 + lane;
+		const bool valid = t < P;
+		const unsigned long long key = valid ? tmp[t] : 0ull;
+		const uint32_t a = valid ? (uint32_t)(key >> 32) >> oshift : 0xffffffffu;
+		const uint32_t peers = __match_any_sync(0xffffffffu, a);
+		const int leader = __ffs(peers) - 1;
+		uint32_t base = 0;
+		if (valid && (int)lane == leader) base = atomicAdd(&cursor[a], (uint32_t)__popc(peers));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if (valid) out[(uint64_t)off[a] + base + __popc(peers & lt)] = key;
+	}
+	grid_barrier(reinterpret_cast<GridBarrier *>(stats->bar_emit), &stats->err);
+	// 3. sort the buckets, three tiers
+	const uint64_t gt = (uint64_t)blockIdx.x * kFusedNT + threadIdx.x;
+	uint32_t longest = 0;
+	for (uint64_t b = gt; b < nbk; b += step) {
+		const uint32_t beg = off[b], len = off[b + 1] - beg;
+		sort_thread_bucket(out, beg, len);
+		longest = max(longest, len);
+	}
+	longest = __reduce_max_sync(0xffffffffu, longest);
+	if (lane == 0 && longest > kSmallSeg) atomicMax(&stats->max_segment, (unsigned long long)longest);
+	if (lane == 0 && longest > kFusedSeg) atomicOr(&stats->err, (uint32_t)kErrSegmentTooLong);
+	const uint64_t warps = step / 32;
+	for (uint64_t b = gt / 32; b < nbk; b += warps) {
+		const uint32_t beg = off[b], len = off[b + 1] - beg;  // uniform over the warp
+		if (len <= kSmallSeg || len > kMidSeg) continue;
+		if (len <= 64) sort_bucket_reg<2, kPack>(out, beg, len, (uint32_t)b, lane, kp);
+		else if (len <= 128) sort_bucket_reg<4, kPack>(out, beg, len, (uint32_t)b, lane, kp);
+		else if (len <= 256) sort_bucket_reg<8, kPack>(out, beg, len, (uint32_t)b, lane, kp);
+		else if (len <= 512) sort_bucket_reg<16, kPack>(out, beg, len, (uint32_t)b, lane, kp);
+		else sort_bucket_reg<32, kPack>(out, beg, len, (uint32_t)b, lane, kp);
+	}
+	for (uint64_t b = blockIdx.x; b < nbk; b += gridDim.x) {
+		const uint32_t beg = off[b], len = off[b + 1] - beg;  // uniform over the block
+		if (len <= kMidSeg || len > kFusedSeg) continue;
+		int m = 1;
+		while ((uint32_t)m < len) m <<= 1;
+		for (int i = threadIdx.x; i < m; i += kFusedNT) keys[i] = (uint32_t)i < len ? pack_key<kPack>(out[beg + i], kp) : 0xffffffffu;
+		__syncthreads();
+		bitonic_u32(keys, m, threadIdx.x, kFusedNT, [] { __syncthreads(); });
+		for (int i = threadIdx.x; (uint32_t)i < len; i += kFusedNT) out[beg + i] = unpack_key<kPack>(keys[i], (uint32_t)b, kp);
 		__syncthreads();
 	}
 }
@@ -1050,14 +1217,100 @@ void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridPar
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
 	if (!n) return;
 	if (b.sm.plans)
-		launch_pdl(k_count<true>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_count, b.owner_count, b.sm, 0);
+		launch_pdl(k_count<true>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_count, b.owner_count, b.sm, 0,
+		           (uint32_t *)nullptr);
 	else
 		launch_pdl(k_count<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_count, b.owner_count, b.sm,
-		                                             b.owner_shift);
+		           b.owner_shift, b.owner_cursor);
+}
+
+// ---------------------------------------------------------------- cell offsets
+// The cell offsets as one cooperative launch (reduce, one grid barrier, scan):
+// each block sums its contiguous chunk of the counts, waits at the barrier,
+// adds up the sums of the blocks before it (at most kScanCoopBlocks words)
+// and scans its chunk on top, zeroing the counts behind it for the scatter's
+// cursors. The single-pass look-back scan spent 13 us of a 1M-body step here
+// almost entirely waiting (1 % SM throughput): its tiles wait on one another
+// at L2 latency, the barrier is one round trip for the whole grid.
+constexpr int kCsNT = 256, kCsIPT = 4, kCsTile = kCsNT * kCsIPT;
+__global__ void __launch_bounds__(kCsNT) k_scan_cells_coop(DevStats *stats, uint32_t g_max, uint32_t *__restrict__ counts,
+                                                         uint32_t *__restrict__ start,
+                                                         unsigned long long *__restrict__ bsum) {
+	__shared__ unsigned long long sm[40];
+	const uint64_t n = min((uint64_t)g_max, (uint64_t)stats->cells);
+	const uint64_t per = ((n + gridDim.x - 1) / gridDim.x + kCsTile - 1) / kCsTile * kCsTile;
+	const uint64_t lo = min(n, (uint64_t)blockIdx.x * per), hi = min(n, lo + per);
+	unsigned long long part = 0;
+	for (uint64_t i = lo + threadIdx.x; i < hi; i += kCsNT) part += counts[i];
+	unsigned long long total;
+	(void)block_excl_scan<unsigned long long, kCsNT>(part, sm, &total);
+	if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+	grid_barrier(reinterpret_cast<GridBarrier *>(stats->bar_scan), &stats->err);
+	unsigned long long before = 0;
+	for (uint32_t j = threadIdx.x; j < blockIdx.x; j += kCsNT) before += __ldcg(bsum + j);
+	unsigned long long run_total;
+	(void)block_excl_scan<unsigned long long, kCsNT>(before, sm, &run_total);
+	for (uint64_t t0 = lo; t0 < hi; t0 += kCsTile) {
+		const uint64_t i = t0 + (uint64_t)threadIdx.x * kCsIPT;
+		uint32_t v[kCsIPT] = {0u, 0u, 0u, 0u};
+		const bool full = i + kCsIPT <= hi;
+		if (full) {
+			const uint4 q = *reinterpret_cast<const uint4 *>(counts + i);
+			v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+			*reinterpret_cast<uint4 *>(counts + i) = make_uint4(0u, 0u, 0u, 0u);
+		} else {
+#pragma unroll
+			for (int j = 0; j < kCsIPT; j++)
+				if (i + j < hi) {
+					v[j] = counts[i + j];
+					counts[i + j] = 0u;
+				}
+		}
+		unsigned long long tile_total;
+		const unsigned long long excl =
+		    block_excl_scan<unsigned long long, kCsNT>((unsigned long long)v[0] + v[1] + v[2] + v[3], sm, &tile_total);
+		uint32_t o[kCsIPT];
+		unsigned long long r = run_total + excl;
+#pragma unroll
+		for (int j = 0; j < kCsIPT; j++) {
+			o[j] = (uint32_t)r;
+			r += v[j];
+		}
+		if (full) {
+			*reinterpret_cast<uint4 *>(start + i) = make_uint4(o[0], o[1], o[2], o[3]);
+		} else {
+#pragma unroll
+			for (int j = 0; j < kCsIPT; j++)
+				if (i + j < hi) start[i + j] = o[j];
+		}
+		run_total += tile_total;
+	}
+	// the block whose chunk ends the counts (block 0 when there are none)
+	// writes the end offset and the entry total
+	if (threadIdx.x == 0 && hi == n && (lo < hi || (n == 0 && blockIdx.x == 0))) {
+		start[n] = (uint32_t)run_total;
+		stats->entries = run_total;
+	}
 }
 
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
 	// the scan leaves the counts zeroed: they are the scatter's cursors
+	if (b.scan_bsum) {
+		static const int per_sm = [] {
+			int v = 0;
+			if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_scan_cells_coop, kCsNT, 0) != cudaSuccess || v < 1) v = 1;
+			return v;
+		}();
+		const unsigned grid = (unsigned)std::max<uint64_t>(
+		    1, std::min<uint64_t>((uint64_t)g_max / (2 * kCsTile), std::min<uint64_t>((uint64_t)per_sm * kNumSMs,
+		                                                                               kScanCoopBlocks)));
+		DevStats *st = b.stats;
+		uint32_t gm = g_max, *cnt = b.cell_count, *start = b.cell_start;
+		unsigned long long *bs = b.scan_bsum;
+		void *args[] = {&st, &gm, &cnt, &start, &bs};
+		cudaLaunchCooperativeKernel((const void *)k_scan_cells_coop, dim3(grid), dim3(kCsNT), args, 0, s);
+		return;
+	}
 	launch_scan_u32_to_u32(b.cell_count, g_max, b.cell_start, b.status, b.ticket, &b.stats->err, s, &b.stats->cells,
 	                       &b.stats->entries, b.pre_zeroed, b.cell_count);
 }
@@ -1152,18 +1405,64 @@ void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cud
 }
 
 void launch_segsort_mid(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
-	launch_pdl(k_segsort_mid, dim3(kNumSMs * 6), dim3(kMidNT), 0, s, b.stats, b.big_cap, b.big_list, b.owner_off, out,
-	                                             KeyPack{b.owner_shift, b.key_bits});
+	const KeyPack kp{b.owner_shift, b.key_bits};
+	if (kp.shift)
+		launch_pdl(k_segsort_mid<true>, dim3(kNumSMs * 6), dim3(kMidNT), 0, s, b.stats, b.big_cap, b.big_list, b.owner_off,
+		           out, kp);
+	else
+		launch_pdl(k_segsort_mid<false>, dim3(kNumSMs * 6), dim3(kMidNT), 0, s, b.stats, b.big_cap, b.big_list, b.owner_off,
+		           out, kp);
 }
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s) {
 	static const bool attr = [] {
-		return cudaFuncSetAttribute(k_segsort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		return cudaFuncSetAttribute(k_segsort_big<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                            kBigSeg * (int)sizeof(uint32_t)) == cudaSuccess &&
+		       cudaFuncSetAttribute(k_segsort_big<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		                            kBigSeg * (int)sizeof(uint32_t)) == cudaSuccess;
 	}();
 	(void)attr;
 	// 64 KB of shared memory a block: three blocks fit on an SM
-	launch_pdl(k_segsort_big, dim3(kNumSMs * 3), dim3(512), kBigSeg * sizeof(uint32_t), s, b.stats, b.big_cap, b.big_list, b.owner_off,
-	                                                                   out, KeyPack{b.owner_shift, b.key_bits});
+	const KeyPack kp{b.owner_shift, b.key_bits};
+	if (kp.shift)
+		launch_pdl(k_segsort_big<true>, dim3(kNumSMs * 3), dim3(512), kBigSeg * sizeof(uint32_t), s, b.stats, b.big_cap,
+		           b.big_list, b.owner_off, out, kp);
+	else
+		launch_pdl(k_segsort_big<false>, dim3(kNumSMs * 3), dim3(512), kBigSeg * sizeof(uint32_t), s, b.stats, b.big_cap,
+		           b.big_list, b.owner_off, out, kp);
+}
+
+bool fused_sort_fits(uint64_t buckets) { return buckets >= 1 && buckets <= kFusedBuckets; }
+bool fused_sort_enabled() {
+	static const bool on = [] {
+		const char *v = getenv("CC_FUSED_SORT");
+		return !(v && v[0] == '0');
+	}();
+	return on;
+}
+
+void launch_owner_sort_fused(uint64_t n, uint64_t out_cap, unsigned long long *out, uint64_t P_hint, const BpBuffers &b,
+                             cudaStream_t s) {
+	const uint32_t nbk = (uint32_t)owner_buckets(n, b.owner_shift);
+	const size_t smem = sizeof(uint32_t) * ((size_t)nbk + 1 + kFusedSeg);
+	static const int per_sm = [] {
+		int v = 0;
+		const int most = (int)(sizeof(uint32_t) * ((size_t)kFusedBuckets + 1 + kFusedSeg));
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_owner_sort_fused<true>, kFusedNT, most) != cudaSuccess || v < 1)
+			v = 1;
+		return v;
+	}();
+	const uint64_t want = (std::max<uint64_t>(P_hint, nbk) + kFusedNT - 1) / kFusedNT;
+	unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)per_sm * kNumSMs));
+	uint64_t pair_cap = b.pair_cap;
+	const unsigned long long *tmp = b.pairs_tmp;
+	const uint32_t *cnt = b.owner_count;
+	uint32_t *cur = b.owner_cursor;
+	int oshift = b.owner_shift;
+	KeyPack kp{b.owner_shift, b.key_bits};
+	DevStats *st = b.stats;
+	void *args[] = {&st, &pair_cap, &out_cap, &tmp, &cnt, &cur, (void *)&nbk, &out, &oshift, &kp};
+	const void *k = kp.shift ? (const void *)k_owner_sort_fused<true> : (const void *)k_owner_sort_fused<false>;
+	cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kFusedNT), args, smem, s);
 }
 
 void launch_ref_count(uint64_t n, const float *aabb_shifted, const DevStats *stats, uint32_t *cnt, cudaStream_t s) {

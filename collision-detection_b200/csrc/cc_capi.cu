@@ -70,6 +70,7 @@ struct cc_ctx {
 	Buf stats, cell_count, cell_start, entries, owner_count, owner_off, pairs_tmp, status, ticket, big_list, dense;
 	Buf ref_cnt, ref_off, ref_keys, ref_tmp, ref_flags, ref_runpos, rx_hist, rx_hoff;
 	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes, np_bsum;
+	Buf bp_bsum;  // block sums of the cooperative cell scan
 	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
 	    out_depth, out_bids;
 	// batch scratch: offsets, scene of each shape, global body ids, per-scene
@@ -93,6 +94,10 @@ struct cc_ctx {
 	// retained broadphase result (owner buckets not yet scattered)
 	bool retained = false;
 	uint64_t retained_n = 0, retained_P = 0;
+	bool retained_fused = false;
+	// this call's pairs are emitted by the fused owner sort (one scene, not
+	// incremental, few owner buckets); set by prepare and the call
+	bool fused_now = false;
 	uint64_t last_E = 0, last_P = 0;
 	int last_dim[3] = {0, 0, 0};
 	// owner buckets of the pair sort (BpBuffers::owner_shift / key_bits), chosen
@@ -305,6 +310,8 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.big_list = ptr<uint32_t>(c->big_list);
 	b.big_cap = c->big_list.bytes / sizeof(uint32_t);
 	b.pre_zeroed = c->pass_zeroed;
+	b.owner_cursor = c->fused_now ? ptr<uint32_t>(c->owner_off) : nullptr;
+	b.scan_bsum = c->bp_bsum.p ? ptr<unsigned long long>(c->bp_bsum) : nullptr;
 	b.sm = c->sm;
 	b.dense = ptr<uint2>(c->dense);
 	b.dense_cap = c->dense.bytes / sizeof(uint2);
@@ -374,7 +381,9 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 
 	} else {
 		choose_owner_shift(c, n);
 	}
+	c->fused_now = !g_override && fused_sort_enabled() && fused_sort_fits(owner_buckets(n, c->owner_shift));
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
+	CC_TRY(ensure(c, c->bp_bsum, sizeof(unsigned long long) * kScanCoopBlocks));
 	CC_TRY(ensure(c, c->cell_count, sizeof(uint32_t) * c->gp.g_max));
 	CC_TRY(ensure(c, c->cell_start, sizeof(uint32_t) * (c->gp.g_max + 1)));
 	CC_TRY(ensure(c, c->owner_count, sizeof(uint32_t) * std::max<uint64_t>(n, 1)));
@@ -490,6 +499,7 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 		StageMark m(c, ST_PAIR_TEST, s);
 		launch_pair_test(n, b, hint_E(c, n), s);
 	}
+	owner_scan = owner_scan && !c->fused_now;  // the fused owner sort scans the buckets itself
 	if (owner_scan) {
 		StageMark m(c, ST_SCAN_OWNER, s);
 		launch_scan_owner(n, b, s);
@@ -501,6 +511,12 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 // count exceeds out_cap or the scratch).
 void enqueue_emit(cc_ctx *c, uint64_t n, unsigned long long *out, uint64_t out_cap, cudaStream_t s) {
 	BpBuffers b = bp_buffers(c);
+	if (c->fused_now) {
+		StageMark m(c, ST_SEGSORT, s);
+		launch_owner_sort_fused(n, out_cap, out, hint_P(c), b, s);
+		c->launches += 1;
+		return;
+	}
 	{
 		StageMark m(c, ST_OWNER_SCATTER, s);
 		launch_owner_scatter(out_cap, out, b, s);
@@ -559,11 +575,12 @@ cc_status enqueue_sort_and_np_overlapped(cc_ctx *c, uint64_t n, const NpArgs &a,
 		           c->np_precision, hint_P(c), c->np_stream);
 	}
 	CC_CUDA(c, cudaEventRecord(c->ev_join, c->np_stream));
-	{
+	if (!c->fused_now) {
 		StageMark m(c, ST_SCAN_OWNER, s);
 		launch_scan_owner(n, b, s);
+		c->launches += 1;
 	}
-	c->launches += 3;  // owner scan, class grouping, MPR
+	c->launches += 2;  // class grouping, MPR
 	enqueue_emit(c, n, reinterpret_cast<unsigned long long *>(a.pairs), pairs_cap, s);
 	CC_CUDA(c, cudaStreamWaitEvent(s, c->ev_join, 0));
 	{
@@ -580,6 +597,7 @@ cc_status reset_pass_counters(cc_ctx *c, uint64_t n, cudaStream_t s) {
 	DevStats *d = ptr<DevStats>(c->stats);
 	CC_CUDA(c, cudaMemsetAsync(c->cell_count.p, 0, sizeof(uint32_t) * c->gp.g_max, s));
 	CC_CUDA(c, cudaMemsetAsync(c->owner_count.p, 0, sizeof(uint32_t) * n, s));
+	if (c->fused_now) CC_CUDA(c, cudaMemsetAsync(c->owner_off.p, 0, sizeof(uint32_t) * n, s));  // the cursors
 	CC_CUDA(c, cudaMemsetAsync(&d->err, 0, sizeof(uint32_t), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->pairs, 0, sizeof(unsigned long long), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
@@ -612,8 +630,8 @@ cc_status settle(cc_ctx *c, uint64_t n, float *aabb, unsigned long long *out, ui
 		b = bp_buffers(c);
 		if (!keep_lists) launch_scatter(n, aabb, b, s);
 		launch_pair_test(n, b, E, s);
-		launch_scan_owner(n, b, s);
-		c->launches += keep_lists ? 3 : 4;
+		if (!c->fused_now) launch_scan_owner(n, b, s);
+		c->launches += (keep_lists ? 3 : 4) - (c->fused_now ? 1 : 0);
 		if (out) enqueue_emit(c, n, out, out_cap, s);
 		if (np) enqueue_np(c, *np, out_cap, &ptr<DevStats>(c->stats)->np_n, s);
 		CC_TRY(check_launch(c));
@@ -654,15 +672,18 @@ void retain(cc_ctx *c, uint64_t n, uint64_t P) {
 	c->retained = true;
 	c->retained_n = n;
 	c->retained_P = P;
+	c->retained_fused = c->fused_now;
 }
 
 // Writes the retained pair list into `out` (cap >= P checked by the caller).
 cc_status emit_retained(cc_ctx *c, unsigned long long *out, uint64_t cap, cudaStream_t s) {
+	PdlScope pdl_(c->retained_n);
 	DevStats *d = ptr<DevStats>(c->stats);
 	c->h_word[0] = c->retained_P;
 	CC_CUDA(c, cudaMemcpyAsync(&d->pairs, c->h_word, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
 	CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 3 * sizeof(unsigned long long), s));
 	CC_CUDA(c, cudaMemsetAsync(&d->err, 0, sizeof(uint32_t), s));
+	c->fused_now = c->retained_fused;
 	enqueue_emit(c, c->retained_n, out, cap, s);
 	CC_TRY(check_launch(c));
 	CC_TRY(read_stats(c, s));
@@ -747,8 +768,10 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
                           int32_t *bids, cudaStream_t s, bool graphs) {
 	c->retained = false;
 	const uint64_t n = sc.n;
+	PdlScope pdl_(n);
 	CC_TRY(prepare(c, n, pairs_cap));
 	const bool inc = c->incremental && !c->sm.plans;
+	if (inc) c->fused_now = false;  // the incremental count kernels keep the five-launch owner path
 	if (inc) {
 		CC_TRY(ensure(c, c->inc_ranges, sizeof(unsigned long long) * n));
 		CC_TRY(ensure(c, c->inc_state, sizeof(IncState)));
@@ -823,7 +846,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	struct {
 		uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
 		const void *p[18];
-		int dims[3], prec, oshift, kbits, ov;
+		int dims[3], prec, oshift, kbits, ov, fused;
 		float env;
 		GridParams gp;
 		uint64_t hslots;
@@ -837,6 +860,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	memcpy(k.p, ps, sizeof(ps));
 	k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.env = envelope; k.gp = c->gp;
 	k.oshift = c->owner_shift; k.kbits = c->key_bits; k.ov = ov ? 1 : 0; k.hslots = ov ? c->np_hslots : 0;
+	k.fused = c->fused_now ? 1 : 0;
 	return run_graphed(c, c->g_collide, &k, sizeof(k), enqueue_all, s);
 }
 
@@ -948,7 +972,7 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
 	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges,
-	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals};
+	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals,   &c->bp_bsum};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
 	c->g_collide.drop();
@@ -1151,6 +1175,7 @@ cc_status cc_broadphase(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy, int 
 	CC_CUDA(c, cudaSetDevice(c->device));
 	cudaStream_t s = (cudaStream_t)stream;
 	CC_TRY(prepare(c, n, 0));
+	PdlScope pdl_(n);
 	const int grid[3] = {gx, gy, gz};
 	{
 		StageMark m(c, ST_BOUNDS, s);
@@ -1329,6 +1354,7 @@ cc_status batch_impl(cc_ctx *c, const cc_batch *bt, int gx, int gy, int gz, floa
 	const uint64_t n = sc.n;
 	if (n == 0) return CC_OK;
 	if (!res->aabb || !sc.active) return set_err(c, CC_ERR_INVALID_ARGUMENT, "null aabb or active array");
+	PdlScope pdl_(n);
 	CC_CUDA(c, cudaSetDevice(c->device));
 	cudaStream_t s = (cudaStream_t)stream;
 	const uint64_t pairs_cap = res->pairs_cap;

@@ -58,10 +58,10 @@ struct DevStats {
 	Plan plan;
 	// grid barriers of the cooperative kernels (GridBarrier: arrived, gen),
 	// zeroed with the rest at the start of a pass
-	uint32_t bar_spare_[2];
+	uint32_t bar_emit[2];  // k_owner_sort_fused
 	uint32_t bar_np[2];
 	uint32_t bar_compact[2];
-	uint32_t pad3_[2];
+	uint32_t bar_scan[2];  // k_scan_cells_coop
 };
 
 constexpr int kMaxDim = 1024;  // cells per axis (10-bit packed cell coordinates)
@@ -165,7 +165,15 @@ struct BpBuffers {
 	// 128) and the grid cap in blocks per SM
 	int pair_window = 96;
 	int pair_blocks_per_sm = 8;
+	// non-null: the fused owner sort (k_owner_sort_fused) emits this call's
+	// pairs; k_count zeroes these per-bucket cursors (owner_buckets(n,
+	// owner_shift) words, in the owner_off scratch) beside the counts
+	uint32_t *owner_cursor = nullptr;
+	// non-null: the cell offsets come from the cooperative scan
+	// (k_scan_cells_coop), these kScanCoopBlocks words hold its block sums
+	unsigned long long *scan_bsum = nullptr;
 };
+constexpr uint32_t kScanCoopBlocks = 2048;
 // Owner buckets of n bodies at a shift.
 __host__ __device__ inline uint64_t owner_buckets(uint64_t n, int shift) {
 	return n ? ((n - 1) >> shift) + 1 : 0;
@@ -204,6 +212,15 @@ void launch_owner_scatter(uint64_t out_cap, unsigned long long *out, const BpBuf
 void launch_segsort(uint64_t n, unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 void launch_segsort_mid(unsigned long long *out, const BpBuffers &b, cudaStream_t s);
 void launch_segsort_big(unsigned long long *out, const BpBuffers &b, cudaStream_t s);
+// The owner scan, bucketing and bucket sorts above as one cooperative kernel,
+// for at most 8191 owner buckets (fused_sort_fits); b.owner_cursor must be set
+// (and was zeroed by this call's launch_count). Same device-driven contract as
+// launch_owner_scatter; P_hint sizes the grid only.
+bool fused_sort_fits(uint64_t buckets);
+// Environment CC_FUSED_SORT=0 keeps the five-launch owner path everywhere.
+bool fused_sort_enabled();
+void launch_owner_sort_fused(uint64_t n, uint64_t out_cap, unsigned long long *out, uint64_t P_hint, const BpBuffers &b,
+                             cudaStream_t s);
 
 // ------------------------------------------------------------------ batches
 // Per-scene accumulators of the batch bounds pass (zeroed per call).

@@ -96,5 +96,5 @@ def test_stage_and_span_profiling_leave_results_unchanged(cb):
             assert set(t) == {"broadphase_span", "narrowphase_span"}
         else:
             assert {"count", "pair_test", "mpr"} <= set(t) and "broadphase_span" not in t
-        assert all(n == 3 and ms > 0 for ms, n in t.values())
+        assert all(n >= 3 and ms > 0 for ms, n in t.values()), t  # the first call may redo stages after sizing
         ctx.set_profiling(False)
