@@ -54,6 +54,11 @@ __device__ __forceinline__ bool tile_vec_ok(const float *aabb, uint64_t n, uint6
 	return i0 + kNT <= n && ((reinterpret_cast<uintptr_t>(aabb + 3 * i0) & 15) == 0) &&
 	       ((reinterpret_cast<uintptr_t>(aabb + 3 * (n + i0)) & 15) == 0);
 }
+// The same for 32-byte vector accesses.
+__device__ __forceinline__ bool tile_vec_ok32(const float *aabb, uint64_t n, uint64_t i0) {
+	return i0 + kNT <= n && ((reinterpret_cast<uintptr_t>(aabb + 3 * i0) & 31) == 0) &&
+	       ((reinterpret_cast<uintptr_t>(aabb + 3 * (n + i0)) & 31) == 0);
+}
 __device__ __forceinline__ void load_tile_aabb(const float *__restrict__ aabb, uint64_t n, uint64_t i0, float *stage) {
 	if (tile_vec_ok(aabb, n, i0)) {
 		const float4 *lo = reinterpret_cast<const float4 *>(aabb + 3 * i0);
@@ -182,23 +187,25 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
 	__syncthreads();
 	if (!kBatch && !sp.valid) return;  // invalid input: nothing is modified
 	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
-	if (!kBatch && tile_vec_ok(aabb, n, i0)) {
-		// in-place shift by fabs(min) (:382-386) on 16-byte vectors, in
-		// registers on the way to shared memory: float 4k + j of a corner run
-		// is component (k + j) mod 3
-		const int k = threadIdx.x;
-		if (k < 3 * kNT / 4) {
-			float4 *lo = reinterpret_cast<float4 *>(aabb + 3 * i0);
-			float4 *hi = reinterpret_cast<float4 *>(aabb + 3 * (n + i0));
-			const int r = k % 3;
+	if (!kBatch && tile_vec_ok32(aabb, n, i0)) {
+		// in-place shift by fabs(min) (:382-386) on 32-byte vectors, in
+		// registers on the way to shared memory: thread k < 96 takes floats
+		// [8k, 8k + 8) of the min-corner run, thread 96 + k those of the
+		// max-corner run; float 8k + j is component (2k + j) mod 3
+		const int t = threadIdx.x;
+		if (t < 3 * kNT / 4) {
+			const int k = t < 3 * kNT / 8 ? t : t - 3 * kNT / 8;
+			float *run = t < 3 * kNT / 8 ? aabb + 3 * i0 : aabb + 3 * (n + i0);
+			const int r = (2 * k) % 3;
 			const float o0 = sp.origin[r], o1 = sp.origin[r == 2 ? 0 : r + 1], o2 = sp.origin[r == 0 ? 2 : r - 1];
-			float4 a = lo[k], b = hi[k];
+			float4 a, b;
+			ld_global_v8(run + 8 * k, a, b);
 			a = make_float4(a.x + o0, a.y + o1, a.z + o2, a.w + o0);
-			b = make_float4(b.x + o0, b.y + o1, b.z + o2, b.w + o0);
-			lo[k] = a;
-			hi[k] = b;
-			reinterpret_cast<float4 *>(stage)[k] = a;
-			reinterpret_cast<float4 *>(stage)[3 * kNT / 4 + k] = b;
+			b = make_float4(b.x + o1, b.y + o2, b.z + o0, b.w + o1);
+			st_global_v8(run + 8 * k, a, b);
+			float4 *st = reinterpret_cast<float4 *>(stage) + (t < 3 * kNT / 8 ? 0 : 3 * kNT / 4);
+			st[2 * k] = a;
+			st[2 * k + 1] = b;
 		}
 		__syncthreads();
 	} else {
@@ -337,7 +344,8 @@ template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
                                                   const uint32_t *__restrict__ cell_start,
                                                   uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
-                                                  uint64_t cap, uint32_t *err, SceneMap sm, const uint32_t *gate) {
+                                                  uint64_t cap, uint32_t *err, SceneMap sm, const uint32_t *gate,
+                                                  unsigned long long *__restrict__ cs) {
 	pdl_begin();
 	if (gate && *gate == 0u) return;  // an incremental step that keeps its cell lists
 	__shared__ Plan sp;
@@ -359,12 +367,21 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 	bool over = false;
 	const float4 elo = make_float4(mn.x, mn.y, mn.z, __uint_as_float((uint32_t)i));
 	const auto put = [&](uint64_t slot, uint32_t packed) {
-		if (slot < cap) {
-			entries[2 * slot] = elo;
-			entries[2 * slot + 1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(packed));
+		if (slot < cap) {  // one 32-byte store (entries are 32-byte aligned)
+			st_global_v8(reinterpret_cast<float *>(entries + 2 * slot), elo,
+			             make_float4(mx.x, mx.y, mx.z, __uint_as_float(packed)));
 		} else {
 			over = true;
 		}
+	};
+	// a slot in cell c: start + cursor, from one packed 64-bit atomic when the
+	// scan wrote the packed words, else a start load and a cursor atomic
+	const auto take = [&](uint32_t c) -> uint64_t {
+		if (cs) {
+			const unsigned long long w = atomicAdd(cs + c, 1ull);
+			return (w >> 32) + (w & 0xffffffffull);
+		}
+		return (uint64_t)cell_start[c] + atomicAdd(&cursor[c], 1u);
 	};
 	const int nx = r.c1[0] - r.c0[0] + 1, ny = r.c1[1] - r.c0[1] + 1, nz = r.c1[2] - r.c0[2] + 1;
 	if (nx <= 2 && ny <= 2 && nz <= 2) {
@@ -381,7 +398,7 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 #pragma unroll
 		for (int q = 0; q < 8; q++)
 			if ((q & 1) < nx && ((q >> 1) & 1) < ny && (q >> 2) < nz)
-				slot[q] = cell_start[cell[q]] + atomicAdd(&cursor[cell[q]], 1u);
+				slot[q] = (uint32_t)take(cell[q]);
 #pragma unroll
 		for (int q = 0; q < 8; q++)
 			if ((q & 1) < nx && ((q >> 1) & 1) < ny && (q >> 2) < nz) put(slot[q], packed[q]);
@@ -390,7 +407,7 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 			for (int y = r.c0[1]; y <= r.c1[1]; y++)
 				for (int x = r.c0[0]; x <= r.c1[0]; x++) {
 					const uint32_t c = cell_index(p, base, x, y, z);
-					put((uint64_t)cell_start[c] + atomicAdd(&cursor[c], 1u), pack_cell(x, y, z));
+					put(take(c), pack_cell(x, y, z));
 				}
 	}
 	if (over) atomicOr(err, (uint32_t)kErrCapacity);
@@ -448,7 +465,10 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 		// stage entries [base, base + kWin) of this warp
 		const uint32_t nwin = (uint32_t)min((uint64_t)kWin, E - base);
 		__syncwarp();
-		for (uint32_t k = lane; k < 2 * nwin; k += 32) win[k] = entries[2 * base + k];
+		// asynchronous 16-byte copies straight into shared memory: all of the
+		// window's loads are in flight at once and hold no registers
+		for (uint32_t k = lane; k < 2 * nwin; k += 32) cp_async16(win + k, entries + 2 * base + k);
+		cp_async_wait_all();
 		__syncwarp();
 		const uint64_t e = base + lane;
 		const bool valid = e < E;
@@ -1235,7 +1255,8 @@ void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s) {
 constexpr int kCsNT = 256, kCsIPT = 4, kCsTile = kCsNT * kCsIPT;
 __global__ void __launch_bounds__(kCsNT) k_scan_cells_coop(DevStats *stats, uint32_t g_max, uint32_t *__restrict__ counts,
                                                          uint32_t *__restrict__ start,
-                                                         unsigned long long *__restrict__ bsum) {
+                                                         unsigned long long *__restrict__ bsum,
+                                                         unsigned long long *__restrict__ cs) {
 	__shared__ unsigned long long sm[40];
 	const uint64_t n = min((uint64_t)g_max, (uint64_t)stats->cells);
 	const uint64_t per = ((n + gridDim.x - 1) / gridDim.x + kCsTile - 1) / kCsTile * kCsTile;
@@ -1283,6 +1304,11 @@ __global__ void __launch_bounds__(kCsNT) k_scan_cells_coop(DevStats *stats, uint
 			for (int j = 0; j < kCsIPT; j++)
 				if (i + j < hi) start[i + j] = o[j];
 		}
+		if (cs) {
+#pragma unroll
+			for (int j = 0; j < kCsIPT; j++)
+				if (i + j < hi) cs[i + j] = (unsigned long long)o[j] << 32;
+		}
 		run_total += tile_total;
 	}
 	// the block whose chunk ends the counts (block 0 when there are none)
@@ -1306,8 +1332,8 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
 		                                                                               kScanCoopBlocks)));
 		DevStats *st = b.stats;
 		uint32_t gm = g_max, *cnt = b.cell_count, *start = b.cell_start;
-		unsigned long long *bs = b.scan_bsum;
-		void *args[] = {&st, &gm, &cnt, &start, &bs};
+		unsigned long long *bs = b.scan_bsum, *cs = b.cell_cs;
+		void *args[] = {&st, &gm, &cnt, &start, &bs, &cs};
 		cudaLaunchCooperativeKernel((const void *)k_scan_cells_coop, dim3(grid), dim3(kCsNT), args, 0, s);
 		return;
 	}
@@ -1315,14 +1341,15 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
 	                       &b.stats->entries, b.pre_zeroed, b.cell_count);
 }
 
-void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
+void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s, bool packed) {
 	if (!n) return;
+	unsigned long long *cs = packed ? b.cell_cs : nullptr;
 	if (b.sm.plans)
-		launch_pdl(k_scatter<true>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
-		                                              b.entry_cap, &b.stats->err, b.sm, nullptr);
+		launch_pdl(k_scatter<true>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count,
+		           b.entries, b.entry_cap, &b.stats->err, b.sm, (const uint32_t *)nullptr, cs);
 	else
-		launch_pdl(k_scatter<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
-		                                               b.entry_cap, &b.stats->err, b.sm, nullptr);
+		launch_pdl(k_scatter<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count,
+		           b.entries, b.entry_cap, &b.stats->err, b.sm, (const uint32_t *)nullptr, cs);
 }
 
 template <bool kBatch, int kWin>
@@ -1365,7 +1392,8 @@ void launch_scan_cells_gated(const BpBuffers &b, uint32_t g_max, cudaStream_t s)
 }
 void launch_scatter_gated(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
 	if (n) launch_pdl(k_scatter<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
-	                                                      b.entry_cap, &b.stats->err, b.sm, &b.stats->rebuild);
+	                                                      b.entry_cap, &b.stats->err, b.sm, (const uint32_t *)&b.stats->rebuild,
+	                                                      (unsigned long long *)nullptr);
 }
 void launch_refresh_entries(uint64_t n, const float *aabb, const BpBuffers &b, const IncState *inc, cudaStream_t s) {
 	const unsigned grid = kNumSMs * 8;

@@ -71,6 +71,7 @@ struct cc_ctx {
 	Buf ref_cnt, ref_off, ref_keys, ref_tmp, ref_flags, ref_runpos, rx_hist, rx_hoff;
 	Buf np_norm, np_pa, np_pb, np_depth, np_ids, np_pairs, np_flag, np_pos, np_order, np_classes, np_bsum;
 	Buf bp_bsum;  // block sums of the cooperative cell scan
+	Buf cell_cs;  // packed (start, cursor) words of the cells
 	Buf in_T, in_A, in_B, in_C, in_R, in_ID, in_pos, in_rot, in_act, out_aabb, out_pairs, out_norm, out_pa, out_pb,
 	    out_depth, out_bids;
 	// batch scratch: offsets, scene of each shape, global body ids, per-scene
@@ -312,6 +313,9 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	b.pre_zeroed = c->pass_zeroed;
 	b.owner_cursor = c->fused_now ? ptr<uint32_t>(c->owner_off) : nullptr;
 	b.scan_bsum = c->bp_bsum.p ? ptr<unsigned long long>(c->bp_bsum) : nullptr;
+	b.cell_cs = c->cell_cs.p && c->cell_cs.bytes >= sizeof(unsigned long long) * c->gp.g_max
+	                ? ptr<unsigned long long>(c->cell_cs)
+	                : nullptr;
 	b.sm = c->sm;
 	b.dense = ptr<uint2>(c->dense);
 	b.dense_cap = c->dense.bytes / sizeof(uint2);
@@ -384,6 +388,7 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 
 	c->fused_now = !g_override && fused_sort_enabled() && fused_sort_fits(owner_buckets(n, c->owner_shift));
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
 	CC_TRY(ensure(c, c->bp_bsum, sizeof(unsigned long long) * kScanCoopBlocks));
+	CC_TRY(ensure(c, c->cell_cs, sizeof(unsigned long long) * c->gp.g_max));
 	CC_TRY(ensure(c, c->cell_count, sizeof(uint32_t) * c->gp.g_max));
 	CC_TRY(ensure(c, c->cell_start, sizeof(uint32_t) * (c->gp.g_max + 1)));
 	CC_TRY(ensure(c, c->owner_count, sizeof(uint32_t) * std::max<uint64_t>(n, 1)));
@@ -493,7 +498,7 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 	}
 	{
 		StageMark m(c, ST_SCATTER, s);
-		launch_scatter(n, aabb, b, s);  // the cell scan left the counts zeroed
+		launch_scatter(n, aabb, b, s, b.scan_bsum && b.cell_cs);  // the cell scan wrote the packed cursors
 	}
 	{
 		StageMark m(c, ST_PAIR_TEST, s);
@@ -972,7 +977,7 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
 	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges,
-	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals,   &c->bp_bsum};
+	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals,   &c->bp_bsum,    &c->cell_cs};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
 	c->g_collide.drop();

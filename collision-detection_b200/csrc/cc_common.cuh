@@ -41,6 +41,29 @@ __host__ __device__ inline float ord2f_host(uint32_t k) {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
+// 16-byte global -> shared copy that bypasses the registers (cp.async, L2
+// only); both addresses 16-byte aligned. cp_async_wait_all waits for this
+// thread's copies; a __syncwarp/__syncthreads after it publishes them.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// 32-byte global accesses (sm_100 256-bit vector ld/st): one L2 request where
+// two 16-byte accesses make two. The address must be 32-byte aligned.
+__device__ __forceinline__ void st_global_v8(float *p, float4 a, float4 b) {
+	asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x), "f"(a.y), "f"(a.z),
+	             "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+	             : "memory");
+}
+__device__ __forceinline__ void ld_global_v8(const float *p, float4 &a, float4 &b) {
+	asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+	             : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+	             : "l"(p)
+	             : "memory");
+}
+
 template <class T>
 __device__ __forceinline__ T warp_incl_scan(T v) {
 #pragma unroll

@@ -172,6 +172,10 @@ struct BpBuffers {
 	// non-null: the cell offsets come from the cooperative scan
 	// (k_scan_cells_coop), these kScanCoopBlocks words hold its block sums
 	unsigned long long *scan_bsum = nullptr;
+	// g_max words (start << 32 | cursor) the cooperative scan writes with
+	// cursor 0: the scatter takes a slot with one 64-bit atomic instead of a
+	// start load plus a cursor atomic (launch_scatter with packed = true)
+	unsigned long long *cell_cs = nullptr;
 };
 constexpr uint32_t kScanCoopBlocks = 2048;
 // Owner buckets of n bodies at a shift.
@@ -185,7 +189,7 @@ void launch_bounds(uint64_t n, const float *aabb, DevStats *stats, const GridPar
 // In-place shift + per-cell counts on the plan's search grid.
 void launch_count(uint64_t n, float *aabb, const BpBuffers &b, cudaStream_t s);
 void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
-void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
+void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s, bool packed = false);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
 // Incremental steps (one scene; the plan's search grid carried over from the
