@@ -1065,7 +1065,7 @@ __global__ void __launch_bounds__(kFusedNT) k_owner_sort_fused(DevStats *stats, 
 	if (!fits) return;  // uniform over the grid: no block reaches the barrier
 	// 1. exclusive scan of the bucket counts: coalesced loads into shared
 	// memory (all in flight at once), then one contiguous run per thread
-	for (uint32_t b = threadIdx.x; b < nbk; b += kFusedNT) off[b] = owner_count[b];
+	copy_words_to_shared<kFusedNT>(off, owner_count, nbk);
 	__syncthreads();
 	const uint32_t per = (nbk + kFusedNT - 1) / kFusedNT;
 	const uint32_t b0 = min(nbk, threadIdx.x * per), b1 = min(nbk, b0 + per);
@@ -1262,7 +1262,13 @@ __global__ void __launch_bounds__(kCsNT) k_scan_cells_coop(DevStats *stats, uint
 	const uint64_t per = ((n + gridDim.x - 1) / gridDim.x + kCsTile - 1) / kCsTile * kCsTile;
 	const uint64_t lo = min(n, (uint64_t)blockIdx.x * per), hi = min(n, lo + per);
 	unsigned long long part = 0;
-	for (uint64_t i = lo + threadIdx.x; i < hi; i += kCsNT) part += counts[i];
+	for (uint64_t i0 = lo + threadIdx.x; i0 < hi; i0 += 8 * kCsNT) {  // 8 loads in flight
+		uint32_t v[8];
+#pragma unroll
+		for (int q = 0; q < 8; q++) v[q] = i0 + q * kCsNT < hi ? counts[i0 + q * kCsNT] : 0u;
+#pragma unroll
+		for (int q = 0; q < 8; q++) part += v[q];
+	}
 	unsigned long long total;
 	(void)block_excl_scan<unsigned long long, kCsNT>(part, sm, &total);
 	if (threadIdx.x == 0) bsum[blockIdx.x] = total;
@@ -1328,7 +1334,7 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
 			return v;
 		}();
 		const unsigned grid = (unsigned)std::max<uint64_t>(
-		    1, std::min<uint64_t>((uint64_t)g_max / (2 * kCsTile), std::min<uint64_t>((uint64_t)per_sm * kNumSMs,
+		    1, std::min<uint64_t>((uint64_t)g_max / (8 * kCsTile), std::min<uint64_t>((uint64_t)per_sm * kNumSMs,
 		                                                                               kScanCoopBlocks)));
 		DevStats *st = b.stats;
 		uint32_t gm = g_max, *cnt = b.cell_count, *start = b.cell_start;

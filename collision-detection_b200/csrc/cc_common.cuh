@@ -50,6 +50,25 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// n words global -> shared, every thread keeping 8 loads in flight (a plain
+// strided loop waits for each load before issuing the next).
+template <int NT>
+__device__ __forceinline__ void copy_words_to_shared(uint32_t *dst, const uint32_t *__restrict__ src, uint32_t n) {
+	for (uint32_t b0 = threadIdx.x; b0 < n; b0 += 8 * NT) {
+		uint32_t v[8];
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const uint32_t b = b0 + q * NT;
+			v[q] = b < n ? src[b] : 0u;
+		}
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const uint32_t b = b0 + q * NT;
+			if (b < n) dst[b] = v[q];
+		}
+	}
+}
+
 // 32-byte global accesses (sm_100 256-bit vector ld/st): one L2 request where
 // two 16-byte accesses make two. The address must be 32-byte aligned.
 __device__ __forceinline__ void st_global_v8(float *p, float4 a, float4 b) {
