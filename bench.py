@@ -797,7 +797,9 @@ def run_ours(args):
     e2e = {"value": world * scene.n / (e2e_ms / 1000.0), "unit": UNIT, "ms_per_step": e2e_ms,
            "h2d_bytes_per_step": hp.input_bytes(), "d2h_bytes_per_step": hp.output_bytes(),
            "how": "cc_collide_host_submit/_wait, two steps in flight, pinned host buffers; CUDA events on the "
-                  "caller's stream around all steps",
+                  "caller's stream around all steps; every input array is copied each step except C, which the "
+                  "library reads from the pinned buffer only for CONE and TRIANGLEMESH shapes (none in this "
+                  "scene)",
            "blocking": {"ms_per_step": blocking_ms, "value": world * scene.n / (blocking_ms / 1000.0),
                         "how": "cc_collide_host, one step at a time"}}
     assert (hq.n_pairs, hq.n_contacts) == (hs.n_pairs, hs.n_contacts)

@@ -430,8 +430,16 @@ def collide(ds: DeviceScene, grid=(16, 16, 16), envelope=0.0, ctx: Context | Non
     dev = ds.T.device
     if aabb is None:
         aabb = torch.zeros((2 * ds.n, 3), dtype=torch.float32, device=dev)
+    # a call whose pair output was too small has already shifted `aabb` in
+    # place: the retry starts again from the caller's boxes (those of RECT and
+    # TRIANGLEMESH shapes are not regenerated)
+    aabb_in = aabb.clone()
     cap = int(pairs_cap or max(1024, ds.n // 4))
+    first = True
     while True:
+        if not first:
+            aabb.copy_(aabb_in)
+        first = False
         pairs = torch.empty(cap, dtype=torch.int64, device=dev)
         norm = torch.empty((cap, 3), dtype=torch.float32, device=dev)
         cpta, cptb = torch.empty_like(norm), torch.empty_like(norm)
@@ -455,14 +463,21 @@ def collide(ds: DeviceScene, grid=(16, 16, 16), envelope=0.0, ctx: Context | Non
 
 class HostSession:
     """End-to-end use from host memory (cc_collide_host): the scene lives in
-    pinned host buffers; every run() copies it to the device, runs the
-    pipeline and copies pairs and contacts back into pinned host buffers."""
+    pinned host buffers (pageable ones with pinned=False); every run() copies
+    it to the device, runs the pipeline and copies pairs and contacts back into
+    pinned host buffers."""
 
     def __init__(self, scene, grid=(16, 16, 16), envelope=0.0, ctx: Context | None = None, pairs_cap=None,
-                 want_aabb=False):
+                 want_aabb=False, pinned=True):
         self.ctx = ctx or default_context()
         self.grid, self.envelope = tuple(int(g) for g in grid), float(envelope)
-        pin = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).pin_memory()  # noqa: E731
+        self.pinned = bool(pinned)
+        # the count of shapes whose third array (C) the device reads: CONE and TRIANGLEMESH
+        self.c_shapes = int(np.count_nonzero((np.asarray(scene.T) == 5) | (np.asarray(scene.T) == 6)))
+
+        def pin(a, dt):
+            t = torch.from_numpy(np.ascontiguousarray(a, dtype=dt))
+            return t.pin_memory() if self.pinned else t.clone()
         self.n, self.nb = scene.n, scene.nb
         self.want_aabb = want_aabb
         self.n_pairs = self.n_contacts = 0
@@ -476,7 +491,8 @@ class HostSession:
     def _alloc(self, cap):
         self.cap = cap
         e = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True)  # noqa: E731
-        self.aabb = e((2 * self.n, 3), torch.float32) if self.want_aabb else None
+        if getattr(self, "aabb", None) is None:  # kept on regrowth: it holds the caller's input boxes
+            self.aabb = e((2 * self.n, 3), torch.float32) if self.want_aabb else None
         self.pairs = e(cap, torch.int64)
         self.norm, self.cpta, self.cptb = (e((cap, 3), torch.float32), e((cap, 3), torch.float32),
                                            e((cap, 3), torch.float32))
@@ -485,9 +501,15 @@ class HostSession:
 
     def input_bytes(self, poses_only=False):
         """Host-to-device bytes of one step: every input array, or with static
-        shapes (Context.set_static_shapes) the body poses and flags alone."""
-        ts = self.inputs[6:] if poses_only else self.inputs
-        return int(sum(t.numel() * t.element_size() for t in ts))
+        shapes (Context.set_static_shapes) the body poses and flags alone. From
+        pinned buffers the library reads C only for the CONE and TRIANGLEMESH
+        shapes (12 bytes each), so only those bytes of C count."""
+        if poses_only:
+            return int(sum(t.numel() * t.element_size() for t in self.inputs[6:]))
+        total = int(sum(t.numel() * t.element_size() for t in self.inputs))
+        if self.pinned:
+            total -= self.inputs[3].numel() * self.inputs[3].element_size() - 12 * self.c_shapes
+        return total
 
     def output_bytes(self):
         k = self.n_contacts

@@ -196,6 +196,24 @@ __global__ void __launch_bounds__(kNT) k_gather(uint64_t n, uint32_t S, const un
 	}
 }
 
+// The third shape array (C) of the shapes that read it: CONE, which GenerateAABB
+// bounds as a triangle (AABBGenerator.cu:103-107), and TRIANGLEMESH, whose
+// third vertex the support map and centre use (Narrowphase.cu:11-17, 44-47).
+// `src` is the caller's pinned host array, read through its device mapping, so
+// a scene without such shapes moves none of its bytes over PCIe.
+__global__ void __launch_bounds__(kNT) k_gather_c(uint64_t n, const int32_t *__restrict__ T,
+                                                   const float *__restrict__ src, float *__restrict__ dst) {
+	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kNT) {
+		const int t = __ldg(T + i);
+		if (t == CONE || t == TRIANGLEMESH) {
+			const float x = src[3 * i], y = src[3 * i + 1], z = src[3 * i + 2];
+			dst[3 * i] = x;
+			dst[3 * i + 1] = y;
+			dst[3 * i + 2] = z;
+		}
+	}
+}
+
 // Counter-based random numbers for the time-step update: SplitMix64's output
 // function (Steele, Lea, Flood 2014) applied to seed + counter, so every body
 // draws the same numbers whatever the launch shape.
@@ -322,6 +340,12 @@ void launch_gather(uint64_t n, uint64_t nb, uint32_t S, const unsigned long long
 		const unsigned g = (unsigned)std::min<uint64_t>((nb + kNT - 1) / kNT, (uint64_t)kNumSMs * 16);
 		k_gather<true><<<g, kNT, 0, s>>>(nb, S, body_off, src, dst);
 	}
+}
+
+void launch_gather_c(uint64_t n, const int32_t *T, const float *src, float *dst, cudaStream_t s) {
+	if (!n) return;
+	const unsigned g = (unsigned)std::min<uint64_t>((n + kNT - 1) / kNT, (uint64_t)kNumSMs * 8);
+	k_gather_c<<<g, kNT, 0, s>>>(n, T, src, dst);
 }
 
 void launch_batch_prep(uint64_t n, uint32_t S, const unsigned long long *shape_off, const unsigned long long *body_off,

@@ -1654,7 +1654,29 @@ cc_status host_copy_out(cc_ctx *c, cc_ctx::HostSlot &h, cc_result *res, uint64_t
 
 // The six shape arrays of a host step (T, A, B, C, R, ID) into dst, unless
 // static shapes are on and dst already holds these host arrays' contents.
-cc_status upload_shapes(cc_ctx *c, cc_ctx::ShapeCopy &sh, Buf *const dst[6], const cc_scene *sc, cudaStream_t t) {
+// The device address of a pinned, mapped host array; null for pageable memory.
+const void *mapped_host(const void *p) {
+	static const bool off = [] {
+		const char *v = getenv("CC_GATHER_C");
+		return v && v[0] == '0';
+	}();
+	if (off) return nullptr;
+	cudaPointerAttributes a;
+	if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+		cudaGetLastError();
+		return nullptr;
+	}
+	return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
+// The six shape arrays to the device. C is read only for CONE and
+// TRIANGLEMESH shapes, so from a pinned host array it is not copied whole:
+// *gather_c receives its device mapping and the caller gathers those shapes'
+// C with launch_gather_c once T is on the device, on its compute stream (a
+// kernel on the copy stream would hold the later copies until the SMs are free).
+cc_status upload_shapes(cc_ctx *c, cc_ctx::ShapeCopy &sh, Buf *const dst[6], const cc_scene *sc, cudaStream_t t,
+                        const float **gather_c) {
+	*gather_c = nullptr;
 	const void *src[6] = {sc->T, sc->A, sc->B, sc->C, sc->R, sc->ID};
 	static const uint64_t bytes[6] = {4, 12, 12, 12, 16, 4};
 	bool same = c->static_shapes && sh.gen == c->shapes_gen && sh.n == sc->n;
@@ -1662,8 +1684,12 @@ cc_status upload_shapes(cc_ctx *c, cc_ctx::ShapeCopy &sh, Buf *const dst[6], con
 		same = same && sh.src[k] == src[k] && sh.dst[k] == dst[k]->p && sh.allocs[k] == dst[k]->allocs;
 	if (same) return CC_OK;
 	sh.gen = 0;  // not valid until every copy is enqueued
+	const float *c_mapped = sc->n ? static_cast<const float *>(mapped_host(sc->C)) : nullptr;
 	for (int k = 0; k < 6; k++) {
-		CC_CUDA(c, cudaMemcpyAsync(dst[k]->p, src[k], bytes[k] * sc->n, cudaMemcpyHostToDevice, t));
+		if (k == 3 && c_mapped)
+			*gather_c = c_mapped;
+		else
+			CC_CUDA(c, cudaMemcpyAsync(dst[k]->p, src[k], bytes[k] * sc->n, cudaMemcpyHostToDevice, t));
 		sh.src[k] = src[k];
 		sh.dst[k] = dst[k]->p;
 		sh.allocs[k] = dst[k]->allocs;
@@ -1738,13 +1764,14 @@ cc_status cc_collide_host_submit(cc_ctx *c, const cc_scene *sc, int gx, int gy, 
 	CC_TRY(host_slot_prepare(c, h, n, nb, cap));
 	if (n) CC_TRY(prepare(c, n, cap));
 	// after the caller's prior work on `stream`
+	const float *gather_c = nullptr;
 	CC_CUDA(c, cudaEventRecord(c->hs_user, (cudaStream_t)stream));
 	CC_CUDA(c, cudaStreamWaitEvent(c->hs_copy, c->hs_user, 0));
 	{
 		StageMark m(c, ST_COPY_IN, c->hs_copy);
 		cudaStream_t t = c->hs_copy;
 		Buf *const dst[6] = {&h.T, &h.A, &h.B, &h.C, &h.R, &h.ID};
-		CC_TRY(upload_shapes(c, c->hs_shapes[c->hs_next], dst, sc, t));
+		CC_TRY(upload_shapes(c, c->hs_shapes[c->hs_next], dst, sc, t, &gather_c));
 		CC_CUDA(c, cudaMemcpyAsync(h.pos.p, sc->body_pos, 12 * nb, cudaMemcpyHostToDevice, t));
 		CC_CUDA(c, cudaMemcpyAsync(h.rot.p, sc->body_rot, 16 * nb, cudaMemcpyHostToDevice, t));
 		CC_CUDA(c, cudaMemcpyAsync(h.act.p, sc->active, nb, cudaMemcpyHostToDevice, t));
@@ -1752,6 +1779,10 @@ cc_status cc_collide_host_submit(cc_ctx *c, const cc_scene *sc, int gx, int gy, 
 		CC_CUDA(c, cudaEventRecord(h.in_done, t));
 	}
 	CC_CUDA(c, cudaStreamWaitEvent(c->hs_comp, h.in_done, 0));
+	if (gather_c) {
+		launch_gather_c(n, ptr<int32_t>(h.T), gather_c, ptr<float>(h.C), c->hs_comp);
+		c->launches += 1;
+	}
 	if (n) {
 		CC_TRY(collide_enqueue(c, h.dev, gx, gy, gz, envelope, ptr<float>(h.aabb), ptr<int64_t>(h.pairs), cap,
 		                       ptr<float>(h.norm), ptr<float>(h.pa), ptr<float>(h.pb), ptr<float>(h.depth),
@@ -1854,7 +1885,12 @@ cc_status cc_collide_host(cc_ctx *c, const cc_scene *sc, int gx, int gy, int gz,
 	std::unique_ptr<StageMark> cin(new StageMark(c, ST_COPY_IN, s));
 	{
 		Buf *const dst[6] = {&c->in_T, &c->in_A, &c->in_B, &c->in_C, &c->in_R, &c->in_ID};
-		CC_TRY(upload_shapes(c, c->in_shapes, dst, sc, s));
+		const float *gather_c = nullptr;
+		CC_TRY(upload_shapes(c, c->in_shapes, dst, sc, s, &gather_c));
+		if (gather_c) {
+			launch_gather_c(n, ptr<int32_t>(c->in_T), gather_c, ptr<float>(c->in_C), s);
+			c->launches += 1;
+		}
 	}
 	CC_CUDA(c, cudaMemcpyAsync(c->in_pos.p, sc->body_pos, 12 * nb, cudaMemcpyHostToDevice, s));
 	CC_CUDA(c, cudaMemcpyAsync(c->in_rot.p, sc->body_rot, 16 * nb, cudaMemcpyHostToDevice, s));

@@ -276,6 +276,10 @@ constexpr size_t kParamCopyMax = 64 * 1024;
 cudaError_t copy_small_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s);
 void launch_gather(uint64_t n, uint64_t nb, uint32_t S, const unsigned long long *shape_off,
                    const unsigned long long *body_off, const SceneSrc *src, const SceneDst &dst, cudaStream_t s);
+// dst[i] = src[i] (3 floats) for the shapes of type CONE or TRIANGLEMESH, the
+// only ones whose C is read; T is on the device, src a device-accessible
+// (pinned, mapped) host array.
+void launch_gather_c(uint64_t n, const int32_t *T, const float *src, float *dst, cudaStream_t s);
 void launch_batch_prep(uint64_t n, uint32_t S, const unsigned long long *shape_off, const unsigned long long *body_off,
                        const uint32_t *ID, uint32_t *scene_of, uint32_t *gid, uint32_t *err, cudaStream_t s);
 void launch_batch_bounds(uint64_t n, const float *aabb, const uint32_t *scene_of, SceneStats *sst, uint32_t *err,

@@ -278,7 +278,11 @@ CC_API cc_status cc_perturb_scenes(cc_ctx *ctx, uint64_t count, const uint64_t *
 
 /* Same with HOST pointers in `scene` and `res` (pinned memory recommended):
  * the inputs are copied to context-owned device buffers, the pipeline runs,
- * and aabb (if non-NULL), pairs and contacts are copied back. */
+ * and aabb (if non-NULL), pairs and contacts are copied back. The third shape
+ * array C is read only for CONE (bounded as a triangle) and TRIANGLEMESH
+ * shapes: from a pinned host array a kernel fetches C for those shapes alone
+ * through its device mapping (no bytes for a scene without them); a pageable C
+ * is copied whole (environment CC_GATHER_C=0 copies it whole always). */
 CC_API cc_status cc_collide_host(cc_ctx *ctx, const cc_scene *scene, int gx, int gy, int gz, float envelope,
                           cc_result *res, void *stream);
 

@@ -3,6 +3,7 @@ steps in flight give the same results as the blocking host entry point, a
 step whose output capacity is too small is redone, and misuse is reported."""
 import numpy as np
 import pytest
+import torch
 
 from collide_b200 import scenes as S
 
@@ -62,3 +63,38 @@ def test_pipelined_misuse_is_reported(cb):
     hs.wait()
     with pytest.raises(IndexError):
         hs.wait()  # nothing in flight (the session keeps its own queue)
+
+
+def test_c_gathered_from_pinned_equals_copied_whole(cb):
+    """From pinned host buffers the library reads the third shape array (C)
+    only for CONE and TRIANGLEMESH shapes; the results equal those of pageable
+    buffers, which are copied whole, even with NaN in every other shape's C."""
+    from test_gpu_shape_types import all_types_scene
+    sc = all_types_scene(n=4000, seed=3)
+    C = sc.C.copy()
+    C[sc.T == S.CONE] = np.random.default_rng(1).uniform(-0.04, 0.04, size=((sc.T == S.CONE).sum(), 3))
+    C[(sc.T != S.CONE) & (sc.T != S.TRIANGLEMESH)] = np.nan
+    sc.C = C.astype(np.float32)
+    # the caller bounds RECT and TRIANGLEMESH shapes (GenerateAABB leaves them)
+    n = sc.n
+    init = np.zeros((2 * n, 3), np.float32)
+    p = sc.pos[sc.ID].astype(np.float32)
+    init[:n], init[n:] = p - 0.05, p + 0.05
+    out = {}
+    for pinned in (True, False):
+        hs = cb.HostSession(sc, ctx=cb.Context(), want_aabb=True, pinned=pinned)
+        snaps = []
+        for step in range(3):
+            hs.aabb.copy_(torch.from_numpy(init))
+            if step < 2:
+                hs.run()
+            else:
+                hs.submit()
+                hs.wait()
+            snaps.append(snapshot(hs) + (hs.aabb.numpy().copy(),))
+        out[pinned] = snaps
+    assert out[True][0][1] > 100  # contacts found
+    for a, b in zip(out[True], out[False]):
+        assert same(a, b)
+    hs = cb.HostSession(sc, ctx=cb.Context(), pinned=True)
+    assert hs.input_bytes() == sum(t.numel() * t.element_size() for t in hs.inputs) - 12 * (n - hs.c_shapes)
