@@ -81,10 +81,12 @@ def perturb_many(ctx: Context, updates, sigma=1e-4, max_angle=1e-3):
 class PinnedScene:
     """A host scene in one pinned buffer laid out exactly as its device copy
     (the nine arrays at 256-byte aligned offsets), so an upload is a single
-    copy into arena space."""
+    copy into arena space. C comes last: it is read only for CONE and
+    TRIANGLEMESH shapes, so a scene without them uploads everything before it
+    (the arena keeps C's space; nothing reads it)."""
 
-    FIELDS = (("T", np.int32), ("A", np.float32), ("B", np.float32), ("C", np.float32), ("R", np.float32),
-              ("ID", np.int32), ("pos", np.float32), ("rot", np.float32), ("active", np.uint8))
+    FIELDS = (("T", np.int32), ("A", np.float32), ("B", np.float32), ("R", np.float32), ("ID", np.int32),
+              ("pos", np.float32), ("rot", np.float32), ("active", np.uint8), ("C", np.float32))
 
     def __init__(self, scene):
         self.scene = scene
@@ -97,6 +99,10 @@ class PinnedScene:
             self.layout.append((k, off, a.shape, dt))
             off += _align(a.nbytes)
         self.total = off
+        T = arrays["T"]
+        needs_c = bool(np.any((T == 5) | (T == 6)))  # CONE, TRIANGLEMESH
+        #: bytes an upload copies
+        self.copy_bytes = self.total if needs_c else next(o for k, o, _, _ in self.layout if k == "C")
         with numa_local():  # pages on the GPU's NUMA node
             self.buf = torch.empty(max(self.total, 1), dtype=torch.uint8, pin_memory=True)
             host = self.buf.numpy()
@@ -117,11 +123,12 @@ class PinnedScene:
         it); without it the scene gets one new allocation."""
         if space is None:
             space = torch.empty(max(self.total, 1), dtype=torch.uint8, device=device)
+        k = self.copy_bytes
         if copy_stream is None:
-            space[:self.total].copy_(self.buf[:self.total], non_blocking=True)
+            space[:k].copy_(self.buf[:k], non_blocking=True)
         else:
             with torch.cuda.stream(copy_stream):
-                space[:self.total].copy_(self.buf[:self.total], non_blocking=True)
+                space[:k].copy_(self.buf[:k], non_blocking=True)
         return ArenaScene(space, self.layout, self.n, self.nb)
 
 
@@ -550,7 +557,7 @@ class Server:
                         timing["admit_s"] += time.perf_counter() - ta
                         if sid is not None:
                             arrivals.append((self.resident[sid], q.seed))
-                            timing["upload_bytes"] += self.pool[q.scene].total
+                            timing["upload_bytes"] += self.pool[q.scene].copy_bytes
                     else:
                         sid = self.slots[q.scene % len(self.slots)]
                         if sid not in self.resident:
