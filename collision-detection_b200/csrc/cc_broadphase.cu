@@ -487,14 +487,20 @@ __global__ void __launch_bounds__(kNT, 5) k_pair_test(const DevStats *stats, con
 			const uint64_t beg = cell_start[c];
 			const uint64_t end = min((uint64_t)cell_start[c + 1], entry_cap);
 			my_n = (int)(end > e + 1 ? end - e - 1 : 0);
-			if (dense && end - beg > dense_cell) {  // left to k_pair_test_dense
-				my_n = 0;
-				if (e == beg) {
-					const uint32_t chunks = (uint32_t)((end - beg + kNT - 1) / kNT);
-					const unsigned long long at = atomicAdd(dense_count, (unsigned long long)chunks);
-					for (uint32_t q = 0; q < chunks; q++)
-						if (at + q < dense_cap) dense[at + q] = make_uint2(c, q * kNT);
-						else atomicOr(err, (uint32_t)kErrCapacity);
+			if (end - beg > dense_cell) {
+				if (dense) {  // left to k_pair_test_dense
+					my_n = 0;
+					if (e == beg) {
+						const uint32_t chunks = (uint32_t)((end - beg + kNT - 1) / kNT);
+						const unsigned long long at = atomicAdd(dense_count, (unsigned long long)chunks);
+						for (uint32_t q = 0; q < chunks; q++)
+							if (at + q < dense_cap) dense[at + q] = make_uint2(c, q * kNT);
+							else atomicOr(err, (uint32_t)kErrCapacity);
+					}
+				} else if (e == beg) {
+					// no dense-cell kernel this call (the last found no dense
+					// cell): tested here, and counted so the next call has one
+					atomicAdd(dense_count, 1ull);
 				}
 			}
 		}

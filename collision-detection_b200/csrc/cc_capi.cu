@@ -99,6 +99,10 @@ struct cc_ctx {
 	// this call's pairs are emitted by the fused owner sort (one scene, not
 	// incremental, few owner buckets); set by prepare and the call
 	bool fused_now = false;
+	// one scene whose last call found no dense cell: the dense-cell pair test is
+	// not launched (the sparse one tests every cell and counts dense ones)
+	bool dense_skip = false;
+	uint64_t last_dense = 1;  // dense cells of the last call (1: none seen yet)
 	uint64_t last_E = 0, last_P = 0;
 	int last_dim[3] = {0, 0, 0};
 	// owner buckets of the pair sort (BpBuffers::owner_shift / key_bits), chosen
@@ -317,7 +321,7 @@ BpBuffers bp_buffers(cc_ctx *c) {
 	                ? ptr<unsigned long long>(c->cell_cs)
 	                : nullptr;
 	b.sm = c->sm;
-	b.dense = ptr<uint2>(c->dense);
+	b.dense = c->dense_skip ? nullptr : ptr<uint2>(c->dense);
 	b.dense_cap = c->dense.bytes / sizeof(uint2);
 	b.dense_cell = c->gp.dense_cell;
 	b.owner_shift = c->owner_shift;
@@ -386,6 +390,7 @@ cc_status prepare(cc_ctx *c, uint64_t n, uint64_t np_cap, uint64_t g_override = 
 		choose_owner_shift(c, n);
 	}
 	c->fused_now = !g_override && fused_sort_enabled() && fused_sort_fits(owner_buckets(n, c->owner_shift));
+	c->dense_skip = !g_override && c->last_dense == 0;
 	CC_TRY(ensure(c, c->stats, sizeof(DevStats)));
 	CC_TRY(ensure(c, c->bp_bsum, sizeof(unsigned long long) * kScanCoopBlocks));
 	CC_TRY(ensure(c, c->cell_cs, sizeof(unsigned long long) * c->gp.g_max));
@@ -483,7 +488,7 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 			StageMark m(c, ST_SCAN_OWNER, s);
 			launch_scan_owner(n, b, s);
 		}
-		c->launches += 9;  // with the dense-cell pair test
+		c->launches += c->dense_skip ? 8 : 9;  // with the dense-cell pair test unless skipped
 		return;
 	}
 	c->inc_valid = false;  // the kept cell lists are overwritten
@@ -509,7 +514,8 @@ void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool inc
 		StageMark m(c, ST_SCAN_OWNER, s);
 		launch_scan_owner(n, b, s);
 	}
-	c->launches += owner_scan ? 6 : 5;  // count, cell scan, scatter, sparse + dense pair test, owner scan
+	// count, cell scan, scatter, sparse + dense pair test, owner scan
+	c->launches += (owner_scan ? 6 : 5) - (c->dense_skip ? 1 : 0);
 }
 
 // Sorted pair list into `out` (device-driven: writes nothing if the pair
@@ -636,7 +642,7 @@ cc_status settle(cc_ctx *c, uint64_t n, float *aabb, unsigned long long *out, ui
 		if (!keep_lists) launch_scatter(n, aabb, b, s);
 		launch_pair_test(n, b, E, s);
 		if (!c->fused_now) launch_scan_owner(n, b, s);
-		c->launches += (keep_lists ? 3 : 4) - (c->fused_now ? 1 : 0);
+		c->launches += (keep_lists ? 3 : 4) - (c->fused_now ? 1 : 0) - (c->dense_skip ? 1 : 0);
 		if (out) enqueue_emit(c, n, out, out_cap, s);
 		if (np) enqueue_np(c, *np, out_cap, &ptr<DevStats>(c->stats)->np_n, s);
 		CC_TRY(check_launch(c));
@@ -670,6 +676,7 @@ cc_status sort_fallback(cc_ctx *c, uint64_t n, uint64_t P, unsigned long long *o
 void remember(cc_ctx *c) {
 	c->last_E = c->h_stats->entries;
 	c->last_P = c->h_stats->pairs;
+	c->last_dense = c->h_stats->dense_items;
 	for (int d = 0; d < 3; d++) c->last_dim[d] = c->h_stats->plan.dim[d];
 }
 
@@ -851,7 +858,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	struct {
 		uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
 		const void *p[18];
-		int dims[3], prec, oshift, kbits, ov, fused;
+		int dims[3], prec, oshift, kbits, ov, fused, dense_skip;
 		float env;
 		GridParams gp;
 		uint64_t hslots;
@@ -866,6 +873,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	k.dims[0] = gx; k.dims[1] = gy; k.dims[2] = gz; k.prec = c->np_precision; k.env = envelope; k.gp = c->gp;
 	k.oshift = c->owner_shift; k.kbits = c->key_bits; k.ov = ov ? 1 : 0; k.hslots = ov ? c->np_hslots : 0;
 	k.fused = c->fused_now ? 1 : 0;
+	k.dense_skip = c->dense_skip ? 1 : 0;
 	return run_graphed(c, c->g_collide, &k, sizeof(k), enqueue_all, s);
 }
 
@@ -1064,6 +1072,7 @@ cc_status cc_set_pair_test_shape(cc_ctx *c, int window, int blocks_per_sm) {
 cc_status cc_set_dense_cell(cc_ctx *c, uint32_t entries) {
 	if (!c) return CC_ERR_INVALID_ARGUMENT;
 	c->gp.dense_cell = entries ? std::max<uint32_t>(entries, kDenseCell) : 0xffffffffu;
+	c->last_dense = 1;  // the next call launches the dense-cell kernel and counts again
 	return CC_OK;
 }
 

@@ -123,6 +123,29 @@ def test_search_grid_does_not_change_pairs(cb, dims):
     assert np.array_equal(p, po), pair_set_diff(p, po)
 
 
+def test_dense_kernel_skipped_after_sparse_calls(cb):
+    """A context whose last call found no dense cell launches no dense-cell
+    kernel; a dense scene then is tested by the lane-per-entry kernel alone
+    (same pairs) and turns the dense-cell kernel back on for the next call."""
+    sparse = O.aabb(S.spheres_uniform(16384, seed=0))
+    _, ps = O.broadphase(sparse, (16, 16, 16))
+    dense = O.aabb(S.clustered_spheres(60_000, seed=2, clusters=2, sigma=0.01, background=0.05))
+    _, pd = O.broadphase(dense, (64, 64, 64))
+    ctx = cb.Context()
+    launches = []
+    for a, want in ((sparse, ps), (sparse, ps), (dense, pd), (dense, pd), (sparse, ps)):
+        _, p = gpu_broadphase(cb, a, (16, 16, 16), ctx)
+        assert np.array_equal(p, want), pair_set_diff(p, want)
+        launches.append(ctx.launches())
+    assert launches[1] == launches[0] - 1  # no dense cell in the first call: none launched in the second
+    # the dense scene's first call skipped it but counted its dense cells, so the
+    # next call runs as on a context that saw the dense scene from the start
+    fresh = cb.Context()
+    for _ in range(2):
+        gpu_broadphase(cb, dense, (16, 16, 16), fresh)
+    assert launches[3] == fresh.launches()
+
+
 @pytest.mark.parametrize("target,ratio", [(1.0, 1.0), (4.0, 2.0), (32.0, 0.5), (0.25, 8.0)])
 def test_tuning_does_not_change_pairs(cb, target, ratio):
     s = S.clustered_spheres(200_000, seed=1)
