@@ -129,7 +129,8 @@ static V3 F(support)(int type, V3 A, V3 B, V3 C, Q4 R, V3 b) {
 #define SWAP3(a, b) do { V3 t_ = (a); (a) = (b); (b) = t_; } while (0)
 
 /* Optional iteration record (test diagnostics): when set, each MPR call
- * stores phase1 * 1000 + phase2 at the sink's cursor. */
+ * stores phase1 * 1000 + phase2 at the sink's cursor (0 for a call that ends
+ * before the discovery loop). */
 static int32_t *F(g_iter_sink) = 0;
 static uint64_t F(g_iter_n) = 0;
 #define CCO_ITERS(p1, p2) do { if (F(g_iter_sink)) F(g_iter_sink)[F(g_iter_n)++] = (p1) * 1000 + (p2); } while (0)
@@ -142,9 +143,10 @@ static int F(mpr)(int tA, V3 AX, V3 AY, V3 AZ, Q4 AR, int tB, V3 BX, V3 BY, V3 B
 	V3 n = F(neg)(v0);
 	V3 v11 = SUP_A(F(neg)(n)), v12 = SUP_B(n);
 	V3 v1 = F(sub)(v12, v11);
-	if (F(dot)(v1, n) <= 0.0) return 0;
+	if (F(dot)(v1, n) <= 0.0) { CCO_ITERS(0, 0); return 0; }
 	n = F(cross)(v1, v0);
 	if (F(iszero3)(n)) {
+		CCO_ITERS(0, 0);
 		n = F(sub)(v1, v0);
 		n = F(normalize)(n);
 		*rn = n;
@@ -154,7 +156,7 @@ static int F(mpr)(int tA, V3 AX, V3 AY, V3 AZ, Q4 AR, int tB, V3 BX, V3 BY, V3 B
 	}
 	V3 v21 = SUP_A(F(neg)(n)), v22 = SUP_B(n);
 	V3 v2 = F(sub)(v22, v21);
-	if (F(dot)(v2, n) <= 0.0) return 0;
+	if (F(dot)(v2, n) <= 0.0) { CCO_ITERS(0, 0); return 0; }
 	n = F(cross)(F(sub)(v1, v0), F(sub)(v2, v0));
 	if (F(dot)(n, v0) > 0.0) {
 		SWAP3(v1, v2); SWAP3(v11, v21); SWAP3(v12, v22);

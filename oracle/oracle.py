@@ -213,6 +213,47 @@ def narrowphase(scene, pairs, envelope=0.0, prec="f64"):
     return _np_call(fn, scene, pairs, envelope)
 
 
+TYPE_NAMES = ("sphere", "ellipsoid", "box", "cylinder", "rect", "cone", "trianglemesh")
+
+
+def mpr_iterations(scene, pairs, prec="f64"):
+    """Portal discovery and refinement iterations of every MPR call of the
+    restated DoNarrowphase (CollideAndFindPoint, Narrowphase.cu:122-314), per
+    shape-type class. Pairs that reach MPR are those not skipped by the
+    active / same-body filters (:344-349) and not sphere-sphere (:382-397),
+    evaluated in list order, so the record of call k belongs to the k-th of
+    them. Returns {(type_a, type_b): dict(pairs, discovery_mean, discovery_max,
+    refinement_mean, refinement_max)} with type_a <= type_b."""
+    L = lib()
+    T, A, B, C, R, ID, pos, rot, act = _scene_args(scene)
+    pr = _c(pairs, np.int64)
+    a, b = (pr >> 32).astype(np.int64), (pr & 0xFFFFFFFF).astype(np.int64)
+    ida, idb = ID.astype(np.int64)[a], ID.astype(np.int64)[b]
+    ta, tb = T[a], T[b]
+    live = (act[ida] != 0) | (act[idb] != 0)
+    mpr = live & (ida != idb) & ~((ta == 0) & (tb == 0))
+    sink = np.zeros(max(int(mpr.sum()), 1), np.int32)
+    getattr(L, f"cco_iter_sink_{prec}")(_p(sink))
+    try:
+        _np_call(getattr(L, f"cco_narrowphase_{prec}_api"), scene, pr, 0.0)
+        cnt = getattr(L, f"cco_iter_count_{prec}")
+        cnt.restype = U64
+        got = int(cnt())
+    finally:
+        getattr(L, f"cco_iter_sink_{prec}")(None)
+    assert got == int(mpr.sum()), (got, int(mpr.sum()))
+    rec = sink[:got]
+    p1, p2 = rec // 1000, rec % 1000
+    lo, hi = np.minimum(ta[mpr], tb[mpr]), np.maximum(ta[mpr], tb[mpr])
+    out = {}
+    for x, y in sorted(set(zip(lo.tolist(), hi.tolist()))):
+        m = (lo == x) & (hi == y)
+        out[(TYPE_NAMES[x], TYPE_NAMES[y])] = dict(
+            pairs=int(m.sum()), discovery_mean=float(p1[m].mean()), discovery_max=int(p1[m].max()),
+            refinement_mean=float(p2[m].mean()), refinement_max=int(p2[m].max()))
+    return out
+
+
 def ref_narrowphase(scene, pairs, envelope=0.0, prec="f32"):
     """The reference's own DoNarrowphase in real=float or real=double."""
     return _np_call(ref(prec).ccref_narrowphase, scene, pairs, envelope)

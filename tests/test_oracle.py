@@ -170,3 +170,18 @@ def test_reference_thread_flags_do_not_change_pairs():
     _, p0 = O.ref_broadphase(a, (16, 16, 16), par=[0] * 10)
     _, p1 = O.ref_broadphase(a, (16, 16, 16), par=[1] * 10)
     assert np.array_equal(p0, p1)
+
+
+def test_mpr_iteration_counts_per_class():
+    """The FP64 oracle's iteration record covers every MPR call (early exits
+    included) and stays within the reference's 35-iteration caps
+    (Narrowphase.cu:201-205, 253)."""
+    m = S.mixed_slab(20_000, seed=4, extent=(0.6, 0.6, 0.1))
+    a = O.aabb(m)
+    _, p = O.broadphase(a, (16, 16, 16))
+    it = O.mpr_iterations(m, p)  # asserts one record per MPR call
+    assert sum(v["pairs"] for v in it.values()) > 500
+    assert ("sphere", "sphere") not in it  # analytic, no MPR
+    for v in it.values():
+        assert 0 <= v["discovery_mean"] <= v["discovery_max"] <= 35
+        assert 0 <= v["refinement_mean"] <= v["refinement_max"] <= 35
