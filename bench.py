@@ -325,6 +325,57 @@ def bench_small(cb, dev, steps=200):
             "l2": "not flushed (the scene is 1.4 MB)"}
 
 
+INCREMENTAL_MARGIN = 2.0  # mean box extents (cc_set_incremental)
+
+
+def bench_incremental(cb, dev, scene, tuned, steps=60):
+    """A time-step loop over the 1M scene: before every step all bodies move by
+    N(0, 1e-4^2) and turn by at most 1e-3 rad (cc_perturb_bodies, outside the
+    timed region); each cc_collide step is timed with CUDA events, with full
+    rebuilds and with the incremental broadphase (candidate lists), and every
+    step's pairs and contacts are compared between the two."""
+    import torch
+    from collide_b200 import serving as SV
+    from collide_b200 import tuner
+    out, ref = {}, []
+    for mode in ("full", "incremental"):
+        ds = cb.DeviceScene(scene, device=dev)
+        ctx = cb.Context()
+        tuner.apply(ctx, tuned)
+        if mode == "incremental":
+            ctx.set_incremental(True, INCREMENTAL_MARGIN)
+        pipe = cb.DevicePipeline(ds, grid=BINS, ctx=ctx)
+        for _ in range(3):
+            pipe.run()
+        times, rebuilds, same = [], 0, True
+        for k in range(steps):
+            SV.perturb_(ctx, ds, 7000 + k, sigma=1e-4, max_angle=1e-3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            pipe.run()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            P, C = pipe.n_pairs, pipe.n_contacts
+            o = (P, C, pipe.pairs[:P].cpu().numpy().tobytes(), pipe.norm[:C].cpu().numpy().tobytes(),
+                 pipe.depth[:C].cpu().numpy().tobytes())
+            if mode == "full":
+                ref.append(o)
+            else:
+                same = same and o == ref[k]
+                rebuilds += int(ctx.last_step_rebuilt() == 1)
+        ms = statistics.median(times)
+        out[mode] = {"ms_per_step_median": ms, "ms_per_step_mean": statistics.mean(times),
+                     "value": scene.n / (ms / 1000.0), "unit": "bodies/s"}
+        if mode == "incremental":
+            out[mode].update({"rebuild_steps": rebuilds, "margin_mean_extents": INCREMENTAL_MARGIN,
+                              "identical_to_full_every_step": same})
+    out["workload"] = (f"{WORKLOAD}; {steps} steps, before each all bodies move by N(0,1e-4^2) and turn by <= "
+                       "1e-3 rad; the step time excludes the move")
+    out["speedup_median"] = out["full"]["ms_per_step_median"] / out["incremental"]["ms_per_step_median"]
+    return out
+
+
 SERVE_WORKLOAD = ("served: Poisson arrivals, 70% time-step updates of a resident scene (positions N(0,1e-4^2), turns "
                   "<= 1e-3 rad), 30% new scenes; 4,096 resident scenes of log-uniform [2,000, 500,000] mixed shapes "
                   "(128 generated scenes, each placed 32 times with its own seeded displacement field); a new scene "
@@ -891,6 +942,7 @@ def run_ours(args):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_batch:
+        line["incremental"] = bench_incremental(cb, dev, scene, tuned)
         line["small"] = bench_small(cb, dev)
         line["batched"] = bench_batched(cb, ctx, dev)
     if rank == 0 and world == 1 and not args.no_serve:

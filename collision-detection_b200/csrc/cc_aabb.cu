@@ -123,8 +123,7 @@ int resident_blocks(K kernel) {
 
 void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
-                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s, const ZeroList &zero,
-                 const IncState *inc, float inc_margin) {
+                 uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s, const ZeroList &zero) {
 	if (n == 0) return;
 	// persistent grid: as many blocks as are resident at once
 	static const int per_sm[2] = {resident_blocks(k_aabb<false>), resident_blocks(k_aabb<true>)};
@@ -136,8 +135,6 @@ void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, c
 	pa.gy = grid ? grid[1] : 1;
 	pa.gz = grid ? grid[2] : 1;
 	pa.n = n;
-	pa.inc = inc;
-	pa.inc_margin = inc_margin;
 	if (stats)
 		launch_pdl(k_aabb<true>, dim3(blocks), dim3(kNT), 0, s, n, T, A, B, C, R, ID, nb, pos, rot, aabb, stats, err, pa, zero);
 	else

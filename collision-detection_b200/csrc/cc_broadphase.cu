@@ -113,15 +113,6 @@ __device__ __forceinline__ CellRange cell_range(const Plan &p, float3 mn, float3
 	r.c1[2] = cell_of(mx.z, p.lo[2], p.inv[2], p.dim[2]);
 	return r;
 }
-// The cells a box enters: its own range, or (incremental steps) the range of
-// the box inflated by the plan's margin.
-__device__ __forceinline__ CellRange entry_range(const Plan &p, float3 mn, float3 mx) {
-	if (p.margin > 0.f) {
-		const float m = p.margin;
-		return cell_range(p, f3(mn.x - m, mn.y - m, mn.z - m), f3(mx.x + m, mx.y + m, mx.z + m));
-	}
-	return cell_range(p, mn, mx);
-}
 __device__ __forceinline__ uint32_t pack_cell(int x, int y, int z) {
 	return (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20);
 }
@@ -244,110 +235,14 @@ __global__ void __launch_bounds__(kNT) k_count(uint64_t n, float *__restrict__ a
 			for (int x = r.c0[0]; x <= r.c1[0]; x++) atomicAdd(&cell_count[cell_index(p, base, x, y, z)], 1u);
 }
 
-// ---- incremental steps (one scene)
-__device__ __forceinline__ unsigned long long pack_range(const CellRange &r) {
-	unsigned long long v = 0;
-	for (int d = 0; d < 3; d++) v |= ((unsigned long long)r.c0[d] << (20 * d)) | ((unsigned long long)r.c1[d] << (20 * d + 10));
-	return v;
-}
-
-// Shift in place (as k_count), zero the owner counts, and check that every
-// box still lies inside the cells it was entered in (its inflated range of
-// the step that built the lists); one that left them means rebuilding.
-__global__ void __launch_bounds__(kNT) k_count_inc(uint64_t n, float *__restrict__ aabb, DevStats *stats,
-                                                    uint32_t *__restrict__ owner_count,
-                                                    unsigned long long *__restrict__ ranges) {
-	__shared__ Plan sp;
-	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
-	if (threadIdx.x < sizeof(Plan) / 4)
-		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
-	__syncthreads();
-	if (!sp.valid) return;
-	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
-	load_tile_aabb(aabb, n, i0, stage);
-	__syncthreads();
-	for (int k = threadIdx.x; k < 6 * kNT; k += kNT) stage[k] = stage[k] + sp.origin[k % 3];
-	__syncthreads();
-	store_tile_aabb(aabb, n, i0, stage);
-	const uint64_t i = i0 + threadIdx.x;
-	bool changed = false;
-	if (i < n) {
-		const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
-		const float *hs = stage + 3 * kNT;
-		const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
-		owner_count[i] = 0u;
-		// the box must still lie in the cells it was entered in
-		const CellRange r = cell_range(sp, mn, mx);
-		const unsigned long long k = ranges[i];
-		for (int d = 0; d < 3; d++) {
-			const int c0 = (int)((k >> (20 * d)) & 1023), c1 = (int)((k >> (20 * d + 10)) & 1023);
-			if (r.c0[d] < c0 || r.c1[d] > c1) changed = true;
-		}
-	}
-	if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) atomicOr(&stats->rebuild, 1u);
-}
-
-// Counting pass of a rebuilding incremental step (the boxes are already
-// shifted): enters each box inflated by the plan's margin and records the
-// range; otherwise only tells the cell scan to do nothing.
-__global__ void __launch_bounds__(kNT) k_count_gated(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
-                                                      uint32_t *__restrict__ cell_count,
-                                                      unsigned long long *__restrict__ ranges) {
-	if (blockIdx.x == 0 && threadIdx.x == 0) stats->cells_scan = stats->rebuild ? stats->cells : 0ull;
-	if (!stats->rebuild || !stats->plan.valid) return;
-	__shared__ Plan sp;
-	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
-	if (threadIdx.x < sizeof(Plan) / 4)
-		reinterpret_cast<uint32_t *>(&sp)[threadIdx.x] = reinterpret_cast<const uint32_t *>(&stats->plan)[threadIdx.x];
-	const uint64_t i0 = (uint64_t)blockIdx.x * kNT;
-	load_tile_aabb(aabb, n, i0, stage);
-	__syncthreads();
-	const uint64_t i = i0 + threadIdx.x;
-	if (i >= n) return;
-	const float3 mn = f3(stage[3 * threadIdx.x], stage[3 * threadIdx.x + 1], stage[3 * threadIdx.x + 2]);
-	const float *hs = stage + 3 * kNT;
-	const float3 mx = f3(hs[3 * threadIdx.x], hs[3 * threadIdx.x + 1], hs[3 * threadIdx.x + 2]);
-	const CellRange r = entry_range(sp, mn, mx);
-	ranges[i] = pack_range(r);
-	for (int z = r.c0[2]; z <= r.c1[2]; z++)
-		for (int y = r.c0[1]; y <= r.c1[1]; y++)
-			for (int x = r.c0[0]; x <= r.c1[0]; x++) atomicAdd(&cell_count[cell_index(sp, 0, x, y, z)], 1u);
-}
-
-// A step that keeps its cell lists: the entries get the bodies' new (shifted)
-// boxes; the entry count is the last step's.
-__global__ void __launch_bounds__(kNT) k_refresh_entries(uint64_t n, const float *__restrict__ aabb, DevStats *stats,
-                                                          float4 *__restrict__ entries, uint64_t entry_cap,
-                                                          const IncState *inc) {
-	if (stats->rebuild || !stats->plan.valid) return;
-	const uint64_t E = min((uint64_t)inc->entries, entry_cap);
-	if (blockIdx.x == 0 && threadIdx.x == 0) stats->entries = E;
-	for (uint64_t e = (uint64_t)blockIdx.x * kNT + threadIdx.x; e < E; e += (uint64_t)gridDim.x * kNT) {
-		float4 lo = entries[2 * e], hi = entries[2 * e + 1];
-		const uint32_t id = __float_as_uint(lo.w);
-		if (id >= n) continue;
-		lo.x = aabb[3 * id]; lo.y = aabb[3 * id + 1]; lo.z = aabb[3 * id + 2];
-		hi.x = aabb[3 * (n + id)]; hi.y = aabb[3 * (n + id) + 1]; hi.z = aabb[3 * (n + id) + 2];
-		entries[2 * e] = lo;
-		entries[2 * e + 1] = hi;
-	}
-}
-
-__global__ void k_save_inc(const DevStats *stats, IncState *inc) {
-	inc->plan = stats->plan;
-	inc->entries = stats->entries;
-	inc->valid = stats->plan.valid && !(stats->err & (kErrCapacity | kErrSpinLimit)) ? 1u : 0u;
-}
-
 // Cell-ordered entries: one thread per body, a cursor atomic per covered cell.
 template <bool kBatch>
 __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__restrict__ aabb, const DevStats *stats,
                                                   const uint32_t *__restrict__ cell_start,
                                                   uint32_t *__restrict__ cursor, float4 *__restrict__ entries,
-                                                  uint64_t cap, uint32_t *err, SceneMap sm, const uint32_t *gate,
+                                                  uint64_t cap, uint32_t *err, SceneMap sm,
                                                   unsigned long long *__restrict__ cs) {
 	pdl_begin();
-	if (gate && *gate == 0u) return;  // an incremental step that keeps its cell lists
 	__shared__ Plan sp;
 	__shared__ __align__(16) float stage[6 * kNT];  // read and written as float4
 	if (threadIdx.x < sizeof(Plan) / 4)
@@ -363,7 +258,7 @@ __global__ void __launch_bounds__(kNT) k_scatter(uint64_t n, const float *__rest
 	uint32_t base;
 	const Plan &p = plan_of<kBatch>(sp, sm, i, base);
 	if (kBatch && !p.valid) return;
-	const CellRange r = entry_range(p, mn, mx);
+	const CellRange r = cell_range(p, mn, mx);
 	bool over = false;
 	const float4 elo = make_float4(mn.x, mn.y, mn.z, __uint_as_float((uint32_t)i));
 	const auto put = [&](uint64_t slot, uint32_t packed) {
@@ -1358,10 +1253,10 @@ void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStrea
 	unsigned long long *cs = packed ? b.cell_cs : nullptr;
 	if (b.sm.plans)
 		launch_pdl(k_scatter<true>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count,
-		           b.entries, b.entry_cap, &b.stats->err, b.sm, (const uint32_t *)nullptr, cs);
+		           b.entries, b.entry_cap, &b.stats->err, b.sm, cs);
 	else
 		launch_pdl(k_scatter<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count,
-		           b.entries, b.entry_cap, &b.stats->err, b.sm, (const uint32_t *)nullptr, cs);
+		           b.entries, b.entry_cap, &b.stats->err, b.sm, cs);
 }
 
 template <bool kBatch, int kWin>
@@ -1392,26 +1287,6 @@ void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cud
 	launch_pair_test_dense(b, s);
 }
 
-void launch_count_inc(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s) {
-	if (n) k_count_inc<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.owner_count, ranges);
-}
-void launch_count_gated(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s) {
-	if (n) k_count_gated<<<blocks_for(n), kNT, 0, s>>>(n, aabb, b.stats, b.cell_count, ranges);
-}
-void launch_scan_cells_gated(const BpBuffers &b, uint32_t g_max, cudaStream_t s) {
-	launch_scan_u32_to_u32(b.cell_count, g_max, b.cell_start, b.status, b.ticket, &b.stats->err, s,
-	                       &b.stats->cells_scan, &b.stats->entries, b.pre_zeroed, b.cell_count);
-}
-void launch_scatter_gated(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s) {
-	if (n) launch_pdl(k_scatter<false>, dim3(blocks_for(n)), dim3(kNT), 0, s, n, aabb, b.stats, b.cell_start, b.cell_count, b.entries,
-	                                                      b.entry_cap, &b.stats->err, b.sm, (const uint32_t *)&b.stats->rebuild,
-	                                                      (unsigned long long *)nullptr);
-}
-void launch_refresh_entries(uint64_t n, const float *aabb, const BpBuffers &b, const IncState *inc, cudaStream_t s) {
-	const unsigned grid = kNumSMs * 8;
-	k_refresh_entries<<<grid, kNT, 0, s>>>(n, aabb, b.stats, b.entries, b.entry_cap, inc);
-}
-void launch_save_inc(const BpBuffers &b, IncState *inc, cudaStream_t s) { k_save_inc<<<1, 1, 0, s>>>(b.stats, inc); }
 
 void launch_pair_test_dense(const BpBuffers &b, cudaStream_t s) {
 	if (!b.dense || !b.dense_cap) return;

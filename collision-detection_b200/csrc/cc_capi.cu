@@ -146,12 +146,17 @@ struct cc_ctx {
 	// look-back status regions (words) of the cell, owner and contact-flag
 	// scans, laid out back to back in `status`
 	uint64_t st_words[3] = {0, 0, 0};
-	// incremental broadphase (cc_set_incremental): per-body cell ranges and
-	// the last step's grid; usable while n and the scratch stay the same
+	// incremental broadphase (cc_set_incremental, cc_verlet.cu): the sorted
+	// candidate pairs of the boxes inflated by inc_margin mean extents, the
+	// rebuild's unshifted boxes, a copy of the current step's unshifted boxes,
+	// and the filter's flags and positions; the candidates are used while the
+	// scene keeps its size (and the buffers holding them were not moved)
 	bool incremental = false, inc_valid = false;
-	float inc_margin = 0.5f;  // insertion margin in mean box extents
-	uint64_t inc_n = 0, inc_gen = 0;
-	Buf inc_state, inc_ranges;
+	float inc_margin = 0.5f;
+	uint64_t inc_n = 0, inc_allocs = 0, inc_nc = 0;
+	float inc_m = 0.f, inc_disp = 0.f;  // the rebuild's margin; the last step's largest displacement
+	int last_rebuilt = -1;
+	Buf v_ref, v_backup, v_scratch, v_cand, v_flags, v_pos, v_status;
 	// the current pass's first kernel zeroed the scan control words, the
 	// narrowphase class counters and the cell counts (ZeroList)
 	bool pass_zeroed = false;
@@ -460,38 +465,9 @@ uint64_t hint_E(const cc_ctx *c, uint64_t n) { return pow2ceil(std::max<uint64_t
 uint64_t hint_P(const cc_ctx *c) { return pow2ceil(std::max<uint64_t>(c->last_P, 1)); }
 
 // count .. owner scan: needs stats zeroed and the plan from the bounds pass.
-void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool incremental = false,
-                    bool owner_scan = true) {
+void enqueue_search(cc_ctx *c, uint64_t n, float *aabb, cudaStream_t s, bool owner_scan = true) {
 	BpBuffers b = bp_buffers(c);
 	const uint32_t gmax = c->gp.g_max;
-	if (incremental) {
-		{
-			StageMark m(c, ST_COUNT, s);
-			launch_count_inc(n, aabb, b, ptr<unsigned long long>(c->inc_ranges), s);
-			launch_count_gated(n, aabb, b, ptr<unsigned long long>(c->inc_ranges), s);
-		}
-		{
-			StageMark m(c, ST_SCAN_CELLS, s);
-			launch_scan_cells_gated(b, gmax, s);
-		}
-		{
-			StageMark m(c, ST_SCATTER, s);
-			launch_scatter_gated(n, aabb, b, s);
-			launch_refresh_entries(n, aabb, b, ptr<IncState>(c->inc_state), s);
-		}
-		{
-			StageMark m(c, ST_PAIR_TEST, s);
-			launch_pair_test(n, b, hint_E(c, n), s);
-		}
-		launch_save_inc(b, ptr<IncState>(c->inc_state), s);
-		{
-			StageMark m(c, ST_SCAN_OWNER, s);
-			launch_scan_owner(n, b, s);
-		}
-		c->launches += c->dense_skip ? 8 : 9;  // with the dense-cell pair test unless skipped
-		return;
-	}
-	c->inc_valid = false;  // the kept cell lists are overwritten
 	{
 		StageMark m(c, ST_COUNT, s);
 		if (!b.pre_zeroed) cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * gmax, s);
@@ -634,15 +610,12 @@ cc_status settle(cc_ctx *c, uint64_t n, float *aabb, unsigned long long *out, ui
 			CC_TRY(ensure(c, c->dense, sizeof(uint2) * ((E + E / 8) / kDenseCell + 1024)));
 		}
 		if (P > b.pair_cap) CC_TRY(ensure(c, c->pairs_tmp, sizeof(unsigned long long) * (P + P / 8)));
-		// an incremental step that kept its cell lists has them in place (its
-		// entry count is unchanged); any other step scatters them again
-		const bool keep_lists = c->incremental && !c->sm.plans && c->h_stats->rebuild == 0;
 		CC_TRY(reset_pass_counters(c, n, s));
 		b = bp_buffers(c);
-		if (!keep_lists) launch_scatter(n, aabb, b, s);
+		launch_scatter(n, aabb, b, s);
 		launch_pair_test(n, b, E, s);
 		if (!c->fused_now) launch_scan_owner(n, b, s);
-		c->launches += (keep_lists ? 3 : 4) - (c->fused_now ? 1 : 0) - (c->dense_skip ? 1 : 0);
+		c->launches += 4 - (c->fused_now ? 1 : 0) - (c->dense_skip ? 1 : 0);
 		if (out) enqueue_emit(c, n, out, out_cap, s);
 		if (np) enqueue_np(c, *np, out_cap, &ptr<DevStats>(c->stats)->np_n, s);
 		CC_TRY(check_launch(c));
@@ -782,13 +755,6 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	const uint64_t n = sc.n;
 	PdlScope pdl_(n);
 	CC_TRY(prepare(c, n, pairs_cap));
-	const bool inc = c->incremental && !c->sm.plans;
-	if (inc) c->fused_now = false;  // the incremental count kernels keep the five-launch owner path
-	if (inc) {
-		CC_TRY(ensure(c, c->inc_ranges, sizeof(unsigned long long) * n));
-		CC_TRY(ensure(c, c->inc_state, sizeof(IncState)));
-	}
-	const bool inc_ready = inc && c->inc_valid && c->inc_n == n && c->inc_gen == c->buf_gen;
 	// overlapped narrowphase: one scene, an output of at most 2^24 pairs
 	const bool ov = c->np_overlap && pairs_cap > 0 && pairs_cap <= ((uint64_t)1 << 24);
 	if (ov) {
@@ -799,7 +765,6 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 		CC_TRY(ensure(c, c->np_hkeys, sizeof(unsigned long long) * c->np_hslots));
 		CC_TRY(ensure(c, c->np_hvals, sizeof(uint32_t) * c->np_hslots));
 	}
-	c->inc_valid = false;  // set again once this step has finished cleanly
 	DevStats *d = ptr<DevStats>(c->stats);
 	const int grid[3] = {gx, gy, gz};
 	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
@@ -827,20 +792,19 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 			StageMark m(c, ST_AABB, st);
 			CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), st));
 			launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb, d, &d->err,
-			            c->gp, grid, st, zero, inc_ready ? ptr<IncState>(c->inc_state) : nullptr,
-			            inc ? c->inc_margin : 0.f);
+			            c->gp, grid, st, zero);
 		}
 		c->launches += 1;
 		c->pass_zeroed = true;
 		if (ov) {
-			enqueue_search(c, n, aabb, st, inc, false);
+			enqueue_search(c, n, aabb, st, false);
 			const cc_status r = enqueue_sort_and_np_overlapped(c, n, a, pairs_cap, st);
 			c->pass_zeroed = false;
 			return r;
 		}
 		{
 			StageMark m(c, ST_SPAN_BROADPHASE, st);
-			enqueue_search(c, n, aabb, st, inc);
+			enqueue_search(c, n, aabb, st);
 			enqueue_emit(c, n, out, pairs_cap, st);
 		}
 		{
@@ -856,7 +820,7 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	}
 	// everything the captured launches depend on
 	struct {
-		uint64_t n, nb, pairs_cap, hE, hP, gen, st[3], incm;
+		uint64_t n, nb, pairs_cap, hE, hP, gen, st[3];
 		const void *p[18];
 		int dims[3], prec, oshift, kbits, ov, fused, dense_skip;
 		float env;
@@ -866,7 +830,6 @@ cc_status collide_enqueue(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz,
 	memset(&k, 0, sizeof(k));
 	k.n = n; k.nb = sc.nb; k.pairs_cap = pairs_cap; k.hE = hint_E(c, n); k.hP = hint_P(c); k.gen = c->buf_gen;
 	for (int r = 0; r < 3; r++) k.st[r] = c->st_words[r];
-	k.incm = (inc ? 2u : 0u) | (inc_ready ? 1u : 0u);
 	const void *ps[18] = {sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, aabb,
 	                      pairs, norm, cpta, cptb, depth, bids, nullptr, nullptr};
 	memcpy(k.p, ps, sizeof(ps));
@@ -919,6 +882,129 @@ cc_status collide_finish(cc_ctx *c, const cc_scene &sc, float envelope, float *a
 	return CC_OK;
 }
 
+// One incremental step of one scene (cc_set_incremental; cc_verlet.cu). A
+// rebuild step (the first, a new size, moved candidate buffers, a step that
+// used more than half of the margin last time, or a redo) searches the boxes
+// inflated by the margin with the full broadphase into the sorted candidate
+// list and keeps the unshifted boxes as the reference; every step then checks
+// the displacement, shifts the boxes in place, keeps the candidates that
+// overlap (in order) and runs the narrowphase on them. A step that moved too
+// far is redone as a rebuild from its unshifted boxes. Two synchronizes in a
+// rebuild step, one otherwise.
+cc_status collide_verlet(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
+                         int64_t *pairs, uint64_t pairs_cap, float *norm, float *cpta, float *cptb, float *depth,
+                         int32_t *bids, uint64_t *n_pairs, uint64_t *n_contacts, cudaStream_t s) {
+	const uint64_t n = sc.n;
+	PdlScope pdl_(n);
+	const int grid[3] = {gx, gy, gz};
+	unsigned long long *out = reinterpret_cast<unsigned long long *>(pairs);
+	const NpArgs a = {n, sc.nb, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.active, sc.body_pos, sc.body_rot, envelope,
+	                  pairs, norm, cpta, cptb, depth, bids};
+	for (int attempt = 0; attempt < 2; attempt++) {
+		CC_TRY(prepare(c, n, pairs_cap));
+		DevStats *d = ptr<DevStats>(c->stats);  // (allocated by the first prepare)
+		c->pass_zeroed = false;
+		CC_TRY(ensure(c, c->v_ref, 24 * n));
+		CC_TRY(ensure(c, c->v_backup, 24 * n));
+		const uint64_t allocs = c->v_ref.allocs + c->v_cand.allocs;
+		const bool rebuild = attempt > 0 || !c->inc_valid || c->inc_n != n || c->inc_allocs != allocs ||
+		                     c->inc_disp > 0.25f * c->inc_m;
+		const auto enqueue_front = [&](cudaStream_t st) -> cc_status {
+			CC_CUDA(c, cudaMemsetAsync(d, 0, sizeof(DevStats), st));
+			launch_aabb(n, sc.T, sc.A, sc.B, sc.C, sc.R, sc.ID, sc.nb, sc.body_pos, sc.body_rot, aabb, d, &d->err,
+			            c->gp, grid, st);
+			c->launches += 1;
+			return CC_OK;
+		};
+		if (rebuild) {
+			CC_TRY(enqueue_front(s));
+			c->inc_valid = false;
+			CC_TRY(ensure(c, c->v_scratch, 24 * n));
+			const uint64_t want = std::max<uint64_t>(2 * c->inc_nc, std::max<uint64_t>(c->last_P, n / 4) + 1024);
+			CC_TRY(ensure(c, c->v_cand, sizeof(unsigned long long) * want));
+			float *scratch = ptr<float>(c->v_scratch);
+			unsigned long long *cand = ptr<unsigned long long>(c->v_cand);
+			CC_CUDA(c, cudaMemcpyAsync(c->v_ref.p, aabb, 24 * n, cudaMemcpyDeviceToDevice, s));
+			launch_vinflate(n, aabb, scratch, d, c->inc_margin, s);
+			uint64_t cap = c->v_cand.bytes / sizeof(unsigned long long);
+			enqueue_search(c, n, scratch, s);
+			enqueue_emit(c, n, cand, cap, s);
+			c->launches += 1;
+			CC_TRY(check_launch(c));
+			CC_TRY(read_stats(c, s));
+			CC_TRY(device_err(c));
+			CC_TRY(settle(c, n, scratch, cand, cap, nullptr, s));
+			uint64_t nc = c->h_stats->pairs;
+			if (nc > cap) {  // more candidates than the list holds: grow it and emit the retained pairs
+				CC_TRY(ensure(c, c->v_cand, sizeof(unsigned long long) * (nc + nc / 8)));
+				cand = ptr<unsigned long long>(c->v_cand);
+				cap = c->v_cand.bytes / sizeof(unsigned long long);
+				retain(c, n, nc);
+				CC_TRY(emit_retained(c, cand, cap, s));
+				c->retained = false;
+				CC_TRY(check_launch(c));
+				CC_TRY(read_stats(c, s));
+			}
+			if (c->h_stats->err & kErrSegmentTooLong) CC_TRY(sort_fallback(c, n, nc, cand, s));
+			c->inc_nc = nc;
+			c->inc_m = c->h_stats->vmargin;
+			// the step goes on with its own counters: clear what the search left
+			CC_CUDA(c, cudaMemsetAsync(&d->err, 0, sizeof(uint32_t), s));
+			CC_CUDA(c, cudaMemsetAsync(&d->pairs, 0, sizeof(unsigned long long), s));
+			CC_CUDA(c, cudaMemsetAsync(&d->np_n, 0, sizeof(unsigned long long), s));
+			CC_CUDA(c, cudaMemsetAsync(&d->contacts, 0, sizeof(unsigned long long), s));
+			CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 3 * sizeof(unsigned long long), s));
+		}
+		const uint64_t nc = c->inc_nc;
+		CC_TRY(ensure(c, c->v_flags, sizeof(uint32_t) * std::max<uint64_t>(nc, 1)));
+		CC_TRY(ensure(c, c->v_pos, sizeof(unsigned long long) * (nc + 1)));
+		CC_TRY(ensure(c, c->v_status, sizeof(uint64_t) * status_words_for(nc + 1)));
+		const auto enqueue_tail = [&](cudaStream_t st) -> cc_status {
+			{
+				StageMark m(c, ST_COUNT, st);
+				launch_vcheck(n, aabb, ptr<float>(c->v_ref), ptr<float>(c->v_backup), d, st);
+			}
+			{
+				StageMark m(c, ST_PAIR_TEST, st);
+				const unsigned long long *cand = ptr<unsigned long long>(c->v_cand);
+				launch_vfilter(nc, cand, aabb, n, d, ptr<uint32_t>(c->v_flags), rebuild, c->inc_m, st);
+				launch_scan_u32_to_u64(ptr<uint32_t>(c->v_flags), nc, ptr<unsigned long long>(c->v_pos),
+				                       ptr<uint64_t>(c->v_status), ptr<uint32_t>(c->ticket) + 12, &d->err, st);
+				launch_vscatter(nc, cand, ptr<uint32_t>(c->v_flags), ptr<unsigned long long>(c->v_pos), out, pairs_cap,
+				                d, st);
+			}
+			c->launches += 4;
+			enqueue_np(c, a, pairs_cap, &d->np_n, st);
+			return CC_OK;
+		};
+		if (!rebuild) CC_TRY(enqueue_front(s));
+		CC_TRY(enqueue_tail(s));
+		CC_TRY(check_launch(c));
+		CC_TRY(read_stats(c, s));
+		CC_TRY(device_err(c));
+		if (c->h_stats->vbad) {  // moved too far: back to the unshifted boxes, redo as a rebuild
+			CC_CUDA(c, cudaMemcpyAsync(aabb, c->v_backup.p, 24 * n, cudaMemcpyDeviceToDevice, s));
+			continue;
+		}
+		c->last_rebuilt = rebuild ? 1 : 0;
+		c->inc_disp = c->h_stats->vdisp ? ord2f_host(c->h_stats->vdisp) : 0.f;
+		c->inc_valid = true;
+		c->inc_n = n;
+		c->inc_allocs = c->v_ref.allocs + c->v_cand.allocs;
+		const uint64_t P = c->h_stats->pairs;
+		c->last_P = P;
+		*n_pairs = P;
+		if (P > pairs_cap)
+			return set_err(c, CC_ERR_CAPACITY, "pair list needs %llu entries, capacity %llu", (unsigned long long)P,
+			               (unsigned long long)pairs_cap);
+		if (c->h_stats->err & kErrBadIndex)
+			return set_err(c, CC_ERR_INVALID_INPUT, "a pair index is >= n or a body id is >= nb");
+		*n_contacts = c->h_stats->contacts;
+		return CC_OK;
+	}
+	return set_err(c, CC_ERR_INTERNAL, "incremental step did not settle");
+}
+
 // GenerateAABB -> broadphase -> narrowphase on device pointers with one
 // synchronize in the common case.
 cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, float envelope, float *aabb,
@@ -928,17 +1014,16 @@ cc_status collide_dev(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, flo
 	*n_contacts = 0;
 	c->retained = false;
 	if (sc.n == 0) return CC_OK;
+	if (c->incremental)
+		return collide_verlet(c, sc, gx, gy, gz, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids,
+		                      n_pairs, n_contacts, s);
 	CC_TRY(collide_enqueue(c, sc, gx, gy, gz, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids, s,
 	                       true));
 	const uint64_t gen = c->buf_gen;
 	CC_TRY(read_stats(c, s));
 	const cc_status st = collide_finish(c, sc, envelope, aabb, pairs, pairs_cap, norm, cpta, cptb, depth, bids,
 	                                    n_pairs, n_contacts, s);
-	if (st == CC_OK && c->incremental && !c->sm.plans && c->buf_gen == gen) {
-		c->inc_valid = true;  // the next step of this size may keep the cell lists
-		c->inc_n = sc.n;
-		c->inc_gen = gen;
-	}
+	(void)gen;
 	return st;
 }
 
@@ -984,7 +1069,7 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_off,    &c->b_scene_of, &c->b_gid,      &c->b_sst,    &c->b_plans,     &c->b_G,
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
-	               &c->g_act,    &c->g_src,      &c->g_off,      &c->inc_state, &c->inc_ranges,
+	               &c->g_act,    &c->g_src,      &c->g_off,      &c->v_ref,    &c->v_backup,   &c->v_scratch, &c->v_cand,   &c->v_flags,   &c->v_pos,     &c->v_status,
 	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals,   &c->bp_bsum,    &c->cell_cs};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);
@@ -1042,7 +1127,7 @@ cc_status cc_set_search_grid(cc_ctx *c, int gx, int gy, int gz) {
 	return CC_OK;
 }
 
-int cc_last_step_rebuilt(const cc_ctx *c) { return c && c->h_stats ? (int)(c->h_stats->rebuild != 0) : -1; }
+int cc_last_step_rebuilt(const cc_ctx *c) { return c ? c->last_rebuilt : -1; }
 
 cc_status cc_set_incremental(cc_ctx *c, int on, float margin) {
 	if (!c || !(margin > 0.f)) return CC_ERR_INVALID_ARGUMENT;
@@ -1113,7 +1198,7 @@ cc_status cc_set_graph_replay(cc_ctx *c, int on) {
 	if (!on) {
 		c->g_collide.drop();
 		c->g_batch.drop();
-	}
+		}
 	return CC_OK;
 }
 
@@ -1235,7 +1320,6 @@ cc_status cc_broadphase_fetch(cc_ctx *c, int64_t *pairs, uint64_t pairs_cap, voi
 cc_status cc_broadphase_bins(cc_ctx *c, uint64_t n, float *aabb, int gx, int gy, int gz, uint32_t *bin_number,
                              uint32_t *body_number, uint64_t entries_cap, uint64_t *n_entries, uint32_t *active_bins,
                              uint32_t *bin_end, uint64_t active_cap, uint64_t *n_active, void *stream) {
-	if (c) c->inc_valid = false;
 	if (!c || !n_entries || !n_active) return CC_ERR_INVALID_ARGUMENT;
 	ProfGuard pg_(c, stream);
 	c->launches = 0;

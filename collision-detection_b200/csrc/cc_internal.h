@@ -20,16 +20,6 @@ struct Plan {
 	float invbin[3];  // reference inverse bin size: grid / fabs(max + fabs(min)) (:380-381)
 	int grid[3];      // reference bins per axis
 	int valid;        // bounds were finite and every box had min <= max
-	float margin;     // incremental steps: boxes enter cells inflated by this much (0 otherwise)
-	int pad_;
-};
-
-// What an incremental broadphase keeps between two steps of one scene.
-struct IncState {
-	Plan plan;                   // the last step's search grid (in its shifted frame) and shift
-	unsigned long long entries;  // its entry count
-	uint32_t valid;
-	uint32_t pad_;
 };
 
 // Per-call device state; zeroed (one memset) at the start of every call.
@@ -50,9 +40,6 @@ struct DevStats {
 	unsigned long long cells;     // plan.G as a 64-bit scan count
 	unsigned long long np_n;      // pairs handed to the narrowphase (0 if an output was too small)
 	unsigned long long dense_items;  // (cell, row chunk) work items of the dense-cell pair test
-	unsigned long long cells_scan;   // incremental steps: cells to scan (0 when the cell lists are reused)
-	uint32_t rebuild;                // incremental steps: the cell lists must be rebuilt
-	uint32_t pad2_;
 	uint32_t blocks_done;         // last-block detection of the bounds reduction
 	uint32_t pad_;
 	Plan plan;
@@ -62,6 +49,12 @@ struct DevStats {
 	uint32_t bar_np[2];
 	uint32_t bar_compact[2];
 	uint32_t bar_scan[2];  // k_scan_cells_coop
+	// incremental steps (candidate lists): largest corner displacement since
+	// the rebuild (ordered bits), a step that moved too far, the margin
+	uint32_t vdisp;
+	uint32_t vbad;
+	float vmargin;
+	uint32_t pad3_;
 };
 
 constexpr int kMaxDim = 1024;  // cells per axis (10-bit packed cell coordinates)
@@ -119,7 +112,7 @@ void radix_sort_u64(unsigned long long *keys, unsigned long long *tmp, uint64_t 
 void launch_aabb(uint64_t n, const int32_t *T, const float *A, const float *B, const float *C, const float *R,
                  const uint32_t *ID, uint64_t nb, const float *pos, const float *rot, float *aabb, DevStats *stats,
                  uint32_t *err, const GridParams &gp, const int grid[3], cudaStream_t s,
-                 const ZeroList &zero = ZeroList(), const IncState *inc = nullptr, float inc_margin = 0.f);
+                 const ZeroList &zero = ZeroList());
 
 // ------------------------------------------------------------------ broadphase
 // A batch of independent scenes laid out as one concatenated scene: every
@@ -192,17 +185,6 @@ void launch_scan_cells(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
 void launch_scatter(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s, bool packed = false);
 void launch_pair_test(uint64_t n, const BpBuffers &b, uint64_t entries_hint, cudaStream_t s);
 void launch_scan_owner(uint64_t n, const BpBuffers &b, cudaStream_t s);
-// Incremental steps (one scene; the plan's search grid carried over from the
-// last step when the scene still fits it): shift + per-body cell ranges
-// compared with the last step's (any change sets stats->rebuild); the count,
-// cell scan and scatter then run only when rebuilding, else the kept entries
-// get the new box coordinates; the last call stores the state.
-void launch_count_inc(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s);
-void launch_count_gated(uint64_t n, float *aabb, const BpBuffers &b, unsigned long long *ranges, cudaStream_t s);
-void launch_scan_cells_gated(const BpBuffers &b, uint32_t g_max, cudaStream_t s);
-void launch_scatter_gated(uint64_t n, const float *aabb, const BpBuffers &b, cudaStream_t s);
-void launch_refresh_entries(uint64_t n, const float *aabb, const BpBuffers &b, const IncState *inc, cudaStream_t s);
-void launch_save_inc(const BpBuffers &b, IncState *inc, cudaStream_t s);
 // Cells holding more than b.dense_cell entries are left out of the
 // lane-per-entry pair test and tested here instead, tile by tile (N-body
 // style); kDenseCell is the default threshold and the smallest sizing unit of
@@ -225,6 +207,24 @@ bool fused_sort_fits(uint64_t buckets);
 bool fused_sort_enabled();
 void launch_owner_sort_fused(uint64_t n, uint64_t out_cap, unsigned long long *out, uint64_t P_hint, const BpBuffers &b,
                              cudaStream_t s);
+
+// ------------------------------------------------------------------ incremental steps
+// Candidate lists for time-stepped scenes (cc_verlet.cu): the boxes inflated
+// by factor x the mean box extent (stats->vmargin receives the margin); the
+// largest corner displacement against the rebuild's reference boxes plus a
+// copy of the unshifted boxes and the in-place shift; the exact test of the
+// candidates on the shifted boxes (all false and stats->vbad set when the
+// step moved farther than the rebuild's margin allows; a rebuild step always
+// passes); the overlapping
+// candidates in order into out (stats->pairs, stats->np_n as the pair test
+// and emission set them).
+void launch_vinflate(uint64_t n, const float *aabb, float *scratch, DevStats *stats, float factor, cudaStream_t s);
+void launch_vcheck(uint64_t n, float *aabb, const float *ref, float *backup, DevStats *stats, cudaStream_t s);
+void launch_vfilter(uint64_t nc, const unsigned long long *cand, const float *aabb, uint64_t n, DevStats *stats,
+                    uint32_t *flags, bool rebuild, float margin, cudaStream_t s);
+void launch_vscatter(uint64_t nc, const unsigned long long *cand, const uint32_t *flags,
+                     const unsigned long long *pos, unsigned long long *out, uint64_t out_cap, DevStats *stats,
+                     cudaStream_t s);
 
 // ------------------------------------------------------------------ batches
 // Per-scene accumulators of the batch bounds pass (zeroed per call).

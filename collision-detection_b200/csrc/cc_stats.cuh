@@ -19,8 +19,6 @@ __device__ inline Plan make_plan(const uint32_t bmin_inv[3], const uint32_t bmax
 	const int grid[3] = {gx, gy, gz};
 	float mn[3], mx[3];
 	p.valid = (err & (kErrNonFinite | kErrInverted | kErrBadIndex)) ? 0 : 1;
-	p.margin = 0.f;
-	p.pad_ = 0;
 	for (int d = 0; d < 3; d++) {
 		mn[d] = ord2f(~bmin_inv[d]);
 		mx[d] = ord2f(bmax[d]);
@@ -68,8 +66,6 @@ struct PlanArgs {
 	GridParams gp;
 	int gx, gy, gz;
 	uint64_t n;
-	const IncState *inc = nullptr;  // incremental step: keep this search grid if the scene still fits it
-	float inc_margin = 0.f;         // incremental mode: insertion margin in mean box extents
 };
 
 // Every thread of the block calls this once with the bounds of the boxes it
@@ -155,42 +151,8 @@ __device__ __forceinline__ void accumulate_stats(float3 mn, float3 mx, bool have
 		}
 		const uint32_t err = __ldcg(&stats->err);
 		Plan p = make_plan(bmin_inv, bmax, err, ext_mean, pa.gp, pa.gx, pa.gy, pa.gz, pa.n);
-		uint32_t rebuild = 1;
-		if (pa.inc && pa.inc->valid && p.valid && pa.gp.user_dim[0] <= 0) {
-			// the last step's search grid, moved with the shift: kept while the
-			// shifted scene stays within a tenth of the grid's extent of it (the
-			// cell map clamps to the grid, so boxes outside still find edge
-			// cells; the reference shift and bin scale stay this step's own)
-			const Plan q = pa.inc->plan;
-			bool fits = true;
-			float lo[3];
-			for (int d = 0; d < 3; d++) {
-				lo[d] = q.lo[d] - q.origin[d] + p.origin[d];
-				const float hi = ord2f(bmax[d]) + p.origin[d];
-				if (q.inv[d] > 0.f) {
-					const float ext = (float)q.dim[d] / q.inv[d], tol = 0.1f * ext;
-					if (p.lo[d] < lo[d] - tol || hi > lo[d] + ext + tol) fits = false;
-				}
-			}
-			if (fits) {
-				for (int d = 0; d < 3; d++) {
-					p.lo[d] = lo[d];
-					p.inv[d] = q.inv[d];
-					p.dim[d] = q.dim[d];
-				}
-				p.G = q.G;
-				p.margin = q.margin;  // the margin the kept lists were built with
-				rebuild = 0;
-			}
-		}
-		if (rebuild) {  // lists built this step: this step's margin
-			float mean_max = 0.f;
-			for (int d = 0; d < 3; d++) mean_max = fmaxf(mean_max, (float)ext_mean[d]);
-			p.margin = pa.inc_margin > 0.f ? pa.inc_margin * mean_max : 0.f;
-		}
 		stats->plan = p;
 		stats->cells = p.G;
-		stats->rebuild = rebuild;
 	}
 }
 

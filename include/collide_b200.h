@@ -85,20 +85,22 @@ CC_API const char *cc_version(void);
  * mean box extents wide. (gx,gy,gz) > 0 pins the grid. */
 CC_API cc_status cc_set_search_grid(cc_ctx *ctx, int gx, int gy, int gz);
 CC_API cc_status cc_set_tuning(cc_ctx *ctx, float cell_target, float min_ratio);
-/* Incremental broadphase for time-step updates (default off). When lists are
- * built, every box enters the cells of itself inflated by `margin` mean box
- * extents (> 0). cc_collide keeps the search grid, those cell lists and each
- * body's entered range; while the next step has the same shape count, the
- * scene still fits that grid and every new box still lies inside the cells
- * it was entered in, the count, cell scan and scatter are skipped and the
- * kept lists get the new boxes; otherwise the lists are rebuilt. Pairs are
- * emitted from the cell holding the larger min corner of the two boxes, which
- * both boxes entered, so results are identical with it on or off. Any other
- * broadphase use of the context drops the kept state. No reference
- * counterpart. */
+/* Incremental broadphase for time-step updates (default off; the reference
+ * rebuilds every step, Broadphase.cu:344-545). A rebuild step of cc_collide
+ * (and cc_collide_host) searches the boxes inflated by `margin` (> 0) mean box
+ * extents into a sorted candidate pair list and keeps its boxes; a later step
+ * whose box corners all moved by less than half the inflation (minus a
+ * rounding allowance) tests only those candidates, exactly, on its own
+ * shifted boxes and keeps the overlapping ones in order: the sorted pair list
+ * of a full search, so results are identical with it on or off. A step that
+ * moved too far is redone as a rebuild; a rebuild also happens when the shape
+ * count changes and, ahead of time, after a step that used more than half
+ * of the allowance. Larger margins rebuild less often and test more
+ * candidates. The pipelined host calls (cc_collide_host_submit) do not use
+ * it. No reference counterpart. */
 CC_API cc_status cc_set_incremental(cc_ctx *ctx, int on, float margin);
-/* 1 if the last broadphase built its cell lists, 0 if an incremental step
- * kept them. */
+/* 1 if the last incremental step rebuilt its candidate list, 0 if it used the
+ * kept one, -1 before any incremental step. */
 CC_API int cc_last_step_rebuilt(const cc_ctx *ctx);
 /* Cells of the search grid holding more than `entries` entries (default 128,
  * at least 128; 0 = never) are tested by the tiled dense-cell kernel instead

@@ -1,7 +1,7 @@
-"""Incremental broadphase (cc_set_incremental): a moving scene stepped with
-kept cell lists gives, every step, exactly the outputs of full rebuilds —
-through small moves (lists kept), a large jump (lists rebuilt) and a scene
-that outgrows its grid (new grid)."""
+"""Incremental broadphase (cc_set_incremental): a moving scene stepped with a
+kept candidate list gives, every step, exactly the outputs of full rebuilds —
+through small moves (list kept), a large jump (rebuilt: the step that moved
+too far is redone) and a scene that outgrows its grid."""
 import numpy as np
 import pytest
 import torch
