@@ -962,7 +962,7 @@ cc_status collide_verlet(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, 
 		const auto enqueue_tail = [&](cudaStream_t st) -> cc_status {
 			{
 				StageMark m(c, ST_COUNT, st);
-				launch_vcheck(n, aabb, ptr<float>(c->v_ref), ptr<float>(c->v_backup), d, st);
+				launch_vcheck(n, aabb, ptr<float>(c->v_ref), ptr<float>(c->v_backup), sc.T, d, st);
 			}
 			{
 				StageMark m(c, ST_PAIR_TEST, st);
@@ -982,7 +982,9 @@ cc_status collide_verlet(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, 
 		CC_TRY(check_launch(c));
 		CC_TRY(read_stats(c, s));
 		CC_TRY(device_err(c));
-		if (c->h_stats->vbad) {  // moved too far: back to the unshifted boxes, redo as a rebuild
+		if (c->h_stats->vbad) {
+			// moved too far: redo as a rebuild, from the caller's RECT / TRIANGLEMESH boxes (the
+			// backup's other entries are stale; GenerateAABB rewrites those boxes first)
 			CC_CUDA(c, cudaMemcpyAsync(aabb, c->v_backup.p, 24 * n, cudaMemcpyDeviceToDevice, s));
 			continue;
 		}

@@ -48,10 +48,13 @@ __global__ void __launch_bounds__(kNT) k_vinflate(uint64_t n, const float *__res
 }
 
 // Largest corner displacement against the reference (ordered bits into
-// stats->vdisp), a copy of the unshifted boxes (for a redo), and the in-place
-// shift by fabs(min) (Broadphase.cu:382-386). Invalid input is left as it is.
+// stats->vdisp), a copy of the unshifted boxes GenerateAABB does not write
+// (RECT and TRIANGLEMESH, AABBGenerator.cu:110-111: a redo regenerates all
+// others), and the in-place shift by fabs(min) (Broadphase.cu:382-386).
+// Invalid input is left as it is.
 __global__ void __launch_bounds__(kNT) k_vcheck(uint64_t n, float *__restrict__ aabb, const float *__restrict__ ref,
-                                                 float *__restrict__ backup, DevStats *stats) {
+                                                 float *__restrict__ backup, const int32_t *__restrict__ T,
+                                                 DevStats *stats) {
 	pdl_begin();
 	__shared__ float origin[3];
 	__shared__ int valid;
@@ -64,7 +67,8 @@ __global__ void __launch_bounds__(kNT) k_vcheck(uint64_t n, float *__restrict__ 
 	for (uint64_t k = (uint64_t)blockIdx.x * kNT + threadIdx.x; k < total; k += step) {
 		const float v = aabb[k];
 		dmax = fmaxf(dmax, fabsf(v - ref[k]));
-		backup[k] = v;
+		const int t = __ldg(T + (k < 3 * n ? k : k - 3 * n) / 3);
+		if (t == RECT || t == TRIANGLEMESH) backup[k] = v;
 		aabb[k] = v + origin[k % 3];
 	}
 	dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, 16));
@@ -146,8 +150,9 @@ void launch_vinflate(uint64_t n, const float *aabb, float *scratch, DevStats *st
 	if (n) launch_pdl(k_vinflate, dim3(grid_for(6 * n)), dim3(kNT), 0, s, n, aabb, scratch, stats, factor);
 }
 
-void launch_vcheck(uint64_t n, float *aabb, const float *ref, float *backup, DevStats *stats, cudaStream_t s) {
-	if (n) launch_pdl(k_vcheck, dim3(grid_for(6 * n)), dim3(kNT), 0, s, n, aabb, ref, backup, stats);
+void launch_vcheck(uint64_t n, float *aabb, const float *ref, float *backup, const int32_t *T, DevStats *stats,
+                   cudaStream_t s) {
+	if (n) launch_pdl(k_vcheck, dim3(grid_for(6 * n)), dim3(kNT), 0, s, n, aabb, ref, backup, T, stats);
 }
 
 void launch_vfilter(uint64_t nc, const unsigned long long *cand, const float *aabb, uint64_t n, DevStats *stats,
