@@ -922,6 +922,12 @@ cc_status collide_verlet(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, 
 			CC_TRY(ensure(c, c->v_scratch, 24 * n));
 			const uint64_t want = std::max<uint64_t>(2 * c->inc_nc, std::max<uint64_t>(c->last_P, n / 4) + 1024);
 			CC_TRY(ensure(c, c->v_cand, sizeof(unsigned long long) * want));
+			// the filter's flags, positions and scan words sized with the list, so
+			// that a slightly longer list next time allocates nothing
+			const uint64_t cw = c->v_cand.bytes / sizeof(unsigned long long);
+			CC_TRY(ensure(c, c->v_flags, sizeof(uint32_t) * cw));
+			CC_TRY(ensure(c, c->v_pos, sizeof(unsigned long long) * (cw + 1)));
+			CC_TRY(ensure(c, c->v_status, sizeof(uint64_t) * status_words_for(cw + 1)));
 			float *scratch = ptr<float>(c->v_scratch);
 			unsigned long long *cand = ptr<unsigned long long>(c->v_cand);
 			CC_CUDA(c, cudaMemcpyAsync(c->v_ref.p, aabb, 24 * n, cudaMemcpyDeviceToDevice, s));
