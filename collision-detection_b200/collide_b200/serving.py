@@ -480,7 +480,8 @@ class Server:
     def _serve_batched(self, stream: Stream):
         """Continuous batching with the host side overlapped: a worker thread
         runs the passes (time-step updates, then one cc_collide_scenes over
-        the pass's scenes) on its own CUDA stream, while this thread admits
+        the pass's scenes, or cc_collide when the pass has one scene) on its
+        own CUDA stream, while this thread admits
         the next arrivals and uploads their new scenes on a copy stream. A
         pass waits for its uploads (an event); scenes referenced by a pass in
         flight are never evicted."""
@@ -510,7 +511,16 @@ class Server:
                         pass_s.wait_event(ev)
                         perturb_many(self.ctx, arrivals, NEW_SIGMA, NEW_ANGLE)
                         perturb_many(self.ctx, updates)
-                        if uniq:
+                        if len(uniq) == 1:
+                            # a pass of one scene runs as a single-scene call (its CUDA graph
+                            # replays; same results as in a batch)
+                            sid = uniq[0]
+                            one = self.collide_one(sid)
+                            for q, _ in live:
+                                q.n_pairs, q.n_contacts = one
+                                if q.record:
+                                    q.result = self._record_plain(sid)
+                        elif uniq:
                             self.batch.run(scenes)
                             co = self.batch.contact_offsets.astype(np.int64)
                             res = {sid: (int(self.batch.scene_pairs[k]), int(co[k + 1] - co[k]))
