@@ -168,10 +168,11 @@ class Context:
     def set_tuning(self, cell_target=4.0, min_ratio=2.0):
         self.check(lib.cc_set_tuning(self.h, float(cell_target), float(min_ratio)), "cc_set_tuning")
 
-    def set_incremental(self, on=True, margin=0.5):
-        """Keep the broadphase's cell lists between time steps of one scene,
-        boxes entered with `margin` mean extents of slack
-        (cc_set_incremental); results are identical either way."""
+    def set_incremental(self, on=True, margin=2.0):
+        """Time steps of one scene test a kept candidate pair list, found on
+        the boxes inflated by `margin` mean extents, while no box has moved
+        more than half that since (cc_set_incremental); results are identical
+        either way."""
         self.check(lib.cc_set_incremental(self.h, int(bool(on)), float(margin)), "cc_set_incremental")
 
     def set_static_shapes(self, on=True):
