@@ -149,14 +149,14 @@ struct cc_ctx {
 	// incremental broadphase (cc_set_incremental, cc_verlet.cu): the sorted
 	// candidate pairs of the boxes inflated by inc_margin mean extents, the
 	// rebuild's unshifted boxes, a copy of the current step's unshifted boxes,
-	// and the filter's flags and positions; the candidates are used while the
+	// and the compaction's look-back words; the candidates are used while the
 	// scene keeps its size (and the buffers holding them were not moved)
 	bool incremental = false, inc_valid = false;
 	float inc_margin = 0.5f;
 	uint64_t inc_n = 0, inc_allocs = 0, inc_nc = 0;
 	float inc_m = 0.f, inc_disp = 0.f;  // the rebuild's margin; the last step's largest displacement
 	int last_rebuilt = -1;
-	Buf v_ref, v_backup, v_scratch, v_cand, v_flags, v_pos, v_status;
+	Buf v_ref, v_backup, v_scratch, v_cand, v_status;
 	// the current pass's first kernel zeroed the scan control words, the
 	// narrowphase class counters and the cell counts (ZeroList)
 	bool pass_zeroed = false;
@@ -922,12 +922,10 @@ cc_status collide_verlet(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, 
 			CC_TRY(ensure(c, c->v_scratch, 24 * n));
 			const uint64_t want = std::max<uint64_t>(2 * c->inc_nc, std::max<uint64_t>(c->last_P, n / 4) + 1024);
 			CC_TRY(ensure(c, c->v_cand, sizeof(unsigned long long) * want));
-			// the filter's flags, positions and scan words sized with the list, so
-			// that a slightly longer list next time allocates nothing
-			const uint64_t cw = c->v_cand.bytes / sizeof(unsigned long long);
-			CC_TRY(ensure(c, c->v_flags, sizeof(uint32_t) * cw));
-			CC_TRY(ensure(c, c->v_pos, sizeof(unsigned long long) * (cw + 1)));
-			CC_TRY(ensure(c, c->v_status, sizeof(uint64_t) * status_words_for(cw + 1)));
+			// the compaction's look-back words sized with the list, so that a
+			// slightly longer list next time allocates nothing
+			CC_TRY(ensure(c, c->v_status,
+			              sizeof(uint64_t) * vcompact_status_words(c->v_cand.bytes / sizeof(unsigned long long))));
 			float *scratch = ptr<float>(c->v_scratch);
 			unsigned long long *cand = ptr<unsigned long long>(c->v_cand);
 			CC_CUDA(c, cudaMemcpyAsync(c->v_ref.p, aabb, 24 * n, cudaMemcpyDeviceToDevice, s));
@@ -962,9 +960,7 @@ cc_status collide_verlet(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, 
 			CC_CUDA(c, cudaMemsetAsync(&d->big_segments, 0, 3 * sizeof(unsigned long long), s));
 		}
 		const uint64_t nc = c->inc_nc;
-		CC_TRY(ensure(c, c->v_flags, sizeof(uint32_t) * std::max<uint64_t>(nc, 1)));
-		CC_TRY(ensure(c, c->v_pos, sizeof(unsigned long long) * (nc + 1)));
-		CC_TRY(ensure(c, c->v_status, sizeof(uint64_t) * status_words_for(nc + 1)));
+		CC_TRY(ensure(c, c->v_status, sizeof(uint64_t) * vcompact_status_words(nc)));
 		const auto enqueue_tail = [&](cudaStream_t st) -> cc_status {
 			{
 				StageMark m(c, ST_COUNT, st);
@@ -972,14 +968,10 @@ cc_status collide_verlet(cc_ctx *c, const cc_scene &sc, int gx, int gy, int gz, 
 			}
 			{
 				StageMark m(c, ST_PAIR_TEST, st);
-				const unsigned long long *cand = ptr<unsigned long long>(c->v_cand);
-				launch_vfilter(nc, cand, aabb, n, d, ptr<uint32_t>(c->v_flags), rebuild, c->inc_m, st);
-				launch_scan_u32_to_u64(ptr<uint32_t>(c->v_flags), nc, ptr<unsigned long long>(c->v_pos),
-				                       ptr<uint64_t>(c->v_status), ptr<uint32_t>(c->ticket) + 12, &d->err, st);
-				launch_vscatter(nc, cand, ptr<uint32_t>(c->v_flags), ptr<unsigned long long>(c->v_pos), out, pairs_cap,
-				                d, st);
+				launch_vcompact(nc, ptr<unsigned long long>(c->v_cand), aabb, n, d, out, pairs_cap,
+				                ptr<uint64_t>(c->v_status), ptr<uint32_t>(c->ticket) + 12, rebuild, c->inc_m, st);
 			}
-			c->launches += 4;
+			c->launches += 2;
 			enqueue_np(c, a, pairs_cap, &d->np_n, st);
 			return CC_OK;
 		};
@@ -1077,7 +1069,7 @@ void cc_ctx_destroy(cc_ctx *c) {
 	               &c->b_off,    &c->b_scene_of, &c->b_gid,      &c->b_sst,    &c->b_plans,     &c->b_G,
 	               &c->b_base,   &c->b_status,   &c->b_ticket,   &c->b_res,    &c->g_T,         &c->g_A,
 	               &c->g_B,      &c->g_C,        &c->g_R,        &c->g_ID,     &c->g_pos,       &c->g_rot,
-	               &c->g_act,    &c->g_src,      &c->g_off,      &c->v_ref,    &c->v_backup,   &c->v_scratch, &c->v_cand,   &c->v_flags,   &c->v_pos,     &c->v_status,
+	               &c->g_act,    &c->g_src,      &c->g_off,      &c->v_ref,    &c->v_backup,   &c->v_scratch, &c->v_cand,   &c->v_status,
 	               &c->np_bsum,  &c->pt_desc,    &c->np_hkeys,   &c->np_hvals,   &c->bp_bsum,    &c->cell_cs};
 	for (Buf *b : bufs)
 		if (b->p) cudaFree(b->p);

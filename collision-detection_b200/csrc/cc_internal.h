@@ -212,20 +212,19 @@ void launch_owner_sort_fused(uint64_t n, uint64_t out_cap, unsigned long long *o
 // Candidate lists for time-stepped scenes (cc_verlet.cu): the boxes inflated
 // by factor x the mean box extent (stats->vmargin receives the margin); the
 // largest corner displacement against the rebuild's reference boxes plus a
-// copy of the unshifted RECT / TRIANGLEMESH boxes and the in-place shift; the exact test of the
-// candidates on the shifted boxes (all false and stats->vbad set when the
-// step moved farther than the rebuild's margin allows; a rebuild step always
-// passes); the overlapping
-// candidates in order into out (stats->pairs, stats->np_n as the pair test
-// and emission set them).
+// copy of the unshifted RECT / TRIANGLEMESH boxes and the in-place shift; the
+// candidates that overlap on the shifted boxes, in order, into out
+// (stats->pairs and stats->np_n as the pair test and emission set them;
+// nothing, and stats->vbad set, when the step moved farther than the
+// rebuild's margin allows; a rebuild step always passes).
 void launch_vinflate(uint64_t n, const float *aabb, float *scratch, DevStats *stats, float factor, cudaStream_t s);
 void launch_vcheck(uint64_t n, float *aabb, const float *ref, float *backup, const int32_t *T, DevStats *stats,
                    cudaStream_t s);
-void launch_vfilter(uint64_t nc, const unsigned long long *cand, const float *aabb, uint64_t n, DevStats *stats,
-                    uint32_t *flags, bool rebuild, float margin, cudaStream_t s);
-void launch_vscatter(uint64_t nc, const unsigned long long *cand, const uint32_t *flags,
-                     const unsigned long long *pos, unsigned long long *out, uint64_t out_cap, DevStats *stats,
-                     cudaStream_t s);
+// Words of the status region launch_vcompact needs for nc candidates.
+uint64_t vcompact_status_words(uint64_t nc);
+void launch_vcompact(uint64_t nc, const unsigned long long *cand, const float *aabb, uint64_t n, DevStats *stats,
+                     unsigned long long *out, uint64_t out_cap, uint64_t *status, uint32_t *ticket, bool rebuild,
+                     float margin, cudaStream_t s);
 
 // ------------------------------------------------------------------ batches
 // Per-scene accumulators of the batch bounds pass (zeroed per call).

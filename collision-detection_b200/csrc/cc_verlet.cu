@@ -62,14 +62,36 @@ __global__ void __launch_bounds__(kNT) k_vcheck(uint64_t n, float *__restrict__ 
 	if (threadIdx.x == 0) valid = stats->plan.valid;
 	__syncthreads();
 	if (!valid) return;
-	const uint64_t total = 6 * n, step = (uint64_t)gridDim.x * kNT;
+	const float o0 = origin[0], o1 = origin[1], o2 = origin[2];
+	float *hi = aabb + 3 * n;
+	const float *rhi = ref + 3 * n;
+	const uint64_t step = (uint64_t)gridDim.x * kNT;
 	float dmax = 0.f;
-	for (uint64_t k = (uint64_t)blockIdx.x * kNT + threadIdx.x; k < total; k += step) {
-		const float v = aabb[k];
-		dmax = fmaxf(dmax, fabsf(v - ref[k]));
-		const int t = __ldg(T + (k < 3 * n ? k : k - 3 * n) / 3);
-		if (t == RECT || t == TRIANGLEMESH) backup[k] = v;
-		aabb[k] = v + origin[k % 3];
+	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < n; i += step) {  // box i: both corners
+		float v[6], r[6];
+#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			v[d] = aabb[3 * i + d];
+			v[3 + d] = hi[3 * i + d];
+			r[d] = ref[3 * i + d];
+			r[3 + d] = rhi[3 * i + d];
+		}
+#pragma unroll
+		for (int k = 0; k < 6; k++) dmax = fmaxf(dmax, fabsf(v[k] - r[k]));
+		const int t = __ldg(T + i);
+		if (t == RECT || t == TRIANGLEMESH) {
+#pragma unroll
+			for (int d = 0; d < 3; d++) {
+				backup[3 * i + d] = v[d];
+				backup[3 * n + 3 * i + d] = v[3 + d];
+			}
+		}
+		aabb[3 * i] = v[0] + o0;
+		aabb[3 * i + 1] = v[1] + o1;
+		aabb[3 * i + 2] = v[2] + o2;
+		hi[3 * i] = v[3] + o0;
+		hi[3 * i + 1] = v[4] + o1;
+		hi[3 * i + 2] = v[5] + o2;
 	}
 	dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, 16));
 	dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, 8));
@@ -94,51 +116,71 @@ __device__ __forceinline__ bool step_fits(const DevStats *stats, float margin) {
 	return stats->vdisp == 0u ? limit >= 0.f : ord2f(stats->vdisp) <= limit;
 }
 
-// flags[i] = candidate i overlaps on this step's shifted boxes (all zero, and
-// stats->vbad set, when the step moved too far).
-// A rebuild step's own candidates always hold its pairs (no displacement).
-__global__ void __launch_bounds__(kNT) k_vfilter(uint64_t nc, const unsigned long long *__restrict__ cand,
-                                                  const float *__restrict__ aabb, uint64_t n, DevStats *stats,
-                                                  uint32_t *__restrict__ flags, int rebuild, float margin) {
+// The candidates that overlap on this step's shifted boxes, in order, into
+// out (positions past out_cap are not written): one pass over tiles of
+// kVcTile candidates with a decoupled look-back for their offsets (tiles take
+// their indices from a ticket, so every tile a tile waits on has started).
+// The last tile writes the total (stats->pairs) and stats->np_n (0 when the
+// list does not fit out). A rebuild step's own candidates always hold its
+// pairs; a kept step that moved too far, or invalid input, passes nothing
+// and sets stats->vbad.
+constexpr int kVcIPT = 8;
+constexpr uint64_t kVcTile = (uint64_t)kNT * kVcIPT;
+__global__ void __launch_bounds__(kNT) k_vcompact(uint64_t nc, const unsigned long long *__restrict__ cand,
+                                                   const float *__restrict__ aabb, uint64_t n, DevStats *stats,
+                                                   unsigned long long *__restrict__ out, uint64_t out_cap,
+                                                   uint64_t *status, uint32_t *ticket, int rebuild, float margin) {
 	pdl_begin();
-	__shared__ int fits;
-	if (threadIdx.x == 0) fits = stats->plan.valid && (rebuild || step_fits(stats, margin));
+	__shared__ uint32_t s_tile;
+	__shared__ int s_fits;
+	__shared__ unsigned long long s_pre;
+	__shared__ unsigned long long sm[40];
+	if (threadIdx.x == 0) {
+		s_tile = atomicAdd(ticket, 1u);
+		s_fits = stats->plan.valid && (rebuild || step_fits(stats, margin));
+	}
 	__syncthreads();
-	if (!fits && blockIdx.x == 0 && threadIdx.x == 0) stats->vbad = 1u;
+	const uint32_t tile = s_tile;
+	const bool fits = s_fits != 0;
+	if (!fits && tile == 0 && threadIdx.x == 0) stats->vbad = 1u;
 	const float *mx = aabb + 3 * n;
-	const uint64_t step = (uint64_t)gridDim.x * kNT;
-	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < nc; i += step) {
-		uint32_t f = 0u;
-		if (fits) {
-			const unsigned long long key = cand[i];
-			const uint64_t a = key >> 32, b = key & 0xffffffffull;
+	const uint64_t i0 = (uint64_t)tile * kVcTile + (uint64_t)threadIdx.x * kVcIPT;
+	unsigned long long key[kVcIPT];
+	uint32_t keep = 0;  // bit j: candidate i0 + j overlaps
+#pragma unroll
+	for (int j = 0; j < kVcIPT; j++) {
+		key[j] = 0ull;
+		const uint64_t i = i0 + j;
+		if (fits && i < nc) {
+			key[j] = cand[i];
+			const uint64_t a = key[j] >> 32, b = key[j] & 0xffffffffull;
 			if (a < n && b < n) {
 				const float *pa = aabb + 3 * a, *pb = aabb + 3 * b, *qa = mx + 3 * a, *qb = mx + 3 * b;
-				f = pa[0] <= qb[0] && pb[0] <= qa[0] && pa[1] <= qb[1] && pb[1] <= qa[1] && pa[2] <= qb[2] &&
-				    pb[2] <= qa[2];
+				if (pa[0] <= qb[0] && pb[0] <= qa[0] && pa[1] <= qb[1] && pb[1] <= qa[1] && pa[2] <= qb[2] &&
+				    pb[2] <= qa[2])
+					keep |= 1u << j;
 			}
 		}
-		flags[i] = f;
 	}
-}
-
-// The overlapping candidates, in order, into out (if they fit its capacity).
-__global__ void __launch_bounds__(kNT) k_vscatter(uint64_t nc, const unsigned long long *__restrict__ cand,
-                                                   const uint32_t *__restrict__ flags,
-                                                   const unsigned long long *__restrict__ pos,
-                                                   unsigned long long *__restrict__ out, uint64_t out_cap,
-                                                   DevStats *stats) {
-	pdl_begin();
-	const unsigned long long P = pos[nc];
-	const bool fits = P <= out_cap;
-	if (blockIdx.x == 0 && threadIdx.x == 0) {
+	unsigned long long total;
+	const unsigned long long excl = block_excl_scan<unsigned long long, kNT>(__popc(keep), sm, &total);
+	if (threadIdx.x < 32) {
+		const unsigned long long pre = lookback_prefix(status, tile, total, &stats->err);
+		if (threadIdx.x == 0) s_pre = pre;
+	}
+	__syncthreads();
+	unsigned long long pos = s_pre + excl;
+#pragma unroll
+	for (int j = 0; j < kVcIPT; j++)
+		if ((keep >> j) & 1u) {
+			if (pos < out_cap) out[pos] = key[j];
+			pos++;
+		}
+	if (tile == gridDim.x - 1 && threadIdx.x == 0) {
+		const unsigned long long P = s_pre + total;
 		stats->pairs = P;
-		stats->np_n = fits ? P : 0ull;
+		stats->np_n = P <= out_cap ? P : 0ull;
 	}
-	if (!fits) return;
-	const uint64_t step = (uint64_t)gridDim.x * kNT;
-	for (uint64_t i = (uint64_t)blockIdx.x * kNT + threadIdx.x; i < nc; i += step)
-		if (flags[i]) out[pos[i]] = cand[i];
 }
 
 unsigned grid_for(uint64_t items) {
@@ -152,18 +194,19 @@ void launch_vinflate(uint64_t n, const float *aabb, float *scratch, DevStats *st
 
 void launch_vcheck(uint64_t n, float *aabb, const float *ref, float *backup, const int32_t *T, DevStats *stats,
                    cudaStream_t s) {
-	if (n) launch_pdl(k_vcheck, dim3(grid_for(6 * n)), dim3(kNT), 0, s, n, aabb, ref, backup, T, stats);
+	if (n) launch_pdl(k_vcheck, dim3(grid_for(n)), dim3(kNT), 0, s, n, aabb, ref, backup, T, stats);
 }
 
-void launch_vfilter(uint64_t nc, const unsigned long long *cand, const float *aabb, uint64_t n, DevStats *stats,
-                    uint32_t *flags, bool rebuild, float margin, cudaStream_t s) {
-	launch_pdl(k_vfilter, dim3(grid_for(nc)), dim3(kNT), 0, s, nc, cand, aabb, n, stats, flags, rebuild ? 1 : 0, margin);
-}
+uint64_t vcompact_status_words(uint64_t nc) { return nc / kVcTile + 2; }
 
-void launch_vscatter(uint64_t nc, const unsigned long long *cand, const uint32_t *flags,
-                     const unsigned long long *pos, unsigned long long *out, uint64_t out_cap, DevStats *stats,
-                     cudaStream_t s) {
-	launch_pdl(k_vscatter, dim3(grid_for(nc)), dim3(kNT), 0, s, nc, cand, flags, pos, out, out_cap, stats);
+void launch_vcompact(uint64_t nc, const unsigned long long *cand, const float *aabb, uint64_t n, DevStats *stats,
+                     unsigned long long *out, uint64_t out_cap, uint64_t *status, uint32_t *ticket, bool rebuild,
+                     float margin, cudaStream_t s) {
+	const uint64_t tiles = (nc + kVcTile - 1) / kVcTile;
+	cudaMemsetAsync(status, 0, sizeof(uint64_t) * vcompact_status_words(nc), s);
+	cudaMemsetAsync(ticket, 0, sizeof(uint32_t), s);
+	launch_pdl(k_vcompact, dim3((unsigned)std::max<uint64_t>(tiles, 1)), dim3(kNT), 0, s, nc, cand, aabb, n, stats,
+	           out, out_cap, status, ticket, rebuild ? 1 : 0, margin);
 }
 
 }  // namespace cc
