@@ -101,6 +101,36 @@ __device__ __forceinline__ vec<T> unit(vec<T> a) {
 		return {a.x * il, a.y * il, a.z * il};
 	}
 }
+
+// a / sqrt(a.a) in double with IEEE results, without the square root and the
+// reciprocal when a.a lies within 2^20 units in the last place of 1 (a vector
+// normalized once already). With s = a.a whose bits are bits(1) + e:
+//  * sqrt(s) has the bits bits(1) + floor(e / 2). For s = 1 + t, sqrt(s) lies
+//    strictly below 1 + t/2 (concavity) and above 1 + t/2 - t^2/8. Above 1
+//    (t = e 2^-52) 1 + t/2 is representable for even e and a midpoint for odd
+//    e; below 1 (t = e 2^-53, spacing 2^-53) the same holds with the halved
+//    spacing. Either way the correctly rounded root is the representable
+//    number at or just below 1 + t/2, t^2/8 being far below half a spacing.
+//  * RN(1 / l) for l with the bits bits(1) + f: for f >= 0, 1/l lies above
+//    1 - f 2^-52 (representable, bits(1) - 2f) by less than f^2 2^-104, under
+//    half the spacing 2^-53 below 1; for f < 0, 1/l lies strictly above
+//    1 - f 2^-53, which is representable (bits(1) - f/2) for even f and a
+//    midpoint for odd f, so RN gives bits(1) + ceil(-f / 2) = bits(1) -
+//    floor(f / 2).
+// The quotients then follow quot_rcp (Markstein) as in div3, so the result is
+// bit for bit unit<double, true>(a).
+__device__ __forceinline__ vec<double> unit_again(vec<double> a) {
+	constexpr long long kOne = 0x3FF0000000000000ll, kNear = 1ll << 20;
+	const long long e = __double_as_longlong(dotp(a, a)) - kOne;
+	if (e >= -kNear && e <= kNear && quot_range(a.x) && quot_range(a.y) && quot_range(a.z)) {
+		const long long f = e >> 1;  // arithmetic shift: floor(e / 2)
+		const double l = __longlong_as_double(kOne + f);
+		const double y = __longlong_as_double(f >= 0 ? kOne - 2 * f : kOne - (f >> 1));
+		return {quot_rcp(a.x, l, y), quot_rcp(a.y, l, y), quot_rcp(a.z, l, y)};
+	}
+	return unit<double, true>(a);
+}
+
 template <class T>
 __device__ __forceinline__ T sgn(T x) { return x > T(0) ? T(1) : (x < T(0) ? T(-1) : T(0)); }
 template <class T>
@@ -569,7 +599,8 @@ __device__ __forceinline__ void run(uint64_t P_cap, const unsigned long long *P_
 		}
 		// the support pair: support(A, -n), support(B, n)
 		vec<S> d = cvt<S>(L.n);
-		if constexpr (kExact) d = unit<S, true>(d);
+		if constexpr (kExact && sizeof(S) == 8) d = unit_again(d);  // n is a unit vector when refining
+		else if constexpr (kExact) d = unit<S, true>(d);
 		const vec<S> pa = support<S, kExact>(L.A, neg(d));
 		const vec<S> pb = support<S, kExact>(L.B, d);
 		if (!post_step(L, pa, pb, sc, ida, idb)) L.st = kIdle;
