@@ -295,7 +295,9 @@ __device__ __forceinline__ Shape<S> load_shape(uint32_t s, uint32_t id, const in
 }
 
 // Per-lane MPR state.
-enum State : int { kIdle = 0, kS1, kS2, kDisc, kRefine, kPost };
+// kParked: the refinement has ended with a hit and the lane waits, its portal
+// kept, for the warp to finish all such pairs together (run()).
+enum State : int { kIdle = 0, kS1, kS2, kDisc, kRefine, kPost, kParked };
 
 template <class S, bool kExact>
 struct Lane {
@@ -441,11 +443,39 @@ __device__ __forceinline__ bool pre_step(Lane<S, kExact> &L) {
 	return true;
 }
 
+// The end of a refinement with a hit (:256-283 once the portal is final): the
+// barycentric contact point and the normal; the post stage then evaluates one
+// more support pair along the normal.
+template <class S, bool kExact>
+__device__ __forceinline__ void finish_refine(Lane<S, kExact> &L) {
+	const D3 v1 = L.v1, v2 = L.v2, v3v = L.v3, v0 = L.v0, n = L.n;
+	double b0 = dotp(crossp(v1, v2), v3v);
+	double b1 = dotp(crossp(v3v, v2), v0);
+	double b2 = dotp(crossp(v0, v1), v3v);
+	double b3 = dotp(crossp(v2, v1), v0);
+	double sum = b0 + b1 + b2 + b3;
+	if (sum <= 0.0) {
+		b0 = 0.0;
+		b1 = dotp(crossp(v2, v3v), n);
+		b2 = dotp(crossp(v3v, v1), n);
+		b3 = dotp(crossp(v1, v2), n);
+		sum = b1 + b2 + b3;
+	}
+	const double inv = 1.0 / sum;
+	const D3 v01 = centre(L.A), v02 = centre(L.B);
+	const D3 p = add(add(add(scl(b0, v01), scl(b1, dd(L.v11))), scl(b2, dd(L.v21))), scl(b3, dd(L.v31)));
+	const D3 q = add(add(add(scl(b0, v02), scl(b1, dd(L.v12))), scl(b2, dd(L.v22))), scl(b3, dd(L.v32)));
+	const D3 pq = add(p, q);
+	const D3 pt = mk(pq.x * inv * 0.5, pq.y * inv * 0.5, pq.z * inv * 0.5);
+	to_post(L, unit<double, kExact>(n), pt);
+}
+
 // State update after the support pair (pa = support(A,-n), pb = support(B,n)).
-// Returns false when the pair is finished.
+// Returns false when the pair is finished. park: a refinement that ends with a
+// hit leaves its portal as it is (kParked) instead of finishing it here.
 template <class S, bool kExact>
 __device__ __forceinline__ bool post_step(Lane<S, kExact> &L, vec<S> pa, vec<S> pb, const NpScratch &sc,
-                                          uint32_t ida, uint32_t idb) {
+                                          uint32_t ida, uint32_t idb, bool park) {
 	switch (L.st) {
 	case kS1: {  // :146-171
 		L.v11 = pa;
@@ -510,26 +540,8 @@ __device__ __forceinline__ bool post_step(Lane<S, kExact> &L, vec<S> pa, vec<S> 
 		             s43 = dotp(crossp(v4, L.v3), L.v0);
 		if (delta <= 1e-20 || depth <= 0.0 || L.phase2 > kMaxIter) {
 			if (!L.hit) return false;
-			const D3 v1 = L.v1, v2 = L.v2, v3v = L.v3, v0 = L.v0, n = L.n;
-			double b0 = dotp(crossp(v1, v2), v3v);
-			double b1 = dotp(crossp(v3v, v2), v0);
-			double b2 = dotp(crossp(v0, v1), v3v);
-			double b3 = dotp(crossp(v2, v1), v0);
-			double sum = b0 + b1 + b2 + b3;
-			if (sum <= 0.0) {
-				b0 = 0.0;
-				b1 = dotp(crossp(v2, v3v), n);
-				b2 = dotp(crossp(v3v, v1), n);
-				b3 = dotp(crossp(v1, v2), n);
-				sum = b1 + b2 + b3;
-			}
-			const double inv = 1.0 / sum;
-			const D3 v01 = centre(L.A), v02 = centre(L.B);
-			const D3 p = add(add(add(scl(b0, v01), scl(b1, dd(L.v11))), scl(b2, dd(L.v21))), scl(b3, dd(L.v31)));
-			const D3 q = add(add(add(scl(b0, v02), scl(b1, dd(L.v12))), scl(b2, dd(L.v22))), scl(b3, dd(L.v32)));
-			const D3 pq = add(p, q);
-			const D3 pt = mk(pq.x * inv * 0.5, pq.y * inv * 0.5, pq.z * inv * 0.5);
-			to_post(L, unit<double, kExact>(n), pt);
+			if (park) L.st = kParked;
+			else finish_refine(L);
 			return true;
 		}
 		if (s41 < 0.0) {
@@ -554,7 +566,12 @@ __device__ __forceinline__ bool post_step(Lane<S, kExact> &L, vec<S> pa, vec<S> 
 
 // Persistent kernel: lanes take pairs from the global queue `order`
 // (P = min(P_cap, *P_dev) entries), one support pair per busy lane per
-// iteration.
+// iteration. Once the warp has seen the queue drained, a refinement that ends
+// with a hit parks, and the parked pairs of the warp are finished together
+// when none of its lanes runs any more: the warp then runs the finishing code
+// (barycentric point, normal, one more support pair, the contact) once instead
+// of once for every pair that ends at a different iteration. The finishing
+// arithmetic reads only the parked portal, so the contacts are the same.
 template <class S, bool kExact, int NT>
 __device__ __forceinline__ void run(uint64_t P_cap, const unsigned long long *P_dev, uint64_t n, const int32_t *T,
                                     const float *A, const float *B, const float *C, const float *R, const uint32_t *ID,
@@ -563,7 +580,8 @@ __device__ __forceinline__ void run(uint64_t P_cap, const unsigned long long *P_
 	const uint64_t P = P_dev ? min(P_cap, (uint64_t)*P_dev) : P_cap;
 	Lane<S, kExact> L;
 	L.st = kIdle;
-	bool done = false;  // the queue is exhausted for this lane
+	bool done = false;     // the queue is exhausted for this lane
+	bool drained = false;  // the warp has taken the last queue entries (warp-uniform)
 	uint32_t ida = 0, idb = 0;
 	const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
 	while (true) {
@@ -575,6 +593,7 @@ __device__ __forceinline__ void run(uint64_t P_cap, const unsigned long long *P_
 			const int leader = __ffs(m) - 1;
 			if ((int)lane == leader) base = atomicAdd(queue, (uint32_t)__popc(m));
 			base = __shfl_sync(0xffffffffu, base, leader);
+			drained = drained || (uint64_t)base + __popc(m) >= P;
 			if (want) {
 				const uint64_t j = (uint64_t)base + __popc(m & lt);
 				if (j >= P) {
@@ -591,8 +610,15 @@ __device__ __forceinline__ void run(uint64_t P_cap, const unsigned long long *P_
 				}
 			}
 		}
-		if (!__any_sync(0xffffffffu, L.st != kIdle || !done)) break;
-		if (L.st == kIdle) continue;
+		done = done || drained;
+		const bool running = L.st != kIdle && L.st != kParked;
+		if (!__any_sync(0xffffffffu, running || !done)) {
+			const bool parked = L.st == kParked;
+			if (!__any_sync(0xffffffffu, parked)) break;
+			if (parked) finish_refine(L);  // -> kPost: the next iteration writes the contact
+			continue;
+		}
+		if (!running) continue;
 		if (!pre_step(L)) {
 			L.st = kIdle;
 			continue;
@@ -603,7 +629,7 @@ __device__ __forceinline__ void run(uint64_t P_cap, const unsigned long long *P_
 		else if constexpr (kExact) d = unit<S, true>(d);
 		const vec<S> pa = support<S, kExact>(L.A, neg(d));
 		const vec<S> pb = support<S, kExact>(L.B, d);
-		if (!post_step(L, pa, pb, sc, ida, idb)) L.st = kIdle;
+		if (!post_step(L, pa, pb, sc, ida, idb, drained)) L.st = kIdle;
 	}
 }
 
