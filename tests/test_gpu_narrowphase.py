@@ -72,6 +72,17 @@ def test_narrowphase_1m_exact_equals_fp64_oracle(cb, scene_1m):
     check_exact(contact_errors(run_np(cb, m, p), ref, scale_of(m)))
 
 
+def test_narrowphase_more_pairs_than_lanes_exact(cb):
+    """66,705 pairs, more than the exact kernel's resident lanes (~38K on
+    B200): early lanes finish their pairs in place and take more from the
+    queue, later ones park their finished refinements until the warp is done.
+    Both ways must give the oracle's contacts."""
+    m = S.mixed_slab(1 << 18, seed=3, extent=(1.6, 1.6, 0.5))
+    _, p = O.broadphase(O.aabb(m), (80, 80, 25))
+    assert len(p) > 60_000
+    check_exact(contact_errors(run_np(cb, m, p), O.narrowphase(m, p, 0.0, "f64"), scale_of(m)))
+
+
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
 def test_narrowphase_1m_fast_modes_within_bounds(cb, scene_1m, mode):
     m, p, ref = scene_1m
